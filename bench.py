@@ -1,0 +1,318 @@
+"""Throughput of the B200 SCN TLM step (node-updates/s and % of HBM roofline).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload heterogeneous|plain|precision] [--storage f32|bf16|f16|f64]
+
+A "step" is one TLM time step (inject, monitors, scatter, connect) of the
+whole grid. Default workload: 192^3 heterogeneous grid (16 lossy dielectric
+boxes, differentiated-Gaussian source, 8 probes), FP32, synthetic and seeded.
+Under torchrun every rank advances its own replica (weak scaling; the
+instances are independent, so no collective is on the data path); times are
+CUDA-event times on the solver's stream, max over ranks.
+
+`--impl reference` times the reference's own CPU TLM step (compiled headless
+under oracle/_ref from its sources) on the host cores for the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TLM node-updates/s"
+UNIT = "node-updates/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10000)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="heterogeneous",
+                   choices=["heterogeneous", "plain", "precision"])
+    p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64"])
+    p.add_argument("--steps-per-launch", type=int, default=0)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def make_workload(name, steps):
+    from emsolver_b200 import workloads
+    if name == "plain":
+        return workloads.plain_free_space(steps=steps)
+    if name == "precision":
+        return workloads.precision_dipole(steps=steps)
+    return workloads.heterogeneous(steps=2000)
+
+
+STORAGE = {"f32": (0, 4, 4), "bf16": (1, 2, 4), "f16": (2, 2, 4), "f64": (3, 8, 8)}
+DTYPE = {"f32": "f32", "bf16": "bf16 storage / f32 arithmetic",
+         "f16": "f16 storage / f32 arithmetic", "f64": "f64"}
+
+
+# ---------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self, n):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            t = torch.zeros(1, device="cuda")
+            self.pg.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([float(v)], device="cuda", dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.path = None
+        self.gpu = gpu_index
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- helpers
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload, storage):
+    """DRAM bytes per step-kernel launch from the committed ncu capture."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    d = json.load(open(path))
+    return d.get(f"{workload}_{storage}")
+
+
+def reference_rate(w, steps_budget, seconds_budget, warm=2):
+    """The reference's own CPU step on this host: node-updates/s over a
+    bounded number of full-grid steps."""
+    from oracle import RefSolver, Oracle, drive, ref_available
+    if ref_available():
+        S, kind = RefSolver(), "reference"
+    else:
+        S, kind = Oracle(False), "port"
+    drive.setup(S, w)
+    drive.advance(S, w, warm)
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps_budget:
+        chunk = min(5, steps_budget - done)
+        drive.advance(S, w, chunk)
+        done += chunk
+        if time.perf_counter() - t0 > seconds_budget:
+            break
+    dt = time.perf_counter() - t0
+    cores = S.threads if kind == "reference" else 1
+    return w.ncells * done / dt, cores, kind, done, dt
+
+
+def run_reference_arm(args):
+    d = Dist(args.gpus) if int(os.environ.get("WORLD_SIZE", "1")) > 1 else None
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from emsolver_b200 import workloads  # noqa: F401
+    w = make_workload(args.workload, args.warmup + args.steps)
+    rate, cores, kind, done, dt = reference_rate(w, args.steps, 120.0, warm=min(args.warmup, 3))
+    line = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * dt / done, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "impl": "reference",
+        "config": {"workload": f"{args.workload} {w.nx}x{w.ny}x{w.nz}", "steps_timed": done},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{done} full-grid steps of {w.nx}x{w.ny}x{w.nz} "
+                                   f"({os.cpu_count()} host cores, {cores} solver threads)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if d:
+        d.close()
+
+
+def run_ours(args):
+    from emsolver_b200.runner import build_solver
+    import torch
+
+    dist = Dist(args.gpus)
+    dev = dist.local if dist.world > 1 else 0
+    code, sbytes, rbytes = STORAGE[args.storage]
+    w = make_workload(args.workload, args.warmup + args.steps)
+    w.steps = args.warmup + args.steps
+    s = build_solver(w, device=dev, storage=code, steps_per_launch=args.steps_per_launch)
+    s.step(args.warmup)
+    torch.cuda.set_device(dev)
+    ext = torch.cuda.ExternalStream(s.stream(), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    s.sync()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    s.setKernelTiming(True)
+    e0.record(ext)
+    s.stepAsync(args.steps)
+    e1.record(ext)
+    s.sync()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    kern_ms, launches = s.kernelTime()
+    s.setKernelTiming(False)
+    ms_max = dist.max(ms)
+    kern_max = dist.max(kern_ms)
+    s.close()
+
+    n = w.ncells
+    value = dist.world * n * args.steps / (ms_max / 1000.0)
+    bytes_step = w.bytes_per_step(sbytes, rbytes)
+    per_launch_ms = kern_max / max(launches, 1)
+    achieved = bytes_step / (per_launch_ms / 1000.0) / 1e9
+    peak, peak_kind = peaks()
+    window = args.steps_per_launch or 64
+    epilogues = -(-args.steps // window)
+
+    # end to end through the public API: host material map in, setup,
+    # K steps, probe and port records back to the host.
+    e2e = None
+    if not args.no_e2e:
+        dist.barrier()
+        t0 = time.perf_counter()
+        s2 = build_solver(w, device=dev, storage=code, steps_per_launch=args.steps_per_launch)
+        s2.step(args.steps)
+        recs = [s2.probe(q) for q in range(len(w.probes_cell))]
+        ports = [s2.port(p) for p in range(len(w.ports))]
+        t1 = time.perf_counter()
+        s2.close()
+        dt = dist.max(t1 - t0)
+        h2d = w.mat.nbytes + 8 * len(w.table) + (w.sv.nbytes if w.sv is not None else 0)
+        d2h = sum(3 * 4 * r.ez.size for r in recs) + sum(2 * 4 * p.vRec.size for p in ports)
+        e2e = {"value": dist.world * n * args.steps / dt, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "seconds": dt, "includes": "setup (H2D of the material map, tables, sources), "
+                                          "all steps, D2H of probe and port records"}
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        rate, cores, kind, done, dt = reference_rate(w, 400, 20.0)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"{done} full-grid steps of {w.nx}x{w.ny}x{w.nz} in {dt:.1f}s "
+                         f"({os.cpu_count()} host cores)"}
+
+    if dist.rank == 0:
+        tr = ncu_traffic(args.workload, args.storage)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": DTYPE[args.storage], "data": "synthetic (seeded)",
+            "config": {"workload": f"{args.workload} {w.nx}x{w.ny}x{w.nz}, {len(w.table)} lossy "
+                                   f"dielectric boxes, {len(w.probes_cell)} probes",
+                       "nodes": n, "dielectric_nodes": w.n_diel(),
+                       "storage": args.storage, "steps_per_launch": window,
+                       "parallelism": f"replicas x{dist.world}",
+                       "l2": f"state {2 * 12 * sbytes * n / 1e6:.0f} MB > L2 (126 MB); no flush"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": tr, "algorithmic_bytes_per_launch": bytes_step,
+                         "kernel_ms_per_launch": per_launch_ms},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches + epilogues,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

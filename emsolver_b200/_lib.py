@@ -1,0 +1,137 @@
+"""ctypes binding of the in-tree C ABI (include/tlm_b200.h).
+
+The library is loaded from this package directory. There is no fallback: if
+``libtlm_b200.so`` is missing or cannot be loaded, importing the binding
+raises, and every compute call fails unless a CUDA device is present.
+Set ``TLM_B200_VARIANT=checked`` to load the bounds-checked build instead.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+TLM_OK, TLM_EINVAL, TLM_ENOMEM, TLM_ECUDA, TLM_ETIMEOUT, TLM_ESTOPPED, TLM_ESTATE, TLM_ENODEV, \
+    TLM_EBUSY = range(9)
+STATUS_NAMES = {0: "TLM_OK", 1: "TLM_EINVAL", 2: "TLM_ENOMEM", 3: "TLM_ECUDA", 4: "TLM_ETIMEOUT",
+                5: "TLM_ESTOPPED", 6: "TLM_ESTATE", 7: "TLM_ENODEV", 8: "TLM_EBUSY"}
+
+STORE_F32, STORE_BF16, STORE_F16, STORE_F64 = range(4)
+WAVE_CW_RAMPED, WAVE_GAUSSIAN_SINE, WAVE_GAUSSIAN_PULSE, WAVE_TABLE = range(4)
+
+
+class TlmError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("origin", C.c_float * 3),
+                ("dl", C.c_float)]
+
+
+class MatPropsC(C.Structure):
+    _fields_ = [("epsr", C.c_float), ("sigma", C.c_float)]
+
+
+class ConfigC(C.Structure):
+    _fields_ = [("f0", C.c_float), ("waveform", C.c_int), ("total_steps", C.c_int),
+                ("settle_steps", C.c_int), ("boundary_rho", C.c_float), ("huy_offset", C.c_int),
+                ("use_gpu", C.c_int), ("record_every", C.c_int), ("storage", C.c_int),
+                ("pulse_scale", C.c_float), ("steps_per_launch", C.c_int)]
+
+
+_h = C.c_void_p
+_st = C.c_int
+_P = C.POINTER
+
+# name -> (restype, argtypes): every symbol include/tlm_b200.h declares.
+SIGNATURES = {
+    "tlm_version": (C.c_char_p, []),
+    "tlm_config_default": (None, [_P(ConfigC)]),
+    "tlm_create": (_st, [_P(_h), C.c_int]),
+    "tlm_destroy": (_st, [_h]),
+    "tlm_last_error": (C.c_char_p, [_h]),
+    "tlm_setup": (_st, [_h, _P(Grid), _P(C.c_uint8), C.c_size_t, _P(MatPropsC), C.c_int,
+                        _P(ConfigC)]),
+    "tlm_add_port": (_st, [_h, _P(C.c_uint64), C.c_int, C.c_int, C.c_float, _P(C.c_int)]),
+    "tlm_add_plane_wave": (_st, [_h, C.c_int, C.c_int, C.c_int, C.c_float]),
+    "tlm_add_probe": (_st, [_h, C.c_float, C.c_float, C.c_float, _P(C.c_int)]),
+    "tlm_add_probe_cell": (_st, [_h, C.c_int, C.c_int, C.c_int, _P(C.c_int)]),
+    "tlm_set_source_table": (_st, [_h, _P(C.c_float), C.c_int]),
+    "tlm_set_port_dft": (_st, [_h, _P(C.c_double), C.c_int]),
+    "tlm_step": (_st, [_h, C.c_int]),
+    "tlm_step_async": (_st, [_h, C.c_int]),
+    "tlm_sync": (_st, [_h]),
+    "tlm_run": (_st, [_h]),
+    "tlm_request_stop": (_st, [_h]),
+    "tlm_current_step": (C.c_int, [_h]),
+    "tlm_current_energy": (C.c_float, [_h]),
+    "tlm_is_running": (C.c_int, [_h]),
+    "tlm_is_finished": (C.c_int, [_h]),
+    "tlm_total_steps": (C.c_int, [_h]),
+    "tlm_timestep": (_st, [_h, _P(C.c_float)]),
+    "tlm_probe_count": (C.c_int, [_h]),
+    "tlm_get_probe": (_st, [_h, C.c_int, _P(C.c_float), _P(C.c_float), _P(C.c_float), C.c_int,
+                            _P(C.c_int)]),
+    "tlm_get_probe_f64": (_st, [_h, C.c_int, _P(C.c_double), _P(C.c_double), _P(C.c_double),
+                                C.c_int, _P(C.c_int)]),
+    "tlm_get_probe_cell": (_st, [_h, C.c_int, _P(C.c_uint64)]),
+    "tlm_port_count": (C.c_int, [_h]),
+    "tlm_get_port": (_st, [_h, C.c_int, _P(C.c_float), _P(C.c_float), C.c_int, _P(C.c_int)]),
+    "tlm_get_port_f64": (_st, [_h, C.c_int, _P(C.c_double), _P(C.c_double), C.c_int,
+                               _P(C.c_int)]),
+    "tlm_get_port_cells": (_st, [_h, C.c_int, _P(C.c_uint64), C.c_int, _P(C.c_int)]),
+    "tlm_get_port_dft": (_st, [_h, C.c_int, _P(C.c_double), _P(C.c_double), _P(C.c_double),
+                               _P(C.c_double), C.c_int, _P(C.c_int)]),
+    "tlm_get_energy_history": (_st, [_h, _P(C.c_int), _P(C.c_float), _P(C.c_double), C.c_int,
+                                     _P(C.c_int)]),
+    "tlm_get_pulses": (_st, [_h, _P(C.c_float), C.c_size_t]),
+    "tlm_get_pulses_f64": (_st, [_h, _P(C.c_double), C.c_size_t]),
+    "tlm_set_pulses": (_st, [_h, _P(C.c_float), C.c_size_t]),
+    "tlm_get_stubs": (_st, [_h, _P(C.c_float), C.c_size_t]),
+    "tlm_get_materials": (_st, [_h, _P(C.c_uint8), C.c_size_t]),
+    "tlm_get_tables": (_st, [_h, _P(C.c_float), _P(C.c_float), C.c_int, _P(C.c_int)]),
+    "tlm_waveform_value": (_st, [C.c_int, C.c_float, C.c_float, C.c_int, _P(C.c_float)]),
+    "tlm_scatter_unitarity_error": (_st, [C.c_int, _P(C.c_float)]),
+    "tlm_stub_unitarity_error": (_st, [C.c_int, C.c_float, _P(C.c_float)]),
+    "tlm_get_stream": (_st, [_h, _P(C.c_void_p)]),
+    "tlm_device_bytes": (_st, [_h, _P(C.c_size_t)]),
+    "tlm_set_kernel_timing": (_st, [_h, C.c_int]),
+    "tlm_kernel_time": (_st, [_h, _P(C.c_double), _P(C.c_longlong)]),
+}
+
+
+def library_path(variant: str | None = None) -> str:
+    variant = variant or os.environ.get("TLM_B200_VARIANT", "")
+    name = "libtlm_b200_checked.so" if variant == "checked" else "libtlm_b200.so"
+    return os.path.join(HERE, name)
+
+
+_LIBS: dict = {}
+
+
+def load(variant: str | None = None):
+    """Load (once) and return the C library with its prototypes set."""
+    path = library_path(variant)
+    if path in _LIBS:
+        return _LIBS[path]
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is not built; run emsolver_b200.build.build() "
+                          "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIBS[path] = lib
+    return lib
+
+
+def check(lib, h, status):
+    if status != TLM_OK:
+        msg = lib.tlm_last_error(h)
+        raise TlmError(status, msg.decode() if msg else "")
+    return status

@@ -1,0 +1,286 @@
+// tlm_aux_kernels.cuh -- small kernels around the step kernel:
+//  * windowEpilogue: once per launch window, turns the per-step monitor
+//    samples into the reference's port V/I and probe E records, advances the
+//    FP64 running DFT of every port, and reduces the block energy partials
+//    in a fixed order (deterministic) into the energy history;
+//  * incidentToAos / aosToIncident / stubsToAos: state import and export in
+//    the reference's AoS layout (cell*12 + slot, cell*3 + j);
+//  * unitarityKernel: the reference's scatter known-answer tests evaluated
+//    with the device scatter functions.
+#pragma once
+
+#include "tlm_device.cuh"
+
+namespace tlmk {
+
+template <class R> struct EpilogueArgs
+{
+    const R *samples;       // [w][nsamp][6]: V_x V_y V_z ZI_x ZI_y ZI_z
+    int nsamp;
+    int w;                  // steps in this window
+    long long base;         // absolute index of the window's first step
+    int nports;
+    const int *port_off;    // [nports+1] into port_slots
+    const int *port_slots;  // sample slot of each kept gap cell, in order
+    const int *port_pol;    // E axis of each port
+    const int *port_nb;     // [nports][4] sample slots of the current loop
+    int nprobes;
+    const int *probe_slot;
+    R probe_scale;          // -1/dl
+    R eta0;
+    double *vrec, *irec;    // [step][nports]
+    double *prec;           // [step][nprobes][3]
+    int nfreq;
+    const double *wdt;      // 2*pi*f*dt per DFT frequency
+    double *dft;            // [nports][nfreq][4]: Vre Vim Ire Iim
+    const double *epart;    // [n_e][nblocks]
+    int nblocks;
+    int n_e;                // energy steps in this window
+    long long e_first;      // absolute index of the first energy step
+    double *ehist;          // [step/16]
+    double *elatest;        // last energy value (polled by the host)
+};
+
+template <class R> __global__ void __launch_bounds__(512) windowEpilogue(const EpilogueArgs<R> a)
+{
+    __shared__ double red[16];
+    const int nent = a.nports + a.nprobes;
+    const long long total = (long long)a.w * nent;
+    // 1. records (TlmSolver.cpp:677-713), float arithmetic in the
+    //    reference's order: V = sum of V_pol over the gap cells;
+    //    I = (-2 * zi) / eta0, zi = ZI_t2(+t1) - ZI_t2(-t1) - ZI_t1(+t2) + ZI_t1(-t2).
+    for (long long idx = threadIdx.x; idx < total; idx += blockDim.x)
+    {
+        const int i = (int)(idx / nent), e = (int)(idx % nent);
+        const long long n = a.base + i;
+        const R *smp = a.samples + (long long)i * a.nsamp * 6;
+        if (e < a.nports)
+        {
+            const int p = e, pol = a.port_pol[p];
+            R vSum = R(0);
+            for (int c = a.port_off[p]; c < a.port_off[p + 1]; ++c)
+                vSum = vSum + smp[a.port_slots[c] * 6 + pol];
+            R cur = R(0);
+            const int *nb = a.port_nb + p * 4;
+            if (nb[0] >= 0)
+            {
+                const int t1 = (pol + 1) % 3, t2 = (pol + 2) % 3;
+                R zi = R(0);
+                zi = zi + smp[nb[0] * 6 + 3 + t2];
+                zi = zi - smp[nb[1] * 6 + 3 + t2];
+                zi = zi - smp[nb[2] * 6 + 3 + t1];
+                zi = zi + smp[nb[3] * 6 + 3 + t1];
+                cur = (R(-2) * zi) / a.eta0;
+            }
+            a.vrec[n * a.nports + p] = (double)vSum;
+            a.irec[n * a.nports + p] = (double)cur;
+        }
+        else
+        {
+            const int pr = e - a.nports;
+            const R *s = smp + a.probe_slot[pr] * 6;
+            double *d = a.prec + (n * a.nprobes + pr) * 3;
+            d[0] = (double)(a.probe_scale * s[0]);
+            d[1] = (double)(a.probe_scale * s[1]);
+            d[2] = (double)(a.probe_scale * s[2]);
+        }
+    }
+    __syncthreads();
+    // 2. FP64 running DFT: X(f) += x[n] exp(-j w n); the phasor is seeded
+    //    with sincos at the window start and rotated per step.
+    for (int idx = threadIdx.x; idx < a.nports * a.nfreq; idx += blockDim.x)
+    {
+        const int p = idx / a.nfreq, f = idx % a.nfreq;
+        const double w = a.wdt[f];
+        double c, s, cw, sw;
+        sincos(w * (double)a.base, &s, &c);
+        sincos(w, &sw, &cw);
+        double *acc = a.dft + ((long long)p * a.nfreq + f) * 4;
+        double vr = acc[0], vi = acc[1], ir = acc[2], ii = acc[3];
+        for (int i = 0; i < a.w; ++i)
+        {
+            const long long n = a.base + i;
+            const double v = a.vrec[n * a.nports + p], cu = a.irec[n * a.nports + p];
+            vr += v * c;
+            vi -= v * s;
+            ir += cu * c;
+            ii -= cu * s;
+            const double c2 = c * cw - s * sw;
+            s = s * cw + c * sw;
+            c = c2;
+        }
+        acc[0] = vr;
+        acc[1] = vi;
+        acc[2] = ir;
+        acc[3] = ii;
+    }
+    // 3. energy history (TlmSolver.cpp:766-789), fixed-order FP64 reduction.
+    for (int e = 0; e < a.n_e; ++e)
+    {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < a.nblocks; b += blockDim.x)
+            s += a.epart[(long long)e * a.nblocks + b];
+        const double tot = blockSumDouble(s, red);
+        if (threadIdx.x == 0)
+        {
+            const long long n = a.e_first + 16LL * e;
+            a.ehist[n / 16] = tot;
+            *a.elatest = tot;
+        }
+        __syncthreads();
+    }
+}
+
+// Connect applied to a reflected state: the incident pulses the next step
+// would see, in the reference's AoS layout (the reference's V).
+template <class S, class O>
+__global__ void incidentToAos(const S *__restrict__ refl, const uint8_t *__restrict__ mat, long long P,
+                              int nx, int ny, int nz, int px, typename Traits<S>::R rho,
+                              typename Traits<S>::R scale, O *__restrict__ out)
+{
+    using R = typename Traits<S>::R;
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(c % nx);
+        const int j = (int)((c / nx) % ny);
+        const int k = (int)(c / ((long long)nx * ny));
+        const long long node = ((long long)k * ny + j) * px + i;
+        O *dst = out + c * 12;
+        if (mat[node] == kPec)
+        {
+            for (int s = 0; s < 12; ++s) dst[s] = O(0);
+            continue;
+        }
+        const int co[3] = { i, j, k };
+        const int dims[3] = { nx, ny, nz };
+        const long long st[3] = { 1, px, (long long)px * ny };
+        for (int s = 0; s < 12; ++s)
+        {
+            const int ax = s >> 2, side = (s >> 1) & 1;
+            const int qn = co[ax] + (side ? 1 : -1);
+            const R own = decode(refl[s * P + node], scale);
+            R v;
+            if (qn < 0 || qn >= dims[ax])
+                v = rho * own;
+            else
+            {
+                const long long nb = node + (side ? st[ax] : -st[ax]);
+                v = (mat[nb] == kPec) ? -own : decode(refl[(s ^ 2) * P + nb], scale);
+            }
+            dst[s] = (O)v;
+        }
+    }
+}
+
+// Incident planes (state written by tlm_set_pulses) -> AoS.
+template <class S, class O>
+__global__ void planesToAos(const S *__restrict__ planes, long long P, int nx, int ny, int nz, int px,
+                            typename Traits<S>::R scale, O *__restrict__ out)
+{
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(c % nx);
+        const int j = (int)((c / nx) % ny);
+        const int k = (int)(c / ((long long)nx * ny));
+        const long long node = ((long long)k * ny + j) * px + i;
+        for (int s = 0; s < 12; ++s) out[c * 12 + s] = (O)decode(planes[s * P + node], scale);
+    }
+}
+
+// Incident AoS state -> incident planes (PEC and padding nodes get 0).
+template <class S, class I>
+__global__ void aosToIncident(const I *__restrict__ in, const uint8_t *__restrict__ mat, long long P,
+                              int nx, int ny, int nz, int px, typename Traits<S>::R inv_scale,
+                              S *__restrict__ planes)
+{
+    using R = typename Traits<S>::R;
+    for (long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x; node < P;
+         node += (long long)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(node % px);
+        const long long r = node / px;
+        const int j = (int)(r % ny), k = (int)(r / ny);
+        const bool real = i < nx && k < nz;
+        const long long c = ((long long)k * ny + j) * nx + i;
+        for (int s = 0; s < 12; ++s)
+        {
+            R v = (real && mat[node] != kPec) ? (R)in[c * 12 + s] : R(0);
+            planes[s * P + node] = encode<S>(v, inv_scale);
+        }
+    }
+}
+
+template <class R, class O>
+__global__ void stubsToAos(const R *__restrict__ stub, long long P, int nx, int ny, int nz, int px,
+                           O *__restrict__ out)
+{
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(c % nx);
+        const int j = (int)((c / nx) % ny);
+        const int k = (int)(c / ((long long)nx * ny));
+        const long long node = ((long long)k * ny + j) * px + i;
+        for (int s = 0; s < 3; ++s) out[c * 3 + s] = (O)stub[s * P + node];
+    }
+}
+
+template <class R>
+__global__ void aosToStubs(const R *__restrict__ in, long long P, int nx, int ny, int nz, int px,
+                           R *__restrict__ stub)
+{
+    for (long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x; node < P;
+         node += (long long)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(node % px);
+        const long long r = node / px;
+        const int j = (int)(r % ny), k = (int)(r / ny);
+        const bool real = i < nx && k < nz;
+        const long long c = ((long long)k * ny + j) * nx + i;
+        for (int s = 0; s < 3; ++s) stub[s * P + node] = real ? in[c * 3 + s] : R(0);
+    }
+}
+
+// Unitarity KATs (TlmSolver.cpp:116-169): max |S^T W S - W| with W = 1 on
+// the 12 links and yh on the 3 stubs (stub case).
+__global__ void unitarityKernel(float epsr, int withStubs, float *err)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int np = withStubs ? 15 : 12;
+    const float yh = 4.0f * (epsr - 1.0f);
+    float S[15][15];
+    for (int c = 0; c < np; ++c)
+    {
+        float in[12], out[12], vs[3] = { 0.0f, 0.0f, 0.0f };
+        for (int r = 0; r < 12; ++r) in[r] = 0.0f;
+        if (c < 12) in[c] = 1.0f; else vs[c - 12] = 1.0f;
+        if (withStubs)
+            scatterStub(in, vs, yh, 0.0f, out);
+        else
+            scatterAir(in, out);
+        for (int r = 0; r < 12; ++r) S[r][c] = out[r];
+        if (withStubs)
+            for (int r = 0; r < 3; ++r) S[12 + r][c] = vs[r];
+    }
+    float worst = 0.0f;
+    for (int a = 0; a < np; ++a)
+        for (int b = 0; b < np; ++b)
+        {
+            float dot = 0.0f;
+            for (int r = 0; r < np; ++r)
+            {
+                const float w = r < 12 ? 1.0f : yh;
+                dot += (withStubs ? w * S[r][a] : S[r][a]) * S[r][b];
+            }
+            const float want = (a == b) ? (a < 12 ? 1.0f : yh) : 0.0f;
+            worst = fmaxf(worst, fabsf(dot - want));
+        }
+    *err = worst;
+}
+
+} // namespace tlmk

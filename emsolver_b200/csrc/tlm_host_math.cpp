@@ -1,0 +1,92 @@
+// tlm_host_math.cpp -- host-side scalar math that must round exactly like the
+// reference's CPU solver: time step, source waveforms and the per-material
+// stub tables. Compiled by g++ with -O2 -ffp-contract=off (no FMA
+// contraction, like the reference built for x86-64 without -march) so the
+// FP32 results are bitwise those of TlmSolver.cpp. The FP64 variants feed the
+// on-device FP64 mode and use the same float constants promoted to double.
+#include "tlm_host_math.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace tlmh {
+
+// Constants as the reference declares them (TlmSolver.cpp:15-16).
+static const float kC0 = 299792458.0f;
+static const float kEta0 = 376.730313f;
+static const double kPiD = 3.14159265358979323846;
+
+float eta0_f32() { return kEta0; }
+
+// dt = dl / (2 c0) (TlmSolver.cpp:268).
+float timestep_f32(float dl) { return dl / (2.0f * kC0); }
+double timestep_f64(float dl) { return (double)dl / (2.0 * (double)kC0); }
+
+// Source waveforms at t = n*dt (TlmSolver.cpp:410-436):
+//  0 CW with a raised-cosine ramp over 3 periods,
+//  1 Gaussian-windowed sine, tau = 2/f0, delay 3 tau,
+//  2 Gaussian pulse, tau = 0.5/f0, delay 3 tau.
+template <class T> static T waveformT(int type, float f0in, T dt, int n)
+{
+    const T pi = (T)kPiD;
+    const T f0 = (T)f0in;
+    T t = (T)n * dt;
+    T w = (T)2 * pi * f0;
+    if (type == 0)
+    {
+        T ramp = (T)3 / f0;
+        T r = (t < ramp) ? (T)0.5 * ((T)1 - std::cos(pi * t / ramp)) : (T)1;
+        return r * std::sin(w * t);
+    }
+    if (type == 1)
+    {
+        T tau = (T)2 / f0, t0 = (T)3 * tau;
+        T u = (t - t0) / tau;
+        return std::exp(-u * u) * std::sin(w * (t - t0));
+    }
+    T tau = (T)0.5 / f0, t0 = (T)3 * tau;
+    T u = (t - t0) / tau;
+    return std::exp(-u * u);
+}
+
+float waveform_f32(int type, float f0, float dt, int n) { return waveformT<float>(type, f0, dt, n); }
+double waveform_f64(int type, float f0, double dt, int n)
+{
+    return waveformT<double>(type, f0, dt, n);
+}
+
+// Stub tables (TlmSolver.cpp:270-276): yhat = 4 (max(1, er) - 1),
+// ghat = (max(0, sigma) * dl) * eta0.
+void tables_f32(const float *epsr, const float *sigma, int n, float dl, float *yhat,
+                float *ghat)
+{
+    for (int t = 0; t < n; ++t)
+    {
+        yhat[t] = 4.0f * (std::max(1.0f, epsr[t]) - 1.0f);
+        ghat[t] = std::max(0.0f, sigma[t]) * dl * kEta0;
+    }
+}
+void tables_f64(const float *epsr, const float *sigma, int n, float dl, double *yhat,
+                double *ghat)
+{
+    for (int t = 0; t < n; ++t)
+    {
+        yhat[t] = 4.0 * (std::max(1.0, (double)epsr[t]) - 1.0);
+        ghat[t] = std::max(0.0, (double)sigma[t]) * (double)dl * (double)kEta0;
+    }
+}
+
+// Probe scale -1/dl (TlmSolver.cpp:709).
+float probe_scale_f32(float dl) { return -1.0f / dl; }
+double probe_scale_f64(float dl) { return -1.0 / (double)dl; }
+
+// Cell containing a world point, floor((p - origin)/dl) in float
+// (Geometry.h:107-112).
+void cell_of(const float origin[3], float dl, float x, float y, float z, int *i, int *j, int *k)
+{
+    *i = (int)std::floor((x - origin[0]) / dl);
+    *j = (int)std::floor((y - origin[1]) / dl);
+    *k = (int)std::floor((z - origin[2]) / dl);
+}
+
+} // namespace tlmh

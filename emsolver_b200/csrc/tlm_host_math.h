@@ -1,0 +1,17 @@
+// tlm_host_math.h -- host scalar math that must match the reference bit for bit.
+#pragma once
+
+namespace tlmh {
+float eta0_f32();
+float timestep_f32(float dl);
+double timestep_f64(float dl);
+float waveform_f32(int type, float f0, float dt, int n);
+double waveform_f64(int type, float f0, double dt, int n);
+void tables_f32(const float *epsr, const float *sigma, int n, float dl, float *yhat,
+                float *ghat);
+void tables_f64(const float *epsr, const float *sigma, int n, float dl, double *yhat,
+                double *ghat);
+float probe_scale_f32(float dl);
+double probe_scale_f64(float dl);
+void cell_of(const float origin[3], float dl, float x, float y, float z, int *i, int *j, int *k);
+} // namespace tlmh

@@ -1,0 +1,1393 @@
+// tlm_solver.cu -- C ABI (include/tlm_b200.h) over the fused SCN TLM kernels.
+//
+// The handle mirrors TlmSolver's life cycle (TlmSolver.h:202-264):
+// setup -> add ports / probes / plane waves -> step or run -> read records.
+// All device state is owned here; there is no CPU execution path.
+#include "tlm_b200.h"
+
+#include "tlm_aux_kernels.cuh"
+#include "tlm_host_math.h"
+#include "tlm_step_kernel.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using tlmk::kBlock;
+using tlmk::kPadX;
+using tlmk::SpecEntry;
+
+namespace {
+
+thread_local std::string g_threadError;
+
+const char *kVersion = "tlm_b200 0.1.0 (sm_100a)";
+
+struct PortInfo
+{
+    std::vector<uint64_t> cells;  // kept (air) cells, caller order
+    int pol = 2;
+    float amp = 1.0f;
+    long long nb[4] = { -1, -1, -1, -1 };  // reference linear indices of the current loop
+};
+struct SourceInfo
+{
+    uint64_t cell;
+    int pol;
+    float amp;
+};
+
+// Scoped device selection that restores the caller's current device.
+struct DeviceGuard
+{
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+size_t storageBytes(int storage)
+{
+    switch (storage)
+    {
+    case TLM_STORE_F64: return 8;
+    case TLM_STORE_BF16:
+    case TLM_STORE_F16: return 2;
+    default: return 4;
+    }
+}
+size_t realBytes(int storage) { return storage == TLM_STORE_F64 ? 8 : 4; }
+int vecWidth(int storage) { return storage == TLM_STORE_F64 ? 2 : 4; }
+
+float pow2Ceil(float v)
+{
+    if (!(v > 0.0f) || !std::isfinite(v)) return 1.0f;
+    int e = 0;
+    std::frexp(v, &e);
+    return std::ldexp(1.0f, e);
+}
+
+} // namespace
+
+struct tlm_solver
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    std::atomic<bool> running{ false };
+    std::atomic<bool> finished{ false };
+    std::atomic<bool> stopFlag{ false };
+    std::atomic<int> doneStep{ 0 };
+    std::atomic<float> energy{ 0.0f };
+
+    // configuration
+    bool configured = false;
+    tlm_grid g{};
+    tlm_config cfg{};
+    int storage = TLM_STORE_F32;
+    std::vector<uint8_t> mat;
+    std::vector<float> epsr, sigma;
+    std::vector<float> yhat32, ghat32;
+    std::vector<double> yhat64, ghat64;
+    int nx = 0, ny = 0, nz = 0, px = 0, V = 4, nq = 0;
+    long long P = 0, ncell = 0, nquads = 0;
+    int nblocks = 0;
+    bool anyDiel = false;
+    float dt32 = 0.0f;
+    double dt64 = 0.0;
+    float scale = 1.0f;
+    int window = 64;
+
+    // sources and monitors
+    std::vector<SourceInfo> sources;
+    std::vector<PortInfo> ports;
+    std::vector<uint64_t> probeCells;
+    std::vector<float> svTable;
+    std::vector<double> dftFreqs;
+    bool prepared = false;
+    int nsamp = 0;
+
+    // time-loop state
+    int curStep = 0;       // steps enqueued
+    int curBuf = 0;        // pulse buffer holding the current state
+    bool stateIncident = false;
+
+    // device memory
+    void *dPulses[2] = { nullptr, nullptr };
+    void *dStub = nullptr;
+    uint8_t *dMat = nullptr;
+    void *dYhat = nullptr, *dGhat = nullptr;
+    SpecEntry *dSpec = nullptr;
+    int *dTile = nullptr;
+    void *dSamples = nullptr;
+    double *dEpart = nullptr;
+    int *dPortOff = nullptr, *dPortSlots = nullptr, *dPortPol = nullptr, *dPortNb = nullptr;
+    int *dProbeSlot = nullptr;
+    double *dVrec = nullptr, *dIrec = nullptr, *dPrec = nullptr;
+    long long recCap = 0;
+    double *dEhist = nullptr;
+    double *dElatest = nullptr;
+    double *dWdt = nullptr, *dDft = nullptr;
+    unsigned *dFault = nullptr;
+    size_t devBytes = 0;
+
+    // kernel timing
+    bool timing = false;
+    std::vector<cudaEvent_t> evs;
+    size_t evUsed = 0;
+
+    tlm_status fail(tlm_status s, const std::string &m)
+    {
+        err = m;
+        return s;
+    }
+    tlm_status cuda(cudaError_t e, const char *what)
+    {
+        if (e == cudaSuccess) return TLM_OK;
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? TLM_ENOMEM : TLM_ECUDA;
+    }
+};
+
+#define TLM_TRY(expr)                                  \
+    do                                                 \
+    {                                                  \
+        tlm_status _s = (expr);                        \
+        if (_s != TLM_OK) return _s;                   \
+    } while (0)
+#define TLM_CU(h, call) TLM_TRY((h)->cuda((call), #call))
+
+namespace {
+
+template <class T> tlm_status devAlloc(tlm_solver *h, T **p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) return TLM_OK;
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        return h->fail(TLM_ENOMEM, "cudaMalloc of " + std::to_string(bytes) +
+                                       " bytes failed: " + cudaGetErrorString(e));
+    }
+    h->devBytes += bytes;
+    *p = static_cast<T *>(q);
+    return TLM_OK;
+}
+// Short-lived buffers of one API call (not counted in the handle's bytes).
+template <class T> tlm_status tmpAlloc(tlm_solver *h, T **p, size_t bytes)
+{
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes > 0 ? bytes : 1);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        *p = nullptr;
+        return h->fail(TLM_ENOMEM, std::string("temporary cudaMalloc failed: ") + cudaGetErrorString(e));
+    }
+    *p = static_cast<T *>(q);
+    return TLM_OK;
+}
+template <class T> void devFree(tlm_solver *h, T *&p)
+{
+    (void)h;
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+void freeMonitors(tlm_solver *h)
+{
+    devFree(h, h->dSpec);
+    devFree(h, h->dTile);
+    devFree(h, h->dSamples);
+    devFree(h, h->dEpart);
+    devFree(h, h->dPortOff);
+    devFree(h, h->dPortSlots);
+    devFree(h, h->dPortPol);
+    devFree(h, h->dPortNb);
+    devFree(h, h->dProbeSlot);
+    devFree(h, h->dVrec);
+    devFree(h, h->dIrec);
+    devFree(h, h->dPrec);
+    devFree(h, h->dEhist);
+    devFree(h, h->dWdt);
+    devFree(h, h->dDft);
+    h->recCap = 0;
+    h->prepared = false;
+}
+
+void freeAll(tlm_solver *h)
+{
+    freeMonitors(h);
+    devFree(h, h->dPulses[0]);
+    devFree(h, h->dPulses[1]);
+    devFree(h, h->dStub);
+    devFree(h, h->dMat);
+    devFree(h, h->dYhat);
+    devFree(h, h->dGhat);
+    h->devBytes = 0;
+}
+
+bool busy(tlm_solver *h) { return h->running.load(); }
+
+// ---- source values ----------------------------------------------------
+double sourceValue(const tlm_solver *h, int n)
+{
+    if (h->cfg.waveform == TLM_WAVE_TABLE)
+        return (n >= 0 && n < (int)h->svTable.size()) ? (double)h->svTable[n] : 0.0;
+    if (h->storage == TLM_STORE_F64)
+        return tlmh::waveform_f64(h->cfg.waveform, h->cfg.f0, h->dt64, n);
+    return (double)tlmh::waveform_f32(h->cfg.waveform, h->cfg.f0, h->dt32, n);
+}
+
+// Padded node index of a reference linear cell index.
+long long paddedNode(const tlm_solver *h, uint64_t cell)
+{
+    const long long i = (long long)(cell % (uint64_t)h->nx);
+    const long long r = (long long)(cell / (uint64_t)h->nx);
+    return r * h->px + i;
+}
+
+// Build the device tables of sources and monitors once, before the first
+// step: the node-sorted entry list, per-block ranges, sample slots, port
+// and probe descriptors, records and DFT accumulators.
+tlm_status prepare(tlm_solver *h)
+{
+    if (h->prepared) return TLM_OK;
+    freeMonitors(h);
+    // unique monitored nodes -> sample slots
+    std::vector<long long> monNodes;
+    for (uint64_t c : h->probeCells) monNodes.push_back(paddedNode(h, c));
+    for (const PortInfo &p : h->ports)
+    {
+        for (uint64_t c : p.cells) monNodes.push_back(paddedNode(h, c));
+        if (!p.cells.empty())
+            for (int t = 0; t < 4; ++t) monNodes.push_back(paddedNode(h, (uint64_t)p.nb[t]));
+    }
+    std::sort(monNodes.begin(), monNodes.end());
+    monNodes.erase(std::unique(monNodes.begin(), monNodes.end()), monNodes.end());
+    h->nsamp = (int)monNodes.size();
+    auto slotOf = [&](uint64_t cell) {
+        long long nd = paddedNode(h, cell);
+        return (int)(std::lower_bound(monNodes.begin(), monNodes.end(), nd) - monNodes.begin());
+    };
+
+    // entries: plane-wave sources, then port cells (the reference's injection
+    // order), then one sample per monitored node; stable-sorted by node.
+    std::vector<SpecEntry> ents;
+    for (const SourceInfo &s : h->sources)
+        ents.push_back({ paddedNode(h, s.cell), tlmk::kInject, s.pol, s.amp, 0 });
+    for (const PortInfo &p : h->ports)
+        for (uint64_t c : p.cells) ents.push_back({ paddedNode(h, c), tlmk::kInject, p.pol, p.amp, 0 });
+    for (int sidx = 0; sidx < h->nsamp; ++sidx)
+        ents.push_back({ monNodes[sidx], tlmk::kSample, sidx, 0.0f, 0 });
+    std::stable_sort(ents.begin(), ents.end(),
+                     [](const SpecEntry &a, const SpecEntry &b) { return a.node < b.node; });
+    std::vector<int> tile(h->nblocks + 1, 0);
+    {
+        size_t e = 0;
+        const long long perBlock = (long long)kBlock * h->V;
+        for (int b = 0; b <= h->nblocks; ++b)
+        {
+            const long long start = (long long)b * perBlock;
+            while (e < ents.size() && ents[e].node < start) ++e;
+            tile[b] = (int)e;
+        }
+    }
+    if (!ents.empty())
+    {
+        TLM_TRY(devAlloc(h, &h->dSpec, ents.size() * sizeof(SpecEntry)));
+        TLM_CU(h, cudaMemcpyAsync(h->dSpec, ents.data(), ents.size() * sizeof(SpecEntry),
+                                  cudaMemcpyHostToDevice, h->stream));
+        TLM_TRY(devAlloc(h, &h->dTile, tile.size() * sizeof(int)));
+        TLM_CU(h, cudaMemcpyAsync(h->dTile, tile.data(), tile.size() * sizeof(int),
+                                  cudaMemcpyHostToDevice, h->stream));
+    }
+    const size_t rb = realBytes(h->storage);
+    TLM_TRY(devAlloc(h, &h->dSamples, (size_t)h->window * std::max(h->nsamp, 1) * 6 * rb));
+    TLM_TRY(devAlloc(h, &h->dEpart, (size_t)(h->window / 16 + 1) * h->nblocks * sizeof(double)));
+
+    // port / probe descriptors
+    const int np = (int)h->ports.size();
+    std::vector<int> off(np + 1, 0), slots, pol(np), nb(np * 4, -1);
+    for (int p = 0; p < np; ++p)
+    {
+        const PortInfo &pi = h->ports[p];
+        for (uint64_t c : pi.cells) slots.push_back(slotOf(c));
+        off[p + 1] = (int)slots.size();
+        pol[p] = pi.pol;
+        if (!pi.cells.empty())
+            for (int t = 0; t < 4; ++t) nb[p * 4 + t] = slotOf((uint64_t)pi.nb[t]);
+    }
+    std::vector<int> pslot;
+    for (uint64_t c : h->probeCells) pslot.push_back(slotOf(c));
+    if (slots.empty()) slots.push_back(0);
+    if (pslot.empty()) pslot.push_back(0);
+    if (np == 0)
+    {
+        pol.push_back(0);
+        nb.assign(4, -1);
+    }
+    TLM_TRY(devAlloc(h, &h->dPortOff, off.size() * sizeof(int)));
+    TLM_TRY(devAlloc(h, &h->dPortSlots, slots.size() * sizeof(int)));
+    TLM_TRY(devAlloc(h, &h->dPortPol, pol.size() * sizeof(int)));
+    TLM_TRY(devAlloc(h, &h->dPortNb, nb.size() * sizeof(int)));
+    TLM_TRY(devAlloc(h, &h->dProbeSlot, pslot.size() * sizeof(int)));
+    TLM_CU(h, cudaMemcpyAsync(h->dPortOff, off.data(), off.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, h->stream));
+    TLM_CU(h, cudaMemcpyAsync(h->dPortSlots, slots.data(), slots.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, h->stream));
+    TLM_CU(h, cudaMemcpyAsync(h->dPortPol, pol.data(), pol.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, h->stream));
+    TLM_CU(h, cudaMemcpyAsync(h->dPortNb, nb.data(), nb.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, h->stream));
+    TLM_CU(h, cudaMemcpyAsync(h->dProbeSlot, pslot.data(), pslot.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, h->stream));
+    // DFT
+    const int nf = (int)h->dftFreqs.size();
+    if (nf > 0 && np > 0)
+    {
+        std::vector<double> wdt(nf);
+        const double dt = h->storage == TLM_STORE_F64 ? h->dt64 : (double)h->dt32;
+        for (int f = 0; f < nf; ++f) wdt[f] = 2.0 * 3.14159265358979323846 * h->dftFreqs[f] * dt;
+        TLM_TRY(devAlloc(h, &h->dWdt, nf * sizeof(double)));
+        TLM_CU(h, cudaMemcpyAsync(h->dWdt, wdt.data(), nf * sizeof(double), cudaMemcpyHostToDevice,
+                                  h->stream));
+        TLM_TRY(devAlloc(h, &h->dDft, (size_t)np * nf * 4 * sizeof(double)));
+        TLM_CU(h, cudaMemsetAsync(h->dDft, 0, (size_t)np * nf * 4 * sizeof(double), h->stream));
+    }
+    h->prepared = true;
+    return TLM_OK;
+}
+
+// Grow the step-major record arrays to hold `need` steps.
+tlm_status ensureRecords(tlm_solver *h, long long need)
+{
+    if (need <= h->recCap) return TLM_OK;
+    long long cap = std::max<long long>(need, std::max<long long>(h->cfg.total_steps, 64));
+    cap = std::max(cap, h->recCap * 2);
+    const int np = std::max<int>((int)h->ports.size(), 1);
+    const int nr = std::max<int>((int)h->probeCells.size(), 1);
+    double *v = nullptr, *i = nullptr, *p = nullptr, *e = nullptr;
+    TLM_TRY(devAlloc(h, &v, (size_t)cap * np * sizeof(double)));
+    TLM_TRY(devAlloc(h, &i, (size_t)cap * np * sizeof(double)));
+    TLM_TRY(devAlloc(h, &p, (size_t)cap * nr * 3 * sizeof(double)));
+    TLM_TRY(devAlloc(h, &e, (size_t)(cap / 16 + 2) * sizeof(double)));
+    if (h->recCap > 0)
+    {
+        TLM_CU(h, cudaMemcpyAsync(v, h->dVrec, (size_t)h->recCap * np * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, h->stream));
+        TLM_CU(h, cudaMemcpyAsync(i, h->dIrec, (size_t)h->recCap * np * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, h->stream));
+        TLM_CU(h, cudaMemcpyAsync(p, h->dPrec, (size_t)h->recCap * nr * 3 * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, h->stream));
+        TLM_CU(h, cudaMemcpyAsync(e, h->dEhist, (size_t)(h->recCap / 16 + 2) * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, h->stream));
+        TLM_CU(h, cudaStreamSynchronize(h->stream));
+        devFree(h, h->dVrec);
+        devFree(h, h->dIrec);
+        devFree(h, h->dPrec);
+        devFree(h, h->dEhist);
+    }
+    h->dVrec = v;
+    h->dIrec = i;
+    h->dPrec = p;
+    h->dEhist = e;
+    h->recCap = cap;
+    return TLM_OK;
+}
+
+template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long eFirst)
+{
+    using R = typename tlmk::Traits<S>::R;
+    tlmk::StepArgs<S> a;
+    a.in = static_cast<const S *>(h->dPulses[h->curBuf]);
+    a.out = static_cast<S *>(h->dPulses[h->curBuf ^ 1]);
+    a.stub = static_cast<R *>(h->dStub);
+    a.mat = h->dMat;
+    a.yhat = static_cast<const R *>(h->dYhat);
+    a.ghat = static_cast<const R *>(h->dGhat);
+    a.P = h->P;
+    a.nquads = h->nquads;
+    a.nx = h->nx;
+    a.ny = h->ny;
+    a.nz = h->nz;
+    a.px = h->px;
+    a.nq = h->nq;
+    a.rho = (R)h->cfg.boundary_rho;
+    a.scale = (R)h->scale;
+    a.inv_scale = (R)(1.0f / h->scale);
+    a.tile_begin = h->dTile;
+    a.spec = h->dSpec;
+    a.sv = (R)sourceValue(h, n);
+    a.samples = static_cast<R *>(h->dSamples) + (size_t)i * h->nsamp * 6;
+    a.epart = (n % 16 == 0) ? h->dEpart + (size_t)((n - eFirst) / 16) * h->nblocks : nullptr;
+    a.fault = h->dFault;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (h->timing)
+    {
+        while (h->evs.size() < h->evUsed + 2)
+        {
+            cudaEvent_t ev;
+            TLM_CU(h, cudaEventCreate(&ev));
+            h->evs.push_back(ev);
+        }
+        e0 = h->evs[h->evUsed];
+        e1 = h->evs[h->evUsed + 1];
+        h->evUsed += 2;
+        TLM_CU(h, cudaEventRecord(e0, h->stream));
+    }
+    if (h->stateIncident)
+        tlmk::stepKernel<S, true><<<h->nblocks, kBlock, 0, h->stream>>>(a);
+    else
+        tlmk::stepKernel<S, false><<<h->nblocks, kBlock, 0, h->stream>>>(a);
+    TLM_CU(h, cudaGetLastError());
+    if (h->timing) TLM_CU(h, cudaEventRecord(e1, h->stream));
+    h->stateIncident = false;
+    h->curBuf ^= 1;
+    return TLM_OK;
+}
+
+template <class R> tlm_status launchEpilogue(tlm_solver *h, long long base, int w, long long eFirst,
+                                             int nE)
+{
+    tlmk::EpilogueArgs<R> a;
+    a.samples = static_cast<const R *>(h->dSamples);
+    a.nsamp = h->nsamp;
+    a.w = w;
+    a.base = base;
+    a.nports = (int)h->ports.size();
+    a.port_off = h->dPortOff;
+    a.port_slots = h->dPortSlots;
+    a.port_pol = h->dPortPol;
+    a.port_nb = h->dPortNb;
+    a.nprobes = (int)h->probeCells.size();
+    a.probe_slot = h->dProbeSlot;
+    a.probe_scale = h->storage == TLM_STORE_F64 ? (R)tlmh::probe_scale_f64(h->g.dl)
+                                                : (R)tlmh::probe_scale_f32(h->g.dl);
+    a.eta0 = (R)tlmh::eta0_f32();
+    a.vrec = h->dVrec;
+    a.irec = h->dIrec;
+    a.prec = h->dPrec;
+    a.nfreq = h->dDft ? (int)h->dftFreqs.size() : 0;
+    a.wdt = h->dWdt;
+    a.dft = h->dDft;
+    a.epart = h->dEpart;
+    a.nblocks = h->nblocks;
+    a.n_e = nE;
+    a.e_first = eFirst;
+    a.ehist = h->dEhist;
+    a.elatest = h->dElatest;
+    tlmk::windowEpilogue<R><<<1, 512, 0, h->stream>>>(a);
+    return h->cuda(cudaGetLastError(), "windowEpilogue launch");
+}
+
+// Enqueue n steps in windows of h->window; optionally stop early.
+tlm_status enqueueSteps(tlm_solver *h, int nsteps, bool honourStop, bool *stopped)
+{
+    if (stopped) *stopped = false;
+    TLM_TRY(prepare(h));
+    int remaining = nsteps;
+    while (remaining > 0)
+    {
+        if (honourStop && h->stopFlag.load())
+        {
+            if (stopped) *stopped = true;
+            break;
+        }
+        const int w = std::min(remaining, h->window);
+        const long long base = h->curStep;
+        TLM_TRY(ensureRecords(h, base + w));
+        const long long eFirst = (base + 15) / 16 * 16;
+        const int nE = eFirst < base + w ? (int)((base + w - 1 - eFirst) / 16 + 1) : 0;
+        for (int i = 0; i < w; ++i)
+        {
+            const int n = (int)(base + i);
+            switch (h->storage)
+            {
+            case TLM_STORE_F64: TLM_TRY(launchStep<double>(h, n, i, eFirst)); break;
+            case TLM_STORE_BF16: TLM_TRY(launchStep<__nv_bfloat16>(h, n, i, eFirst)); break;
+            case TLM_STORE_F16: TLM_TRY(launchStep<__half>(h, n, i, eFirst)); break;
+            default: TLM_TRY(launchStep<float>(h, n, i, eFirst)); break;
+            }
+        }
+        if (h->storage == TLM_STORE_F64)
+            TLM_TRY(launchEpilogue<double>(h, base, w, eFirst, nE));
+        else
+            TLM_TRY(launchEpilogue<float>(h, base, w, eFirst, nE));
+        h->curStep += w;
+        remaining -= w;
+        if (honourStop)
+        {
+            // keep at most one window in flight so that a stop request or a
+            // progress poll sees the device's actual position
+            TLM_CU(h, cudaStreamSynchronize(h->stream));
+            h->doneStep.store(h->curStep);
+            double e = 0.0;
+            TLM_CU(h, cudaMemcpy(&e, h->dElatest, sizeof(double), cudaMemcpyDeviceToHost));
+            h->energy.store((float)e);
+        }
+    }
+    return TLM_OK;
+}
+
+tlm_status syncState(tlm_solver *h)
+{
+    TLM_CU(h, cudaStreamSynchronize(h->stream));
+    if (h->dFault)
+    {
+        unsigned f = 0;
+        TLM_CU(h, cudaMemcpy(&f, h->dFault, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (f) return h->fail(TLM_ECUDA, "bounds check tripped, code mask " + std::to_string(f));
+    }
+    h->doneStep.store(h->curStep);
+    if (h->dElatest)
+    {
+        double e = 0.0;
+        TLM_CU(h, cudaMemcpy(&e, h->dElatest, sizeof(double), cudaMemcpyDeviceToHost));
+        h->energy.store((float)e);
+    }
+    return TLM_OK;
+}
+
+tlm_status checkHandle(tlm_solver *h)
+{
+    if (!h)
+    {
+        g_threadError = "null handle";
+        return TLM_EINVAL;
+    }
+    return TLM_OK;
+}
+
+tlm_status checkReady(tlm_solver *h)
+{
+    TLM_TRY(checkHandle(h));
+    if (!h->configured) return h->fail(TLM_ESTATE, "tlm_setup has not been called");
+    if (busy(h)) return h->fail(TLM_EBUSY, "the handle is running");
+    return TLM_OK;
+}
+
+tlm_status checkAddable(tlm_solver *h)
+{
+    TLM_TRY(checkReady(h));
+    if (h->curStep > 0)
+        return h->fail(TLM_ESTATE, "sources and monitors must be added before the first step");
+    h->prepared = false;
+    return TLM_OK;
+}
+
+int gridBlocksFor(long long n)
+{
+    long long b = (n + 255) / 256;
+    return (int)std::max<long long>(1, std::min<long long>(b, 148LL * 32));
+}
+
+template <class S, class O> static tlm_status pulsesToHost(tlm_solver *h, O *out, size_t cap)
+{
+    using R = typename tlmk::Traits<S>::R;
+    const size_t need = (size_t)h->ncell * 12;
+    if (cap < need) return h->fail(TLM_EINVAL, "output holds " + std::to_string(cap) +
+                                                   " values, the state has " + std::to_string(need));
+    O *d = nullptr;
+    TLM_TRY(tmpAlloc(h, &d, need * sizeof(O)));
+    const S *cur = static_cast<const S *>(h->dPulses[h->curBuf]);
+    if (h->stateIncident)  // state written by tlm_set_pulses: already incident
+        tlmk::planesToAos<S, O><<<gridBlocksFor(h->ncell), 256, 0, h->stream>>>(
+            cur, h->P, h->nx, h->ny, h->nz, h->px, (R)h->scale, d);
+    else
+        tlmk::incidentToAos<S, O><<<gridBlocksFor(h->ncell), 256, 0, h->stream>>>(
+            cur, h->dMat, h->P, h->nx, h->ny, h->nz, h->px, (R)h->cfg.boundary_rho, (R)h->scale, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, need * sizeof(O), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    return h->cuda(e, "incident state export");
+}
+
+template <class O> static tlm_status getPulsesImpl(tlm_solver *h, O *out, size_t cap)
+{
+    TLM_TRY(checkReady(h));
+    if (!out) return h->fail(TLM_EINVAL, "null output");
+    DeviceGuard dg(h->device);
+    TLM_TRY(syncState(h));
+    switch (h->storage)
+    {
+    case TLM_STORE_F64: return pulsesToHost<double, O>(h, out, cap);
+    case TLM_STORE_BF16: return pulsesToHost<__nv_bfloat16, O>(h, out, cap);
+    case TLM_STORE_F16: return pulsesToHost<__half, O>(h, out, cap);
+    default: return pulsesToHost<float, O>(h, out, cap);
+    }
+}
+
+template <class S> static tlm_status setPulsesT(tlm_solver *h, const float *in)
+{
+    using R = typename tlmk::Traits<S>::R;
+    const size_t need = (size_t)h->ncell * 12;
+    float *d = nullptr;
+    TLM_TRY(tmpAlloc(h, &d, need * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(d, in, need * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+    {
+        tlmk::aosToIncident<S, float><<<gridBlocksFor(h->P), 256, 0, h->stream>>>(
+            d, h->dMat, h->P, h->nx, h->ny, h->nz, h->px, (R)(1.0f / h->scale),
+            static_cast<S *>(h->dPulses[h->curBuf]));
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    TLM_CU(h, e);
+    h->stateIncident = true;
+    return TLM_OK;
+}
+
+} // namespace
+
+// ======================================================================
+extern "C" {
+
+const char *tlm_version(void) { return kVersion; }
+
+void tlm_config_default(tlm_config *c)
+{
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->f0 = 1e9f;
+    c->waveform = TLM_WAVE_CW_RAMPED;
+    c->total_steps = 2000;
+    c->settle_steps = 600;
+    c->boundary_rho = 0.0f;
+    c->huy_offset = 0;
+    c->use_gpu = 1;
+    c->record_every = 0;
+    c->storage = TLM_STORE_F32;
+    c->pulse_scale = 0.0f;
+    c->steps_per_launch = 0;
+}
+
+tlm_status tlm_create(tlm_handle *out, int device)
+{
+    if (!out)
+    {
+        g_threadError = "null output pointer";
+        return TLM_EINVAL;
+    }
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+    {
+        cudaGetLastError();
+        g_threadError = std::string("no CUDA device: ") +
+                        (e != cudaSuccess ? cudaGetErrorString(e) : "device count is 0");
+        return TLM_ENODEV;
+    }
+    if (device < 0 || device >= count)
+    {
+        g_threadError = "device index out of range";
+        return TLM_EINVAL;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10)
+    {
+        cudaGetLastError();
+        g_threadError = "the kernels are built for sm_100a; device " + std::to_string(device) +
+                        " is sm_" + std::to_string(prop.major) + std::to_string(prop.minor);
+        return TLM_ENODEV;
+    }
+    tlm_solver *h = new tlm_solver();
+    h->device = device;
+    DeviceGuard dg(device);
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess)
+    {
+        g_threadError = std::string("cudaStreamCreate: ") + cudaGetErrorString(e);
+        delete h;
+        return TLM_ECUDA;
+    }
+    e = cudaMalloc(&h->dElatest, sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(h->dElatest, 0, sizeof(double));
+#ifdef TLM_CHECKED
+    if (e == cudaSuccess) e = cudaMalloc(&h->dFault, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(h->dFault, 0, sizeof(unsigned));
+#endif
+    if (e != cudaSuccess)
+    {
+        g_threadError = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        cudaStreamDestroy(h->stream);
+        delete h;
+        return TLM_ENOMEM;
+    }
+    *out = h;
+    return TLM_OK;
+}
+
+tlm_status tlm_destroy(tlm_handle h)
+{
+    if (!h) return TLM_OK;
+    if (busy(h)) return h->fail(TLM_EBUSY, "cannot destroy a running handle");
+    DeviceGuard dg(h->device);
+    cudaStreamSynchronize(h->stream);
+    freeAll(h);
+    if (h->dElatest) cudaFree(h->dElatest);
+    if (h->dFault) cudaFree(h->dFault);
+    for (cudaEvent_t ev : h->evs) cudaEventDestroy(ev);
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return TLM_OK;
+}
+
+const char *tlm_last_error(tlm_handle h)
+{
+    if (!h) return g_threadError.c_str();
+    return h->err.c_str();
+}
+
+tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, size_t n_cells,
+                     const tlm_matprops *table, int n_table, const tlm_config *cfg)
+{
+    TLM_TRY(checkHandle(h));
+    if (busy(h)) return h->fail(TLM_EBUSY, "the handle is running");
+    if (!grid || !mat || !cfg) return h->fail(TLM_EINVAL, "null grid, material map or config");
+    if (grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0)
+        return h->fail(TLM_EINVAL, "grid dimensions must be positive");
+    if (!(grid->dl > 0.0f) || !std::isfinite(grid->dl))
+        return h->fail(TLM_EINVAL, "cell size dl must be positive and finite");
+    const long long n = (long long)grid->nx * grid->ny * grid->nz;
+    if ((long long)n_cells != n)
+        return h->fail(TLM_EINVAL, "material map has " + std::to_string(n_cells) +
+                                       " cells, the grid has " + std::to_string(n));
+    if (n_table < 0 || n_table > 254 || (n_table > 0 && !table))
+        return h->fail(TLM_EINVAL, "material table must have 0..254 entries");
+    if (cfg->storage < TLM_STORE_F32 || cfg->storage > TLM_STORE_F64)
+        return h->fail(TLM_EINVAL, "unknown pulse storage mode");
+    if (cfg->waveform < 0 || cfg->waveform > TLM_WAVE_TABLE)
+        return h->fail(TLM_EINVAL, "unknown waveform");
+    if (cfg->total_steps < 0) return h->fail(TLM_EINVAL, "total_steps must be >= 0");
+    if (!std::isfinite(cfg->boundary_rho)) return h->fail(TLM_EINVAL, "boundary_rho not finite");
+    bool anyDiel = false;
+    for (long long c = 0; c < n; ++c)
+    {
+        if (mat[c] >= TLM_MAT_DIEL0)
+        {
+            anyDiel = true;
+            if (mat[c] - TLM_MAT_DIEL0 >= n_table)
+                return h->fail(TLM_EINVAL, "material id " + std::to_string(mat[c]) + " at cell " +
+                                               std::to_string(c) + " has no table entry");
+        }
+    }
+    DeviceGuard dg(h->device);
+    cudaStreamSynchronize(h->stream);
+    freeAll(h);
+    h->configured = false;
+
+    h->g = *grid;
+    h->cfg = *cfg;
+    h->storage = cfg->storage;
+    h->window = cfg->steps_per_launch > 0 ? std::min(cfg->steps_per_launch, 4096) : 64;
+    h->nx = grid->nx;
+    h->ny = grid->ny;
+    h->nz = grid->nz;
+    h->V = vecWidth(h->storage);
+    h->px = (h->nx + kPadX - 1) / kPadX * kPadX;
+    h->nq = h->px / h->V;
+    h->P = (long long)h->px * h->ny * h->nz;
+    h->ncell = n;
+    h->nquads = (long long)h->nq * h->ny * h->nz;
+    const long long nb = (h->nquads + kBlock - 1) / kBlock;
+    if (nb > 0x7fffffffLL) return h->fail(TLM_EINVAL, "grid too large");
+    h->nblocks = (int)nb;
+    h->anyDiel = anyDiel;
+    h->mat.assign(mat, mat + n);
+    h->epsr.resize(n_table);
+    h->sigma.resize(n_table);
+    for (int t = 0; t < n_table; ++t)
+    {
+        h->epsr[t] = table[t].epsr;
+        h->sigma[t] = table[t].sigma;
+    }
+    h->yhat32.assign(std::max(n_table, 1), 0.0f);
+    h->ghat32.assign(std::max(n_table, 1), 0.0f);
+    h->yhat64.assign(std::max(n_table, 1), 0.0);
+    h->ghat64.assign(std::max(n_table, 1), 0.0);
+    tlmh::tables_f32(h->epsr.data(), h->sigma.data(), n_table, grid->dl, h->yhat32.data(),
+                     h->ghat32.data());
+    tlmh::tables_f64(h->epsr.data(), h->sigma.data(), n_table, grid->dl, h->yhat64.data(),
+                     h->ghat64.data());
+    h->dt32 = tlmh::timestep_f32(grid->dl);
+    h->dt64 = tlmh::timestep_f64(grid->dl);
+    h->sources.clear();
+    h->ports.clear();
+    h->probeCells.clear();
+    h->svTable.clear();
+    h->dftFreqs.clear();
+    h->curStep = 0;
+    h->curBuf = 0;
+    h->stateIncident = false;
+    h->doneStep.store(0);
+    h->energy.store(0.0f);
+    h->finished.store(false);
+    h->stopFlag.store(false);
+    h->evUsed = 0;
+    h->scale = 1.0f;
+
+    // HBM admission: refuse up front if the state would not fit.
+    const size_t sb = storageBytes(h->storage), rb = realBytes(h->storage);
+    const size_t need = 2 * 12 * (size_t)h->P * sb + (anyDiel ? 3 * (size_t)h->P * rb : 0) +
+                        (size_t)h->P + (size_t)h->nblocks * 8 * 8;
+    size_t freeB = 0, totalB = 0;
+    TLM_CU(h, cudaMemGetInfo(&freeB, &totalB));
+    if (need + (size_t)(256u << 20) > freeB)
+        return h->fail(TLM_ENOMEM, "grid needs " + std::to_string(need >> 20) + " MiB of HBM, " +
+                                       std::to_string(freeB >> 20) + " MiB free");
+
+    TLM_TRY(devAlloc(h, &h->dPulses[0], 12 * (size_t)h->P * sb));
+    TLM_TRY(devAlloc(h, &h->dPulses[1], 12 * (size_t)h->P * sb));
+    TLM_CU(h, cudaMemsetAsync(h->dPulses[0], 0, 12 * (size_t)h->P * sb, h->stream));
+    TLM_CU(h, cudaMemsetAsync(h->dPulses[1], 0, 12 * (size_t)h->P * sb, h->stream));
+    if (anyDiel)
+    {
+        TLM_TRY(devAlloc(h, &h->dStub, 3 * (size_t)h->P * rb));
+        TLM_CU(h, cudaMemsetAsync(h->dStub, 0, 3 * (size_t)h->P * rb, h->stream));
+    }
+    // padded material map: padding columns are PEC (never updated, zero)
+    {
+        std::vector<uint8_t> pm((size_t)h->P, (uint8_t)TLM_MAT_PEC);
+        for (long long r = 0; r < (long long)h->ny * h->nz; ++r)
+            std::memcpy(&pm[(size_t)r * h->px], &mat[(size_t)r * h->nx], h->nx);
+        TLM_TRY(devAlloc(h, &h->dMat, (size_t)h->P));
+        TLM_CU(h, cudaMemcpyAsync(h->dMat, pm.data(), (size_t)h->P, cudaMemcpyHostToDevice,
+                                  h->stream));
+        TLM_CU(h, cudaStreamSynchronize(h->stream));
+    }
+    TLM_TRY(devAlloc(h, &h->dYhat, h->yhat32.size() * rb));
+    TLM_TRY(devAlloc(h, &h->dGhat, h->ghat32.size() * rb));
+    if (h->storage == TLM_STORE_F64)
+    {
+        TLM_CU(h, cudaMemcpy(h->dYhat, h->yhat64.data(), h->yhat64.size() * 8, cudaMemcpyHostToDevice));
+        TLM_CU(h, cudaMemcpy(h->dGhat, h->ghat64.data(), h->ghat64.size() * 8, cudaMemcpyHostToDevice));
+    }
+    else
+    {
+        TLM_CU(h, cudaMemcpy(h->dYhat, h->yhat32.data(), h->yhat32.size() * 4, cudaMemcpyHostToDevice));
+        TLM_CU(h, cudaMemcpy(h->dGhat, h->ghat32.data(), h->ghat32.size() * 4, cudaMemcpyHostToDevice));
+    }
+    TLM_CU(h, cudaMemset(h->dElatest, 0, sizeof(double)));
+    h->configured = true;
+    return TLM_OK;
+}
+
+tlm_status tlm_add_port(tlm_handle h, const uint64_t *cells, int n_cells, int pol_axis, float amp,
+                        int *out_idx)
+{
+    TLM_TRY(checkAddable(h));
+    if (pol_axis < 0 || pol_axis > 2) return h->fail(TLM_EINVAL, "pol_axis must be 0, 1 or 2");
+    if (n_cells < 0 || (n_cells > 0 && !cells)) return h->fail(TLM_EINVAL, "bad cell list");
+    PortInfo p;
+    p.pol = pol_axis;
+    p.amp = amp;
+    for (int t = 0; t < n_cells; ++t)
+        if (cells[t] < (uint64_t)h->ncell && h->mat[cells[t]] == TLM_MAT_AIR) p.cells.push_back(cells[t]);
+    if (!p.cells.empty())
+    {
+        const long long stride[3] = { 1, h->nx, (long long)h->nx * h->ny };
+        const long long c = (long long)p.cells[p.cells.size() / 2];
+        const long long s1 = stride[(pol_axis + 1) % 3], s2 = stride[(pol_axis + 2) % 3];
+        const long long nb[4] = { c + s1, c - s1, c + s2, c - s2 };
+        for (int t = 0; t < 4; ++t)
+        {
+            if (nb[t] < 0 || nb[t] >= h->ncell)
+                return h->fail(TLM_EINVAL, "port current loop around cell " + std::to_string(c) +
+                                               " leaves the grid");
+            p.nb[t] = nb[t];
+        }
+    }
+    h->ports.push_back(p);
+    if (out_idx) *out_idx = (int)h->ports.size() - 1;
+    return TLM_OK;
+}
+
+tlm_status tlm_add_plane_wave(tlm_handle h, int prop_axis, int plane_index, int pol_axis, float amp)
+{
+    TLM_TRY(checkAddable(h));
+    if (prop_axis < 0 || prop_axis > 2 || pol_axis < 0 || pol_axis > 2)
+        return h->fail(TLM_EINVAL, "axes must be 0, 1 or 2");
+    for (int k = 0; k < h->nz; ++k)
+        for (int j = 0; j < h->ny; ++j)
+            for (int i = 0; i < h->nx; ++i)
+            {
+                const int co[3] = { i, j, k };
+                if (co[prop_axis] != plane_index) continue;
+                const uint64_t c = ((uint64_t)k * h->ny + j) * h->nx + i;
+                if (h->mat[c] == TLM_MAT_AIR) h->sources.push_back({ c, pol_axis, amp });
+            }
+    return TLM_OK;
+}
+
+tlm_status tlm_add_probe(tlm_handle h, float x, float y, float z, int *out_idx)
+{
+    TLM_TRY(checkAddable(h));
+    int i, j, k;
+    tlmh::cell_of(h->g.origin, h->g.dl, x, y, z, &i, &j, &k);
+    if (i < 0 || j < 0 || k < 0 || i >= h->nx || j >= h->ny || k >= h->nz)
+    {
+        if (out_idx) *out_idx = -1;
+        return TLM_OK;
+    }
+    h->probeCells.push_back(((uint64_t)k * h->ny + j) * h->nx + i);
+    if (out_idx) *out_idx = (int)h->probeCells.size() - 1;
+    return TLM_OK;
+}
+
+tlm_status tlm_add_probe_cell(tlm_handle h, int i, int j, int k, int *out_idx)
+{
+    TLM_TRY(checkAddable(h));
+    if (i < 0 || j < 0 || k < 0 || i >= h->nx || j >= h->ny || k >= h->nz)
+    {
+        if (out_idx) *out_idx = -1;
+        return TLM_OK;
+    }
+    h->probeCells.push_back(((uint64_t)k * h->ny + j) * h->nx + i);
+    if (out_idx) *out_idx = (int)h->probeCells.size() - 1;
+    return TLM_OK;
+}
+
+tlm_status tlm_set_source_table(tlm_handle h, const float *sv, int n_steps)
+{
+    TLM_TRY(checkReady(h));
+    if (n_steps < 0 || (n_steps > 0 && !sv)) return h->fail(TLM_EINVAL, "bad source table");
+    h->svTable.assign(sv, sv + n_steps);
+    return TLM_OK;
+}
+
+tlm_status tlm_set_port_dft(tlm_handle h, const double *freqs, int n_freq)
+{
+    TLM_TRY(checkAddable(h));
+    if (n_freq < 0 || n_freq > 4096 || (n_freq > 0 && !freqs))
+        return h->fail(TLM_EINVAL, "bad DFT frequency list");
+    h->dftFreqs.assign(freqs, freqs + n_freq);
+    return TLM_OK;
+}
+
+static tlm_status chooseScale(tlm_solver *h)
+{
+    if (h->storage != TLM_STORE_F16 && h->storage != TLM_STORE_BF16)
+    {
+        h->scale = 1.0f;
+        return TLM_OK;
+    }
+    if (h->cfg.pulse_scale > 0.0f)
+    {
+        h->scale = pow2Ceil(h->cfg.pulse_scale);
+        return TLM_OK;
+    }
+    // Largest single injection 0.5*|amp|*max|sv| bounds the pulse peak; store
+    // it near 2^10 so that FP16 keeps ~20 binades of headroom below it.
+    float amax = 0.0f;
+    for (const SourceInfo &s : h->sources) amax = std::max(amax, std::fabs(s.amp));
+    for (const PortInfo &p : h->ports)
+        if (!p.cells.empty()) amax = std::max(amax, std::fabs(p.amp) * (float)p.cells.size());
+    float svmax = 1.0f;
+    if (h->cfg.waveform == TLM_WAVE_TABLE)
+    {
+        svmax = 0.0f;
+        for (float v : h->svTable) svmax = std::max(svmax, std::fabs(v));
+    }
+    const float peak = std::max(0.5f * amax * svmax, 1e-30f);
+    h->scale = h->storage == TLM_STORE_F16 ? pow2Ceil(peak) / 1024.0f : 1.0f;
+    return TLM_OK;
+}
+
+tlm_status tlm_step_async(tlm_handle h, int n_steps)
+{
+    TLM_TRY(checkReady(h));
+    if (n_steps < 0) return h->fail(TLM_EINVAL, "n_steps must be >= 0");
+    DeviceGuard dg(h->device);
+    if (h->curStep == 0 && !h->prepared) TLM_TRY(chooseScale(h));
+    return enqueueSteps(h, n_steps, false, nullptr);
+}
+
+tlm_status tlm_sync(tlm_handle h)
+{
+    TLM_TRY(checkReady(h));
+    DeviceGuard dg(h->device);
+    return syncState(h);
+}
+
+tlm_status tlm_step(tlm_handle h, int n_steps)
+{
+    TLM_TRY(tlm_step_async(h, n_steps));
+    DeviceGuard dg(h->device);
+    return syncState(h);
+}
+
+tlm_status tlm_run(tlm_handle h)
+{
+    TLM_TRY(checkReady(h));
+    DeviceGuard dg(h->device);
+    bool expected = false;
+    if (!h->running.compare_exchange_strong(expected, true))
+        return h->fail(TLM_EBUSY, "already running");
+    h->finished.store(false);
+    tlm_status st = TLM_OK;
+    bool stopped = false;
+    if (h->curStep == 0 && !h->prepared) st = chooseScale(h);
+    const int todo = h->cfg.total_steps - h->curStep;
+    if (st == TLM_OK && todo > 0) st = enqueueSteps(h, todo, true, &stopped);
+    if (st == TLM_OK) st = syncState(h);
+    h->finished.store(true);
+    h->running.store(false);
+    if (st == TLM_OK && stopped) return h->fail(TLM_ESTOPPED, "stopped at step " + std::to_string(h->curStep));
+    return st;
+}
+
+tlm_status tlm_request_stop(tlm_handle h)
+{
+    if (!h) return TLM_EINVAL;
+    h->stopFlag.store(true);
+    return TLM_OK;
+}
+int tlm_current_step(tlm_handle h) { return h ? h->doneStep.load() : -1; }
+float tlm_current_energy(tlm_handle h) { return h ? h->energy.load() : 0.0f; }
+int tlm_is_running(tlm_handle h) { return h ? (int)h->running.load() : 0; }
+int tlm_is_finished(tlm_handle h) { return h ? (int)h->finished.load() : 0; }
+int tlm_total_steps(tlm_handle h) { return h ? h->cfg.total_steps : 0; }
+
+tlm_status tlm_timestep(tlm_handle h, float *dt)
+{
+    TLM_TRY(checkHandle(h));
+    if (!h->configured) return h->fail(TLM_ESTATE, "tlm_setup has not been called");
+    if (dt) *dt = h->dt32;
+    return TLM_OK;
+}
+
+int tlm_probe_count(tlm_handle h) { return h ? (int)h->probeCells.size() : 0; }
+int tlm_port_count(tlm_handle h) { return h ? (int)h->ports.size() : 0; }
+
+static tlm_status getProbeImpl(tlm_solver *h, int idx, double *ex, double *ey, double *ez, float *fx,
+                               float *fy, float *fz, int cap, int *n_out)
+{
+    TLM_TRY(checkReady(h));
+    if (idx < 0 || idx >= (int)h->probeCells.size()) return h->fail(TLM_EINVAL, "probe index out of range");
+    DeviceGuard dg(h->device);
+    TLM_TRY(syncState(h));
+    const int nr = (int)h->probeCells.size();
+    const int steps = h->curStep;
+    const int n = std::min(steps, cap);
+    if (n_out) *n_out = steps;
+    if (n <= 0) return TLM_OK;
+    std::vector<double> buf((size_t)n * nr * 3);
+    TLM_CU(h, cudaMemcpy(buf.data(), h->dPrec, buf.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < n; ++t)
+    {
+        const double *d = &buf[((size_t)t * nr + idx) * 3];
+        if (ex) ex[t] = d[0];
+        if (ey) ey[t] = d[1];
+        if (ez) ez[t] = d[2];
+        if (fx) fx[t] = (float)d[0];
+        if (fy) fy[t] = (float)d[1];
+        if (fz) fz[t] = (float)d[2];
+    }
+    return TLM_OK;
+}
+
+tlm_status tlm_get_probe(tlm_handle h, int idx, float *ex, float *ey, float *ez, int cap, int *n_out)
+{
+    return getProbeImpl(h, idx, nullptr, nullptr, nullptr, ex, ey, ez, cap, n_out);
+}
+tlm_status tlm_get_probe_f64(tlm_handle h, int idx, double *ex, double *ey, double *ez, int cap,
+                             int *n_out)
+{
+    return getProbeImpl(h, idx, ex, ey, ez, nullptr, nullptr, nullptr, cap, n_out);
+}
+tlm_status tlm_get_probe_cell(tlm_handle h, int idx, uint64_t *cell)
+{
+    TLM_TRY(checkHandle(h));
+    if (idx < 0 || idx >= (int)h->probeCells.size()) return h->fail(TLM_EINVAL, "probe index out of range");
+    if (cell) *cell = h->probeCells[idx];
+    return TLM_OK;
+}
+
+static tlm_status getPortImpl(tlm_solver *h, int idx, double *v, double *i, float *fv, float *fi,
+                              int cap, int *n_out)
+{
+    TLM_TRY(checkReady(h));
+    if (idx < 0 || idx >= (int)h->ports.size()) return h->fail(TLM_EINVAL, "port index out of range");
+    DeviceGuard dg(h->device);
+    TLM_TRY(syncState(h));
+    const int np = (int)h->ports.size();
+    const int steps = h->curStep;
+    const int n = std::min(steps, cap);
+    if (n_out) *n_out = steps;
+    if (n <= 0) return TLM_OK;
+    std::vector<double> bv((size_t)n * np), bi((size_t)n * np);
+    TLM_CU(h, cudaMemcpy(bv.data(), h->dVrec, bv.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    TLM_CU(h, cudaMemcpy(bi.data(), h->dIrec, bi.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < n; ++t)
+    {
+        const double a = bv[(size_t)t * np + idx], b = bi[(size_t)t * np + idx];
+        if (v) v[t] = a;
+        if (i) i[t] = b;
+        if (fv) fv[t] = (float)a;
+        if (fi) fi[t] = (float)b;
+    }
+    return TLM_OK;
+}
+
+tlm_status tlm_get_port(tlm_handle h, int idx, float *v, float *i, int cap, int *n_out)
+{
+    return getPortImpl(h, idx, nullptr, nullptr, v, i, cap, n_out);
+}
+tlm_status tlm_get_port_f64(tlm_handle h, int idx, double *v, double *i, int cap, int *n_out)
+{
+    return getPortImpl(h, idx, v, i, nullptr, nullptr, cap, n_out);
+}
+tlm_status tlm_get_port_cells(tlm_handle h, int idx, uint64_t *cells, int cap, int *n_out)
+{
+    TLM_TRY(checkHandle(h));
+    if (idx < 0 || idx >= (int)h->ports.size()) return h->fail(TLM_EINVAL, "port index out of range");
+    const auto &c = h->ports[idx].cells;
+    if (n_out) *n_out = (int)c.size();
+    for (int t = 0; cells && t < (int)c.size() && t < cap; ++t) cells[t] = c[t];
+    return TLM_OK;
+}
+
+tlm_status tlm_get_port_dft(tlm_handle h, int idx, double *v_re, double *v_im, double *i_re,
+                            double *i_im, int cap, int *n_out)
+{
+    TLM_TRY(checkReady(h));
+    if (idx < 0 || idx >= (int)h->ports.size()) return h->fail(TLM_EINVAL, "port index out of range");
+    const int nf = (int)h->dftFreqs.size();
+    if (n_out) *n_out = nf;
+    if (nf == 0) return TLM_OK;
+    DeviceGuard dg(h->device);
+    TLM_TRY(prepare(h));
+    TLM_TRY(syncState(h));
+    std::vector<double> buf((size_t)nf * 4);
+    TLM_CU(h, cudaMemcpy(buf.data(), h->dDft + (size_t)idx * nf * 4, buf.size() * sizeof(double),
+                         cudaMemcpyDeviceToHost));
+    for (int f = 0; f < nf && f < cap; ++f)
+    {
+        if (v_re) v_re[f] = buf[f * 4 + 0];
+        if (v_im) v_im[f] = buf[f * 4 + 1];
+        if (i_re) i_re[f] = buf[f * 4 + 2];
+        if (i_im) i_im[f] = buf[f * 4 + 3];
+    }
+    return TLM_OK;
+}
+
+tlm_status tlm_get_energy_history(tlm_handle h, int *steps, float *vals, double *vals64, int cap,
+                                  int *n_out)
+{
+    TLM_TRY(checkReady(h));
+    DeviceGuard dg(h->device);
+    TLM_TRY(syncState(h));
+    const int ne = h->curStep > 0 ? (h->curStep - 1) / 16 + 1 : 0;
+    if (n_out) *n_out = ne;
+    const int n = std::min(ne, cap);
+    if (n <= 0) return TLM_OK;
+    std::vector<double> buf(n);
+    TLM_CU(h, cudaMemcpy(buf.data(), h->dEhist, n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < n; ++t)
+    {
+        if (steps) steps[t] = 16 * t;
+        if (vals) vals[t] = (float)buf[t];
+        if (vals64) vals64[t] = buf[t];
+    }
+    return TLM_OK;
+}
+
+tlm_status tlm_get_pulses(tlm_handle h, float *out, size_t cap) { return getPulsesImpl(h, out, cap); }
+tlm_status tlm_get_pulses_f64(tlm_handle h, double *out, size_t cap) { return getPulsesImpl(h, out, cap); }
+
+tlm_status tlm_set_pulses(tlm_handle h, const float *in, size_t n)
+{
+    TLM_TRY(checkReady(h));
+    if (!in || n != (size_t)h->ncell * 12)
+        return h->fail(TLM_EINVAL, "pulse array must hold 12 values per cell");
+    DeviceGuard dg(h->device);
+    TLM_TRY(syncState(h));
+    switch (h->storage)
+    {
+    case TLM_STORE_F64: return setPulsesT<double>(h, in);
+    case TLM_STORE_BF16: return setPulsesT<__nv_bfloat16>(h, in);
+    case TLM_STORE_F16: return setPulsesT<__half>(h, in);
+    default: return setPulsesT<float>(h, in);
+    }
+}
+
+tlm_status tlm_get_stubs(tlm_handle h, float *out, size_t cap)
+{
+    TLM_TRY(checkReady(h));
+    if (!out) return h->fail(TLM_EINVAL, "null output");
+    const size_t need = (size_t)h->ncell * 3;
+    if (cap < need) return h->fail(TLM_EINVAL, "output too small for the stub state");
+    DeviceGuard dg(h->device);
+    TLM_TRY(syncState(h));
+    if (!h->dStub)
+    {
+        std::fill(out, out + need, 0.0f);
+        return TLM_OK;
+    }
+    float *d = nullptr;
+    TLM_TRY(tmpAlloc(h, &d, need * sizeof(float)));
+    if (h->storage == TLM_STORE_F64)
+        tlmk::stubsToAos<double, float><<<gridBlocksFor(h->ncell), 256, 0, h->stream>>>(
+            static_cast<const double *>(h->dStub), h->P, h->nx, h->ny, h->nz, h->px, d);
+    else
+        tlmk::stubsToAos<float, float><<<gridBlocksFor(h->ncell), 256, 0, h->stream>>>(
+            static_cast<const float *>(h->dStub), h->P, h->nx, h->ny, h->nz, h->px, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, need * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    return h->cuda(e, "stub export");
+}
+
+tlm_status tlm_get_materials(tlm_handle h, uint8_t *out, size_t cap)
+{
+    TLM_TRY(checkReady(h));
+    if (!out || cap < (size_t)h->ncell) return h->fail(TLM_EINVAL, "output too small");
+    DeviceGuard dg(h->device);
+    TLM_TRY(syncState(h));
+    std::vector<uint8_t> pm((size_t)h->P);
+    TLM_CU(h, cudaMemcpy(pm.data(), h->dMat, pm.size(), cudaMemcpyDeviceToHost));
+    for (long long r = 0; r < (long long)h->ny * h->nz; ++r)
+        std::memcpy(out + (size_t)r * h->nx, &pm[(size_t)r * h->px], h->nx);
+    return TLM_OK;
+}
+
+tlm_status tlm_get_tables(tlm_handle h, float *yhat, float *ghat, int cap, int *n_out)
+{
+    TLM_TRY(checkReady(h));
+    const int n = (int)h->epsr.size();
+    if (n_out) *n_out = n;
+    DeviceGuard dg(h->device);
+    if (h->storage == TLM_STORE_F64)
+    {
+        std::vector<double> y(std::max(n, 1)), gg(std::max(n, 1));
+        TLM_CU(h, cudaMemcpy(y.data(), h->dYhat, y.size() * 8, cudaMemcpyDeviceToHost));
+        TLM_CU(h, cudaMemcpy(gg.data(), h->dGhat, gg.size() * 8, cudaMemcpyDeviceToHost));
+        for (int t = 0; t < n && t < cap; ++t)
+        {
+            if (yhat) yhat[t] = (float)y[t];
+            if (ghat) ghat[t] = (float)gg[t];
+        }
+        return TLM_OK;
+    }
+    std::vector<float> y(std::max(n, 1)), gg(std::max(n, 1));
+    TLM_CU(h, cudaMemcpy(y.data(), h->dYhat, y.size() * 4, cudaMemcpyDeviceToHost));
+    TLM_CU(h, cudaMemcpy(gg.data(), h->dGhat, gg.size() * 4, cudaMemcpyDeviceToHost));
+    for (int t = 0; t < n && t < cap; ++t)
+    {
+        if (yhat) yhat[t] = y[t];
+        if (ghat) ghat[t] = gg[t];
+    }
+    return TLM_OK;
+}
+
+tlm_status tlm_waveform_value(int waveform, float f0, float dl, int n, float *out)
+{
+    if (!out || waveform < 0 || waveform > TLM_WAVE_GAUSSIAN_PULSE || !(dl > 0.0f))
+    {
+        g_threadError = "bad waveform arguments";
+        return TLM_EINVAL;
+    }
+    *out = tlmh::waveform_f32(waveform, f0, tlmh::timestep_f32(dl), n);
+    return TLM_OK;
+}
+
+static tlm_status unitarity(int device, float epsr, int stubs, float *err)
+{
+    if (!err)
+    {
+        g_threadError = "null output";
+        return TLM_EINVAL;
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+    {
+        cudaGetLastError();
+        g_threadError = "no such CUDA device";
+        return TLM_ENODEV;
+    }
+    DeviceGuard dg(device);
+    float *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(float));
+    if (e == cudaSuccess)
+    {
+        tlmk::unitarityKernel<<<1, 32>>>(epsr, stubs, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(err, d, sizeof(float), cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess)
+    {
+        g_threadError = std::string("unitarity kernel: ") + cudaGetErrorString(e);
+        return TLM_ECUDA;
+    }
+    return TLM_OK;
+}
+
+tlm_status tlm_scatter_unitarity_error(int device, float *err) { return unitarity(device, 1.0f, 0, err); }
+tlm_status tlm_stub_unitarity_error(int device, float epsr, float *err)
+{
+    return unitarity(device, epsr, 1, err);
+}
+
+tlm_status tlm_get_stream(tlm_handle h, void **stream)
+{
+    TLM_TRY(checkHandle(h));
+    if (stream) *stream = (void *)h->stream;
+    return TLM_OK;
+}
+
+tlm_status tlm_device_bytes(tlm_handle h, size_t *bytes)
+{
+    TLM_TRY(checkHandle(h));
+    if (bytes) *bytes = h->devBytes;
+    return TLM_OK;
+}
+
+tlm_status tlm_set_kernel_timing(tlm_handle h, int enable)
+{
+    TLM_TRY(checkHandle(h));
+    DeviceGuard dg(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->timing = enable != 0;
+    h->evUsed = 0;
+    return TLM_OK;
+}
+
+tlm_status tlm_kernel_time(tlm_handle h, double *ms, long long *launches)
+{
+    TLM_TRY(checkHandle(h));
+    DeviceGuard dg(h->device);
+    TLM_CU(h, cudaStreamSynchronize(h->stream));
+    double tot = 0.0;
+    for (size_t t = 0; t + 1 < h->evUsed; t += 2)
+    {
+        float m = 0.0f;
+        TLM_CU(h, cudaEventElapsedTime(&m, h->evs[t], h->evs[t + 1]));
+        tot += m;
+    }
+    if (ms) *ms = tot;
+    if (launches) *launches = (long long)(h->evUsed / 2);
+    return TLM_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,444 @@
+// tlm_step_kernel.cuh -- the fused SCN TLM time step (one launch per step).
+//
+// One thread owns V consecutive nodes along x (one aligned vector per plane).
+// Per step it:
+//   1. gathers the 12 incident pulses of its nodes from the reflected pulses
+//      of the previous step (connect, TlmSolver.cpp:551-613): x-neighbours
+//      come from the same vector or a lane shuffle, y/z neighbours from
+//      aligned vector loads one row / one plane away;
+//   2. adds the soft sources of its nodes (TlmSolver.cpp:487-505);
+//   3. records monitor samples (node voltages and circulations) for probes
+//      and ports (TlmSolver.cpp:677-713) and, every 16 steps, the block's
+//      FP64 share of the link energy (TlmSolver.cpp:766-789);
+//   4. scatters (air / stub-loaded, TlmSolver.cpp:59-113) and stores the
+//      reflected pulses at its own, aligned position.
+// DRAM traffic per node: 12 pulses read + 12 written + 1 material byte
+// (+ 3 stub pulses read and written on dielectric nodes).
+#pragma once
+
+#include "tlm_device.cuh"
+
+namespace tlmk {
+
+template <class S> struct StepArgs
+{
+    using R = typename Traits<S>::R;
+    const S *__restrict__ in;      // 12 planes, reflected pulses of step n-1
+    S *__restrict__ out;           // 12 planes, reflected pulses of step n
+    R *__restrict__ stub;          // 3 planes (nullptr without dielectrics)
+    const uint8_t *__restrict__ mat;
+    const R *__restrict__ yhat;
+    const R *__restrict__ ghat;
+    long long P;                   // plane stride (elements)
+    long long nquads;              // number of V-node groups
+    int nx, ny, nz, px, nq;        // nq = px / V
+    R rho;
+    R scale, inv_scale;            // pulse = stored * scale (BF16/F16)
+    // sources and monitors
+    const int *__restrict__ tile_begin;  // [gridDim.x + 1] ranges into spec
+    const SpecEntry *__restrict__ spec;
+    R sv;                          // source value of this step
+    R *__restrict__ samples;       // [nsamp][6] of this step
+    double *__restrict__ epart;    // [gridDim.x] energy partials (energy steps)
+    unsigned int *__restrict__ fault;  // bounds-check record (checked builds)
+};
+
+#ifdef TLM_CHECKED
+#define TLM_GUARD(idx, limit, code)                                                         \
+    (((idx) >= 0 && (idx) < (limit)) ? true : (atomicOr(a.fault, (unsigned)(code)), false))
+#else
+#define TLM_GUARD(idx, limit, code) true
+#endif
+
+template <class S, int V>
+__device__ __forceinline__ void loadPack(const S *__restrict__ base, long long idx,
+                                         typename Traits<S>::R (&dst)[V],
+                                         typename Traits<S>::R scale)
+{
+    const Pack<S, V> p = *reinterpret_cast<const Pack<S, V> *>(base + idx);
+#pragma unroll
+    for (int c = 0; c < V; ++c) dst[c] = decode(p.v[c], scale);
+}
+
+template <int V> __device__ __forceinline__ void loadMat(const uint8_t *__restrict__ m, long long idx,
+                                                         uint8_t (&dst)[V])
+{
+    const Pack<uint8_t, V> p = *reinterpret_cast<const Pack<uint8_t, V> *>(m + idx);
+#pragma unroll
+    for (int c = 0; c < V; ++c) dst[c] = p.v[c];
+}
+
+template <int V> __device__ __forceinline__ unsigned pecMask(const uint8_t (&m)[V])
+{
+    unsigned r = 0;
+#pragma unroll
+    for (int c = 0; c < V; ++c) r |= (m[c] == kPec ? 1u : 0u) << c;
+    return r;
+}
+
+// kIncident: the input planes hold INCIDENT pulses (state written by
+// tlm_set_pulses) instead of reflected ones; the gather is skipped.
+template <class S, bool kIncident>
+__global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
+{
+    using R = typename Traits<S>::R;
+    constexpr int V = Traits<S>::V;
+    __shared__ double red[kBlock / 32];
+
+    const int lane = threadIdx.x & 31;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    const bool live = q < a.nquads;
+    const long long qq = live ? q : 0;
+    const int xq = (int)(qq % a.nq);
+    const long long row = qq / a.nq;
+    const int j = (int)(row % a.ny);
+    const int k = (int)(row / a.ny);
+    const int x0 = xq * V;
+    const long long node0 = qq * V;
+    const long long P = a.P;
+    const long long sy = a.px, sz = (long long)a.px * a.ny;
+
+    uint8_t m[V];
+    if (live && TLM_GUARD(node0, P - V + 1, 1))
+        loadMat<V>(a.mat, node0, m);
+    else
+    {
+#pragma unroll
+        for (int c = 0; c < V; ++c) m[c] = kPec;
+    }
+
+    R inc[12][V];
+    unsigned nodeLive = 0;  // bit c: node x0+c is inside the grid and not PEC
+#pragma unroll
+    for (int c = 0; c < V; ++c)
+        nodeLive |= ((live && x0 + c < a.nx && m[c] != kPec) ? 1u : 0u) << c;
+
+    if (kIncident)
+    {
+#pragma unroll
+        for (int s = 0; s < 12; ++s)
+        {
+            if (live && TLM_GUARD(s * P + node0, 12 * P - V + 1, 2))
+                loadPack<S, V>(a.in, s * P + node0, inc[s], a.scale);
+            else
+            {
+#pragma unroll
+                for (int c = 0; c < V; ++c) inc[s][c] = R(0);
+            }
+        }
+    }
+    else
+    {
+        // ---- neighbour materials (PEC masks per direction) ----
+        uint8_t mn[V];
+        unsigned pecYm = 0, pecYp = 0, pecZm = 0, pecZp = 0;
+        if (live && j > 0 && TLM_GUARD(node0 - sy, P - V + 1, 3))
+        {
+            loadMat<V>(a.mat, node0 - sy, mn);
+            pecYm = pecMask<V>(mn);
+        }
+        if (live && j < a.ny - 1 && TLM_GUARD(node0 + sy, P - V + 1, 3))
+        {
+            loadMat<V>(a.mat, node0 + sy, mn);
+            pecYp = pecMask<V>(mn);
+        }
+        if (live && k > 0 && TLM_GUARD(node0 - sz, P - V + 1, 3))
+        {
+            loadMat<V>(a.mat, node0 - sz, mn);
+            pecZm = pecMask<V>(mn);
+        }
+        if (live && k < a.nz - 1 && TLM_GUARD(node0 + sz, P - V + 1, 3))
+        {
+            loadMat<V>(a.mat, node0 + sz, mn);
+            pecZp = pecMask<V>(mn);
+        }
+        const unsigned pecOwn = pecMask<V>(m);
+        // x neighbours: inside the vector, else the adjacent lane's vector,
+        // else (warp edge) one scalar load.
+        unsigned prevPec = __shfl_up_sync(0xffffffffu, (pecOwn >> (V - 1)) & 1u, 1);
+        unsigned nextPec = __shfl_down_sync(0xffffffffu, pecOwn & 1u, 1);
+        const bool needPrev = live && x0 > 0;
+        const bool needNext = live && x0 + V <= a.nx - 1;
+        if (lane == 0 && needPrev && TLM_GUARD(node0 - 1, P, 4))
+            prevPec = a.mat[node0 - 1] == kPec;
+        if (lane == 31 && needNext && TLM_GUARD(node0 + V, P, 4))
+            nextPec = a.mat[node0 + V] == kPec;
+        const unsigned pecXm = ((pecOwn << 1) | (prevPec & 1u)) & ((1u << V) - 1);
+        const unsigned pecXp = (pecOwn >> 1) | ((nextPec & 1u) << (V - 1));
+
+        // ---- x axis: own vectors of slots 0..3 ----
+        R ox[4][V];
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+        {
+            if (live && TLM_GUARD(s * P + node0, 12 * P - V + 1, 5))
+                loadPack<S, V>(a.in, s * P + node0, ox[s], a.scale);
+            else
+            {
+#pragma unroll
+                for (int c = 0; c < V; ++c) ox[s][c] = R(0);
+            }
+        }
+        R prevX[2], nextX[2];
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+        {
+            prevX[t] = __shfl_up_sync(0xffffffffu, ox[2 + t][V - 1], 1);
+            nextX[t] = __shfl_down_sync(0xffffffffu, ox[t][0], 1);
+        }
+        if (lane == 0 && needPrev)
+        {
+#pragma unroll
+            for (int t = 0; t < 2; ++t)
+                if (TLM_GUARD((2 + t) * P + node0 - 1, 12 * P, 6))
+                    prevX[t] = decode(a.in[(2 + t) * P + node0 - 1], a.scale);
+        }
+        if (lane == 31 && needNext)
+        {
+#pragma unroll
+            for (int t = 0; t < 2; ++t)
+                if (TLM_GUARD(t * P + node0 + V, 12 * P, 6))
+                    nextX[t] = decode(a.in[t * P + node0 + V], a.scale);
+        }
+#pragma unroll
+        for (int c = 0; c < V; ++c)
+        {
+            const int x = x0 + c;
+#pragma unroll
+            for (int t = 0; t < 2; ++t)
+            {
+                // face -x: neighbour's +x reflected pulse (slot 2+t)
+                R from = (c > 0) ? ox[2 + t][c > 0 ? c - 1 : 0] : prevX[t];
+                R lo = (x == 0) ? a.rho * ox[t][c] : (((pecXm >> c) & 1u) ? -ox[t][c] : from);
+                // face +x: neighbour's -x reflected pulse (slot t)
+                R fromH = (c < V - 1) ? ox[t][c < V - 1 ? c + 1 : 0] : nextX[t];
+                R hi = (x == a.nx - 1) ? a.rho * ox[2 + t][c]
+                                       : (((pecXp >> c) & 1u) ? -ox[2 + t][c] : fromH);
+                inc[t][c] = lo;
+                inc[2 + t][c] = hi;
+            }
+        }
+
+        // ---- y and z axes ----
+        // face -a of node c reads slot (a,+,t) of the node one row/plane
+        // below; face +a reads slot (a,-,t) one row/plane above. On the outer
+        // face the own reflected pulse is loaded instead and scaled by rho;
+        // next to a PEC node the own pulse is loaded as well and negated.
+#pragma unroll
+        for (int ax = 1; ax < 3; ++ax)
+        {
+            const long long st = ax == 1 ? sy : sz;
+            const bool atLo = ax == 1 ? (j == 0) : (k == 0);
+            const bool atHi = ax == 1 ? (j == a.ny - 1) : (k == a.nz - 1);
+            const unsigned pm = ax == 1 ? pecYm : pecZm;
+            const unsigned pp = ax == 1 ? pecYp : pecZp;
+#pragma unroll
+            for (int t = 0; t < 2; ++t)
+            {
+                const int sLo = ax * 4 + t;      // face -a
+                const int sHi = ax * 4 + 2 + t;  // face +a
+                R vLo[V], vHi[V];
+                // -a face
+                {
+                    const long long idx = atLo ? sLo * P + node0 : sHi * P + node0 - st;
+                    if (live && TLM_GUARD(idx, 12 * P - V + 1, 7))
+                        loadPack<S, V>(a.in, idx, vLo, a.scale);
+                    else
+                    {
+#pragma unroll
+                        for (int c = 0; c < V; ++c) vLo[c] = R(0);
+                    }
+                    if (atLo)
+                    {
+#pragma unroll
+                        for (int c = 0; c < V; ++c) vLo[c] = a.rho * vLo[c];
+                    }
+                    else if (pm & nodeLive)
+                    {
+                        R own[V];
+                        if (TLM_GUARD(sLo * P + node0, 12 * P - V + 1, 8))
+                            loadPack<S, V>(a.in, sLo * P + node0, own, a.scale);
+#pragma unroll
+                        for (int c = 0; c < V; ++c)
+                            if ((pm >> c) & 1u) vLo[c] = -own[c];
+                    }
+                }
+                // +a face
+                {
+                    const long long idx = atHi ? sHi * P + node0 : sLo * P + node0 + st;
+                    if (live && TLM_GUARD(idx, 12 * P - V + 1, 9))
+                        loadPack<S, V>(a.in, idx, vHi, a.scale);
+                    else
+                    {
+#pragma unroll
+                        for (int c = 0; c < V; ++c) vHi[c] = R(0);
+                    }
+                    if (atHi)
+                    {
+#pragma unroll
+                        for (int c = 0; c < V; ++c) vHi[c] = a.rho * vHi[c];
+                    }
+                    else if (pp & nodeLive)
+                    {
+                        R own[V];
+                        if (TLM_GUARD(sHi * P + node0, 12 * P - V + 1, 10))
+                            loadPack<S, V>(a.in, sHi * P + node0, own, a.scale);
+#pragma unroll
+                        for (int c = 0; c < V; ++c)
+                            if ((pp >> c) & 1u) vHi[c] = -own[c];
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < V; ++c)
+                {
+                    inc[sLo][c] = vLo[c];
+                    inc[sHi][c] = vHi[c];
+                }
+            }
+        }
+    }
+
+    // ---- sources and monitor samples (rare: only blocks that hold one) ----
+    if (a.tile_begin != nullptr)
+    {
+        const int b0 = a.tile_begin[blockIdx.x], b1 = a.tile_begin[blockIdx.x + 1];
+        if (b0 < b1 && live)
+        {
+            int lo = b0, hi = b1;
+            while (lo < hi)
+            {
+                const int mid = (lo + hi) >> 1;
+                if (a.spec[mid].node < node0) lo = mid + 1; else hi = mid;
+            }
+            for (int e = lo; e < b1; ++e)
+            {
+                const SpecEntry se = a.spec[e];
+                if (se.node >= node0 + V) break;
+                const int c = (int)(se.node - node0);
+                if (se.kind == kInject)
+                {
+                    // q = (0.5*amp)*sv onto the 4 links carrying E_pol
+                    const R qv = (R(0.5) * R(se.amp)) * a.sv;
+                    const int pol = se.arg;
+#pragma unroll
+                    for (int s = 0; s < 12; ++s)
+                    {
+                        if ((s >> 2) != pol && fieldOfSlot(s) == pol)
+                        {
+#pragma unroll
+                            for (int cc = 0; cc < V; ++cc)
+                                if (cc == c) inc[s][cc] = inc[s][cc] + qv;
+                        }
+                    }
+                }
+                else
+                {
+                    R v[12];
+#pragma unroll
+                    for (int s = 0; s < 12; ++s)
+                    {
+                        v[s] = inc[s][0];
+#pragma unroll
+                        for (int cc = 1; cc < V; ++cc)
+                            if (cc == c) v[s] = inc[s][cc];
+                    }
+                    R *dst = a.samples + (long long)se.arg * 6;
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj) dst[jj] = nodeVoltage(v, jj);
+#pragma unroll
+                    for (int kk = 0; kk < 3; ++kk) dst[3 + kk] = circulation(v, kk);
+                }
+            }
+        }
+    }
+
+    // ---- energy: sum of squares of the incident link pulses, FP64 ----
+    if (a.epart != nullptr)
+    {
+        double e = 0.0;
+#pragma unroll
+        for (int c = 0; c < V; ++c)
+        {
+            if ((nodeLive >> c) & 1u)
+            {
+#pragma unroll
+                for (int s = 0; s < 12; ++s) e += (double)inc[s][c] * (double)inc[s][c];
+            }
+        }
+        const double tot = blockSumDouble(e, red);
+        if (threadIdx.x == 0) a.epart[blockIdx.x] = tot;
+    }
+
+    // ---- scatter and store ----
+    R outv[12][V];
+    R vs[3][V];
+    const bool anyDiel = a.stub != nullptr && live;
+    unsigned dielMask = 0;
+#pragma unroll
+    for (int c = 0; c < V; ++c) dielMask |= ((m[c] >= kDiel0) ? 1u : 0u) << c;
+    dielMask &= nodeLive;
+    if (anyDiel && dielMask)
+    {
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj)
+        {
+            if (TLM_GUARD(jj * P + node0, 3 * P - V + 1, 11))
+            {
+                const Pack<R, V> p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
+#pragma unroll
+                for (int c = 0; c < V; ++c) vs[jj][c] = p.v[c];
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < V; ++c)
+    {
+        R in1[12], o1[12];
+#pragma unroll
+        for (int s = 0; s < 12; ++s) in1[s] = inc[s][c];
+        if ((dielMask >> c) & 1u)
+        {
+            const int id = m[c] - kDiel0;
+            R v3[3] = { vs[0][c], vs[1][c], vs[2][c] };
+            scatterStub(in1, v3, a.yhat[id], a.ghat[id], o1);
+            vs[0][c] = v3[0];
+            vs[1][c] = v3[1];
+            vs[2][c] = v3[2];
+        }
+        else
+            scatterAir(in1, o1);
+        const bool on = (nodeLive >> c) & 1u;
+#pragma unroll
+        for (int s = 0; s < 12; ++s) outv[s][c] = on ? o1[s] : R(0);
+    }
+    if (live)
+    {
+#pragma unroll
+        for (int s = 0; s < 12; ++s)
+        {
+            if (TLM_GUARD(s * P + node0, 12 * P - V + 1, 12))
+            {
+                Pack<S, V> p;
+#pragma unroll
+                for (int c = 0; c < V; ++c) p.v[c] = encode<S>(outv[s][c], a.inv_scale);
+                *reinterpret_cast<Pack<S, V> *>(a.out + s * P + node0) = p;
+            }
+        }
+        if (anyDiel && dielMask)
+        {
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+            {
+                if (TLM_GUARD(jj * P + node0, 3 * P - V + 1, 13))
+                {
+                    Pack<R, V> p;
+#pragma unroll
+                    for (int c = 0; c < V; ++c) p.v[c] = vs[jj][c];
+                    *reinterpret_cast<Pack<R, V> *>(a.stub + jj * P + node0) = p;
+                }
+            }
+        }
+    }
+}
+
+} // namespace tlmk

@@ -1,0 +1,266 @@
+/*
+ * tlm_b200.h -- C ABI of the B200-native SCN TLM time step.
+ *
+ * Drop-in replacement for the time loop behind smilima/EMSolver's
+ * TlmSolver (TlmSolver.h:202-264, the IFieldSolver implementation at
+ * TlmSolver.h:148-192). Every entry point below names the reference
+ * interface it stands in for. Plain C types only: no CUDA or C++ types cross
+ * this boundary, so cgo / JNI / ctypes / C++ can bind it directly.
+ *
+ * Conventions
+ *  - Every call returns a tlm_status; TLM_OK is 0. On failure the handle's
+ *    message (tlm_last_error) says why; failures before a handle exists go
+ *    to the thread's message (tlm_last_error(NULL)).
+ *  - The library owns all device state. Input arrays are copied during the
+ *    call. Output arrays are caller-allocated with a stated capacity; the
+ *    number of valid elements is written to *n_out.
+ *  - A handle is not re-entrant: one thread drives it. tlm_request_stop,
+ *    tlm_current_step, tlm_current_energy, tlm_is_running and
+ *    tlm_is_finished may be called from any thread at any time, which is
+ *    how the reference's UI polls a solver running on a worker thread
+ *    (MainUnit.cpp:991, :1453).
+ *  - There is no CPU fallback. If the CUDA device or the kernels are not
+ *    usable the call fails with TLM_ENODEV / TLM_ECUDA.
+ *
+ * Cell indexing is the reference's VoxelGridSpec::cellIndex
+ * (Geometry.h:91-94): cell = (k*ny + j)*nx + i. Link-pulse slots follow the
+ * reference's portOf (TlmSolver.cpp:19-29): slot = axis*4 + side*2 + pol.
+ */
+#ifndef TLM_B200_H
+#define TLM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define TLM_API __attribute__((visibility("default")))
+#else
+#define TLM_API
+#endif
+
+typedef enum tlm_status {
+    TLM_OK = 0,
+    TLM_EINVAL = 1,    /* bad argument or inconsistent inputs */
+    TLM_ENOMEM = 2,    /* HBM admission refused or allocation failed */
+    TLM_ECUDA = 3,     /* CUDA runtime / kernel error */
+    TLM_ETIMEOUT = 4,  /* a bounded device wait ran out */
+    TLM_ESTOPPED = 5,  /* run ended early by tlm_request_stop */
+    TLM_ESTATE = 6,    /* call not valid in the handle's current state */
+    TLM_ENODEV = 7,    /* no usable CUDA device / kernels not loadable */
+    TLM_EBUSY = 8      /* the handle is running on another thread */
+} tlm_status;
+
+/* Material ids of the map (TlmSolver.h:59): 0 air, 1 PEC, id >= 2 a
+ * dielectric whose properties are table[id - 2]. */
+enum { TLM_MAT_AIR = 0, TLM_MAT_PEC = 1, TLM_MAT_DIEL0 = 2 };
+
+/* WaveformType (TlmSolver.h:70) plus TLM_WAVE_TABLE: per-step source values
+ * supplied by tlm_set_source_table (the harness-side waveform hook). */
+typedef enum tlm_waveform {
+    TLM_WAVE_CW_RAMPED = 0,
+    TLM_WAVE_GAUSSIAN_SINE = 1,
+    TLM_WAVE_GAUSSIAN_PULSE = 2,
+    TLM_WAVE_TABLE = 3
+} tlm_waveform;
+
+/* Pulse storage. Scatter arithmetic is FP32 for F32/BF16/F16 and FP64 for
+ * F64 (the on-device FP64 oracle mode). BF16/F16 store pulse/scale. */
+typedef enum tlm_storage {
+    TLM_STORE_F32 = 0,
+    TLM_STORE_BF16 = 1,
+    TLM_STORE_F16 = 2,
+    TLM_STORE_F64 = 3
+} tlm_storage;
+
+/* VoxelGridSpec (Geometry.h:85-113). */
+typedef struct tlm_grid {
+    int nx, ny, nz;
+    float origin[3];
+    float dl;
+} tlm_grid;
+
+/* MatProps (TlmSolver.h:61-65). */
+typedef struct tlm_matprops {
+    float epsr;
+    float sigma;
+} tlm_matprops;
+
+/* TlmConfig (TlmSolver.h:113-123) and the B200 extensions after it. */
+typedef struct tlm_config {
+    float f0;            /* excitation / analysis frequency (Hz) */
+    int waveform;        /* tlm_waveform */
+    int total_steps;     /* tlm_run stops here */
+    int settle_steps;    /* kept for interface parity (Js DFT start) */
+    float boundary_rho;  /* outer-face reflection coefficient */
+    int huy_offset;      /* Huygens box inset; accepted, not yet used */
+    int use_gpu;         /* ignored: this library always runs on the GPU */
+    int record_every;    /* accepted, playback frames not yet produced */
+    /* --- extensions --- */
+    int storage;         /* tlm_storage */
+    float pulse_scale;   /* BF16/F16 per-grid scale (0 = choose from sources) */
+    int steps_per_launch;/* steps per monitor window; 0 = default (64) */
+} tlm_config;
+
+typedef struct tlm_solver *tlm_handle;
+
+/* ---- lifetime ------------------------------------------------------- */
+
+/* Version string of the library. */
+TLM_API const char *tlm_version(void);
+
+/* Fill *cfg with TlmConfig's defaults (TlmSolver.h:113-123). */
+TLM_API void tlm_config_default(tlm_config *cfg);
+
+/* Replaces `new TlmSolver()` (TlmSolver.cpp:245-250): binds a handle to a
+ * CUDA device and creates its stream. */
+TLM_API tlm_status tlm_create(tlm_handle *out, int device);
+
+/* Replaces `delete solver` (TlmSolver.cpp:253-256). */
+TLM_API tlm_status tlm_destroy(tlm_handle h);
+
+/* Message of the last failure on h (NULL: of the calling thread). */
+TLM_API const char *tlm_last_error(tlm_handle h);
+
+/* ---- setup (TlmSolver::setup, TlmSolver.cpp:259-304) ---------------- */
+
+/* Copies the material map (n_cells = nx*ny*nz bytes) and the dielectric
+ * table, derives yhat = 4*(max(1,epsr)-1) and ghat = max(0,sigma)*dl*eta0
+ * per table entry, zeroes all pulse state, clears ports/probes/sources and
+ * allocates device memory (refused with TLM_ENOMEM if it would not fit).
+ * Unlike the reference, a material id >= 2 without a table entry is
+ * rejected (TLM_EINVAL) instead of reading past the table. */
+TLM_API tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat,
+                             size_t n_cells, const tlm_matprops *table, int n_table,
+                             const tlm_config *cfg);
+
+/* TlmSolver::addPort (TlmSolver.cpp:362-374). Cells that are not air (or
+ * out of range) are dropped silently, as in the reference. *out_idx gets
+ * the port index. A port whose current loop (the 4 transverse linear-index
+ * neighbours of its middle cell, TlmSolver.cpp:687-698) would read outside
+ * the grid is refused with TLM_EINVAL; the reference reads out of bounds. */
+TLM_API tlm_status tlm_add_port(tlm_handle h, const uint64_t *cells, int n_cells,
+                                int pol_axis, float amp, int *out_idx);
+
+/* TlmSolver::addPlaneWave (TlmSolver.cpp:394-407). */
+TLM_API tlm_status tlm_add_plane_wave(tlm_handle h, int prop_axis, int plane_index,
+                                      int pol_axis, float amp);
+
+/* TlmSolver::addProbe (TlmSolver.cpp:377-391): *out_idx = -1 when the world
+ * point is outside the grid (status TLM_OK, like the reference). */
+TLM_API tlm_status tlm_add_probe(tlm_handle h, float x, float y, float z, int *out_idx);
+
+/* Probe at a cell given by its indices (no world-position rounding). */
+TLM_API tlm_status tlm_add_probe_cell(tlm_handle h, int i, int j, int k, int *out_idx);
+
+/* Per-step source values for TLM_WAVE_TABLE (steps past the table get 0).
+ * Stands in for TlmSolver::waveformValue (TlmSolver.cpp:410-436). */
+TLM_API tlm_status tlm_set_source_table(tlm_handle h, const float *sv, int n_steps);
+
+/* Frequencies (Hz) of the on-device FP64 running DFT of every port's V and
+ * I records: V(f) = sum_n v[n] exp(-j 2 pi f n dt), the transform the
+ * reference computes after the run from the float records
+ * (SelfTest.cpp:182-195, MainUnit.cpp:1830-1846). Call before stepping. */
+TLM_API tlm_status tlm_set_port_dft(tlm_handle h, const double *freqs_hz, int n_freq);
+
+/* ---- time loop -------------------------------------------------------- */
+
+/* Advance n_steps time steps (TlmSolver::step, TlmSolver.cpp:485-513, once
+ * per step: inject, monitors, scatter, connect) and wait for the device. */
+TLM_API tlm_status tlm_step(tlm_handle h, int n_steps);
+
+/* Same, without waiting: the work is queued on the handle's stream.
+ * Results are visible after tlm_sync (or any getter, which syncs). */
+TLM_API tlm_status tlm_step_async(tlm_handle h, int n_steps);
+TLM_API tlm_status tlm_sync(tlm_handle h);
+
+/* TlmSolver::run (TlmSolver.cpp:439-464): steps from the current step to
+ * total_steps, checking the stop flag between launch windows. Returns
+ * TLM_ESTOPPED if tlm_request_stop ended it early; calling it again resumes
+ * from the current step, as runCpu does. */
+TLM_API tlm_status tlm_run(tlm_handle h);
+
+/* TlmSolver::requestStop / currentStep / currentEnergy / isRunning /
+ * isFinished / totalSteps / timestep (TlmSolver.h:219-234). Thread-safe. */
+TLM_API tlm_status tlm_request_stop(tlm_handle h);
+TLM_API int tlm_current_step(tlm_handle h);
+TLM_API float tlm_current_energy(tlm_handle h);
+TLM_API int tlm_is_running(tlm_handle h);
+TLM_API int tlm_is_finished(tlm_handle h);
+TLM_API int tlm_total_steps(tlm_handle h);
+TLM_API tlm_status tlm_timestep(tlm_handle h, float *dt);
+
+/* ---- results ------------------------------------------------------- */
+
+TLM_API int tlm_probe_count(tlm_handle h);
+/* TlmSolver::probe(i) (TlmSolver.h:260): the E series, one value per step. */
+TLM_API tlm_status tlm_get_probe(tlm_handle h, int idx, float *ex, float *ey, float *ez,
+                                 int cap, int *n_out);
+TLM_API tlm_status tlm_get_probe_f64(tlm_handle h, int idx, double *ex, double *ey,
+                                     double *ez, int cap, int *n_out);
+TLM_API tlm_status tlm_get_probe_cell(tlm_handle h, int idx, uint64_t *cell);
+
+TLM_API int tlm_port_count(tlm_handle h);
+/* TlmSolver::ports()[i].vRec / iRec (TlmSolver.h:81-87). */
+TLM_API tlm_status tlm_get_port(tlm_handle h, int idx, float *v, float *i, int cap,
+                                int *n_out);
+TLM_API tlm_status tlm_get_port_f64(tlm_handle h, int idx, double *v, double *i, int cap,
+                                    int *n_out);
+/* Gap cells kept by tlm_add_port (air cells only, in the caller's order). */
+TLM_API tlm_status tlm_get_port_cells(tlm_handle h, int idx, uint64_t *cells, int cap,
+                                      int *n_out);
+/* FP64 running DFT of port idx at the tlm_set_port_dft frequencies. */
+TLM_API tlm_status tlm_get_port_dft(tlm_handle h, int idx, double *v_re, double *v_im,
+                                    double *i_re, double *i_im, int cap, int *n_out);
+
+/* TlmSolver::getEnergyHistory (TlmSolver.cpp:793-799): sum of the squares
+ * of all link pulses every 16 steps, accumulated in FP64. vals (float, as
+ * the reference) and/or vals64 may be NULL. */
+TLM_API tlm_status tlm_get_energy_history(tlm_handle h, int *steps, float *vals,
+                                          double *vals64, int cap, int *n_out);
+
+/* Incident pulses in the reference's AoS layout (cell*12 + slot), i.e. the
+ * reference's V after the last completed step; float or double. */
+TLM_API tlm_status tlm_get_pulses(tlm_handle h, float *out, size_t cap);
+TLM_API tlm_status tlm_get_pulses_f64(tlm_handle h, double *out, size_t cap);
+/* Overwrite the incident pulses (snapshot restore / test set-up). */
+TLM_API tlm_status tlm_set_pulses(tlm_handle h, const float *in, size_t n);
+/* Stub pulses (cell*3 + j; zeros when the grid has no dielectric). */
+TLM_API tlm_status tlm_get_stubs(tlm_handle h, float *out, size_t cap);
+/* Device copies of the material map and the yhat / ghat tables. */
+TLM_API tlm_status tlm_get_materials(tlm_handle h, uint8_t *out, size_t cap);
+TLM_API tlm_status tlm_get_tables(tlm_handle h, float *yhat, float *ghat, int cap,
+                                  int *n_out);
+
+/* TlmSolver::waveformValue (TlmSolver.cpp:410-436) for a grid of cell size
+ * dl: the source value the step kernels inject at step n (FP32 modes).
+ * Host-only; needs no device. */
+TLM_API tlm_status tlm_waveform_value(int waveform, float f0, float dl, int n, float *out);
+
+/* ---- known-answer tests run on the device --------------------------- */
+
+/* TlmSolver::ScatterUnitarityError / DielScatterUnitarityError
+ * (TlmSolver.cpp:116-169), evaluated with the device scatter functions. */
+TLM_API tlm_status tlm_scatter_unitarity_error(int device, float *err);
+TLM_API tlm_status tlm_stub_unitarity_error(int device, float epsr, float *err);
+
+/* ---- bench / integration helpers ------------------------------------ */
+
+/* The handle's CUDA stream (cudaStream_t) for event timing by the caller. */
+TLM_API tlm_status tlm_get_stream(tlm_handle h, void **stream);
+/* Bytes of device memory the handle holds. */
+TLM_API tlm_status tlm_device_bytes(tlm_handle h, size_t *bytes);
+/* Kernel timing: when enabled, every step-kernel launch is bracketed by CUDA
+ * events on the handle's stream; tlm_kernel_time returns the summed
+ * duration and launch count since the last enable. */
+TLM_API tlm_status tlm_set_kernel_timing(tlm_handle h, int enable);
+TLM_API tlm_status tlm_kernel_time(tlm_handle h, double *ms, long long *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TLM_B200_H */

@@ -1,0 +1,371 @@
+"""ctypes wrappers for the oracle libraries (TEST INFRASTRUCTURE ONLY)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libtlmref.so")
+
+_u8p = C.POINTER(C.c_uint8)
+_f32p = C.POINTER(C.c_float)
+_f64p = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int)
+_u64p = C.POINTER(C.c_uint64)
+
+
+def build_oracle(quiet: bool = True) -> None:
+    """Compile liboracle.so (and the reference under _ref/ when its sources exist)."""
+    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+def _setup_args(nx, ny, nz, origin, dl, mat, table):
+    mat = np.ascontiguousarray(mat, dtype=np.uint8).reshape(-1)
+    if mat.size != nx * ny * nz:
+        raise ValueError("material map size mismatch")
+    eps = np.ascontiguousarray([t[0] for t in table] or [1.0], dtype=np.float32)
+    sig = np.ascontiguousarray([t[1] for t in table] or [0.0], dtype=np.float32)
+    ox, oy, oz = (float(v) for v in origin)
+    return mat, eps, sig, ox, oy, oz
+
+
+class Oracle:
+    """The CPU restatement; ``fp64=False`` is bitwise the reference's float step."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not os.path.exists(ORACLE_SO):
+                build_oracle()
+            L = C.CDLL(ORACLE_SO)
+            L.orc_create.restype = C.c_void_p
+            L.orc_create.argtypes = [C.c_int]
+            L.orc_destroy.argtypes = [C.c_void_p]
+            L.orc_setup.restype = C.c_int
+            L.orc_setup.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                    C.c_float, C.c_float, _u8p, _f32p, _f32p, C.c_int, C.c_float,
+                                    C.c_int, C.c_int, C.c_int, C.c_float]
+            L.orc_add_port.restype = C.c_int
+            L.orc_add_port.argtypes = [C.c_void_p, _u64p, C.c_int, C.c_int, C.c_float]
+            L.orc_add_probe.restype = C.c_int
+            L.orc_add_probe.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float]
+            L.orc_add_plane_wave.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float]
+            L.orc_waveform.restype = C.c_double
+            L.orc_waveform.argtypes = [C.c_void_p, C.c_int]
+            L.orc_dt.restype = C.c_double
+            L.orc_dt.argtypes = [C.c_void_p]
+            L.orc_steps.argtypes = [C.c_void_p, C.c_int, C.c_int, _f64p]
+            for nm in ("orc_get_pulses", "orc_get_stubs"):
+                getattr(L, nm).restype = C.c_size_t
+                getattr(L, nm).argtypes = [C.c_void_p, _f64p, C.c_size_t]
+            L.orc_set_pulses.restype = C.c_size_t
+            L.orc_set_pulses.argtypes = [C.c_void_p, _f64p, C.c_size_t]
+            L.orc_get_tables.restype = C.c_int
+            L.orc_get_tables.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int]
+            L.orc_probe_count.restype = C.c_int
+            L.orc_probe_count.argtypes = [C.c_void_p]
+            L.orc_get_probe.restype = C.c_int
+            L.orc_get_probe.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p, C.c_int, _u64p]
+            L.orc_port_count.restype = C.c_int
+            L.orc_port_count.argtypes = [C.c_void_p]
+            L.orc_get_port.restype = C.c_int
+            L.orc_get_port.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, C.c_int]
+            L.orc_energy_history.restype = C.c_int
+            L.orc_energy_history.argtypes = [C.c_void_p, _i32p, _f64p, C.c_int]
+            L.orc_scatter_unitarity.restype = C.c_double
+            L.orc_scatter_unitarity.argtypes = [C.c_int]
+            L.orc_stub_unitarity.restype = C.c_double
+            L.orc_stub_unitarity.argtypes = [C.c_int, C.c_double]
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, fp64: bool = False):
+        self.L = self.lib()
+        self.fp64 = bool(fp64)
+        self.h = self.L.orc_create(1 if fp64 else 0)
+        self.n = 0
+        self.step_index = 0
+        self.dtype = np.float64 if fp64 else np.float32
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.L.orc_destroy(h)
+            self.h = None
+
+    def setup(self, nx, ny, nz, mat, table=(), origin=(0.0, 0.0, 0.0), dl=1e-3, f0=1e9,
+              waveform=2, total_steps=2000, settle_steps=600, rho=0.0):
+        mat, eps, sig, ox, oy, oz = _setup_args(nx, ny, nz, origin, dl, mat, table)
+        rc = self.L.orc_setup(self.h, nx, ny, nz, ox, oy, oz, dl, _ptr(mat, _u8p), _ptr(eps, _f32p),
+                              _ptr(sig, _f32p), len(table), f0, waveform, total_steps,
+                              settle_steps, rho)
+        if rc != 0:
+            raise ValueError(f"oracle setup rejected the inputs (code {rc})")
+        self.n = nx * ny * nz
+        self.step_index = 0
+
+    def add_port(self, cells, pol, amp=1.0):
+        c = np.ascontiguousarray(cells, dtype=np.uint64).reshape(-1)
+        return self.L.orc_add_port(self.h, _ptr(c, _u64p), c.size, pol, amp)
+
+    def add_probe(self, x, y, z):
+        return self.L.orc_add_probe(self.h, x, y, z)
+
+    def add_plane_wave(self, prop_axis, plane_index, pol_axis, amp=1.0):
+        self.L.orc_add_plane_wave(self.h, prop_axis, plane_index, pol_axis, amp)
+
+    def waveform(self, n):
+        return self.L.orc_waveform(self.h, n)
+
+    @property
+    def dt(self):
+        return self.L.orc_dt(self.h)
+
+    def steps(self, count, sv=None):
+        if sv is not None:
+            sv = np.ascontiguousarray(sv, dtype=np.float64).reshape(-1)
+            assert sv.size >= count
+            self.L.orc_steps(self.h, self.step_index, count, _ptr(sv, _f64p))
+        else:
+            self.L.orc_steps(self.h, self.step_index, count, None)
+        self.step_index += count
+
+    def pulses(self):
+        out = np.empty(self.n * 12, np.float64)
+        self.L.orc_get_pulses(self.h, _ptr(out, _f64p), out.size)
+        return out.astype(self.dtype)
+
+    def set_pulses(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        if self.L.orc_set_pulses(self.h, _ptr(v, _f64p), v.size) != v.size:
+            raise ValueError("pulse array size mismatch")
+
+    def stubs(self):
+        n = self.L.orc_get_stubs(self.h, None, 0)
+        out = np.empty(n, np.float64)
+        if n:
+            self.L.orc_get_stubs(self.h, _ptr(out, _f64p), n)
+        return out.astype(self.dtype)
+
+    def tables(self):
+        y = np.empty(256, np.float64)
+        g = np.empty(256, np.float64)
+        n = self.L.orc_get_tables(self.h, _ptr(y, _f64p), _ptr(g, _f64p), 256)
+        return y[:n].astype(self.dtype), g[:n].astype(self.dtype)
+
+    def probe(self, idx):
+        cap = self.step_index
+        ex, ey, ez = (np.empty(max(cap, 1), np.float64) for _ in range(3))
+        cell = C.c_uint64(0)
+        n = self.L.orc_get_probe(self.h, idx, _ptr(ex, _f64p), _ptr(ey, _f64p), _ptr(ez, _f64p),
+                                 cap, C.byref(cell))
+        return (ex[:n].astype(self.dtype), ey[:n].astype(self.dtype), ez[:n].astype(self.dtype))
+
+    def port(self, idx):
+        cap = self.step_index
+        v, i = (np.empty(max(cap, 1), np.float64) for _ in range(2))
+        n = self.L.orc_get_port(self.h, idx, _ptr(v, _f64p), _ptr(i, _f64p), cap)
+        return v[:n].astype(self.dtype), i[:n].astype(self.dtype)
+
+    def energy_history(self):
+        cap = self.step_index // 16 + 2
+        st = np.empty(cap, np.int32)
+        va = np.empty(cap, np.float64)
+        n = self.L.orc_energy_history(self.h, _ptr(st, _i32p), _ptr(va, _f64p), cap)
+        return st[:n].copy(), va[:n].copy()
+
+    @classmethod
+    def scatter_unitarity(cls, fp64=False):
+        return cls.lib().orc_scatter_unitarity(1 if fp64 else 0)
+
+    @classmethod
+    def stub_unitarity(cls, epsr, fp64=False):
+        return cls.lib().orc_stub_unitarity(1 if fp64 else 0, epsr)
+
+
+class RefSolver:
+    """The reference's own TlmSolver (compiled headless), same methods as ``Oracle``."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not os.path.exists(REF_SO):
+                raise FileNotFoundError(
+                    "oracle/_ref/libtlmref.so is missing (it is built from the reference sources "
+                    "by `make -C oracle`)")
+            L = C.CDLL(REF_SO)
+            L.ref_create.restype = C.c_void_p
+            L.ref_destroy.argtypes = [C.c_void_p]
+            L.ref_setup.restype = C.c_int
+            L.ref_setup.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                    C.c_float, C.c_float, _u8p, _f32p, _f32p, C.c_int, C.c_float,
+                                    C.c_int, C.c_int, C.c_int, C.c_float]
+            L.ref_add_port.restype = C.c_int
+            L.ref_add_port.argtypes = [C.c_void_p, _u64p, C.c_int, C.c_int, C.c_float]
+            L.ref_add_probe.restype = C.c_int
+            L.ref_add_probe.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float]
+            L.ref_add_plane_wave.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float]
+            L.ref_steps.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            L.ref_steps_sv.argtypes = [C.c_void_p, C.c_int, C.c_int, _f32p]
+            L.ref_run.argtypes = [C.c_void_p]
+            L.ref_waveform.restype = C.c_float
+            L.ref_waveform.argtypes = [C.c_void_p, C.c_int]
+            L.ref_dt.restype = C.c_float
+            L.ref_dt.argtypes = [C.c_void_p]
+            L.ref_threads.restype = C.c_int
+            L.ref_threads.argtypes = [C.c_void_p]
+            L.ref_current_step.restype = C.c_int
+            L.ref_current_step.argtypes = [C.c_void_p]
+            for nm in ("ref_get_pulses", "ref_get_stubs"):
+                getattr(L, nm).restype = C.c_size_t
+                getattr(L, nm).argtypes = [C.c_void_p, _f32p, C.c_size_t]
+            L.ref_set_pulses.restype = C.c_size_t
+            L.ref_set_pulses.argtypes = [C.c_void_p, _f32p, C.c_size_t]
+            L.ref_get_tables.restype = C.c_int
+            L.ref_get_tables.argtypes = [C.c_void_p, _f32p, _f32p, C.c_int]
+            L.ref_probe_count.restype = C.c_int
+            L.ref_probe_count.argtypes = [C.c_void_p]
+            L.ref_get_probe.restype = C.c_int
+            L.ref_get_probe.argtypes = [C.c_void_p, C.c_int, _f32p, _f32p, _f32p, C.c_int, _u64p]
+            L.ref_port_count.restype = C.c_int
+            L.ref_port_count.argtypes = [C.c_void_p]
+            L.ref_get_port.restype = C.c_int
+            L.ref_get_port.argtypes = [C.c_void_p, C.c_int, _f32p, _f32p, C.c_int, _u64p, C.c_int,
+                                       _i32p]
+            L.ref_energy_history.restype = C.c_int
+            L.ref_energy_history.argtypes = [C.c_void_p, _i32p, _f32p, C.c_int]
+            L.ref_scatter_unitarity.restype = C.c_float
+            L.ref_diel_unitarity.restype = C.c_float
+            L.ref_diel_unitarity.argtypes = [C.c_float]
+            L.ref_hw_concurrency.restype = C.c_uint
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self):
+        self.L = self.lib()
+        self.h = self.L.ref_create()
+        self.n = 0
+        self.step_index = 0
+        self.dtype = np.float32
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.L.ref_destroy(h)
+            self.h = None
+
+    @property
+    def threads(self):
+        return self.L.ref_threads(self.h)
+
+    def setup(self, nx, ny, nz, mat, table=(), origin=(0.0, 0.0, 0.0), dl=1e-3, f0=1e9,
+              waveform=2, total_steps=2000, settle_steps=600, rho=0.0):
+        mat, eps, sig, ox, oy, oz = _setup_args(nx, ny, nz, origin, dl, mat, table)
+        self.L.ref_setup(self.h, nx, ny, nz, ox, oy, oz, dl, _ptr(mat, _u8p), _ptr(eps, _f32p),
+                         _ptr(sig, _f32p), len(table), f0, waveform, total_steps, settle_steps, rho)
+        self.n = nx * ny * nz
+        self.step_index = 0
+
+    def add_port(self, cells, pol, amp=1.0):
+        c = np.ascontiguousarray(cells, dtype=np.uint64).reshape(-1)
+        return self.L.ref_add_port(self.h, _ptr(c, _u64p), c.size, pol, amp)
+
+    def add_probe(self, x, y, z):
+        return self.L.ref_add_probe(self.h, x, y, z)
+
+    def add_plane_wave(self, prop_axis, plane_index, pol_axis, amp=1.0):
+        self.L.ref_add_plane_wave(self.h, prop_axis, plane_index, pol_axis, amp)
+
+    def waveform(self, n):
+        return self.L.ref_waveform(self.h, n)
+
+    @property
+    def dt(self):
+        return self.L.ref_dt(self.h)
+
+    def steps(self, count, sv=None):
+        if sv is not None:
+            sv = np.ascontiguousarray(sv, dtype=np.float32).reshape(-1)
+            assert sv.size >= count
+            self.L.ref_steps_sv(self.h, self.step_index, count, _ptr(sv, _f32p))
+        else:
+            self.L.ref_steps(self.h, self.step_index, count)
+        self.step_index += count
+
+    def run(self):
+        self.L.ref_run(self.h)
+        self.step_index = self.L.ref_current_step(self.h)
+
+    def pulses(self):
+        out = np.empty(self.n * 12, np.float32)
+        self.L.ref_get_pulses(self.h, _ptr(out, _f32p), out.size)
+        return out
+
+    def set_pulses(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float32).reshape(-1)
+        if self.L.ref_set_pulses(self.h, _ptr(v, _f32p), v.size) != v.size:
+            raise ValueError("pulse array size mismatch")
+
+    def stubs(self):
+        n = self.L.ref_get_stubs(self.h, None, 0)
+        out = np.empty(n, np.float32)
+        if n:
+            self.L.ref_get_stubs(self.h, _ptr(out, _f32p), n)
+        return out
+
+    def tables(self):
+        y = np.empty(256, np.float32)
+        g = np.empty(256, np.float32)
+        n = self.L.ref_get_tables(self.h, _ptr(y, _f32p), _ptr(g, _f32p), 256)
+        return y[:n].copy(), g[:n].copy()
+
+    def probe(self, idx):
+        cap = self.step_index
+        ex, ey, ez = (np.empty(max(cap, 1), np.float32) for _ in range(3))
+        cell = C.c_uint64(0)
+        n = self.L.ref_get_probe(self.h, idx, _ptr(ex, _f32p), _ptr(ey, _f32p), _ptr(ez, _f32p),
+                                 cap, C.byref(cell))
+        return ex[:n].copy(), ey[:n].copy(), ez[:n].copy()
+
+    def port(self, idx):
+        cap = self.step_index
+        v, i = (np.empty(max(cap, 1), np.float32) for _ in range(2))
+        nc = C.c_int(0)
+        n = self.L.ref_get_port(self.h, idx, _ptr(v, _f32p), _ptr(i, _f32p), cap, None, 0,
+                                C.byref(nc))
+        return v[:n].copy(), i[:n].copy()
+
+    def energy_history(self):
+        cap = self.step_index // 16 + 2
+        st = np.empty(cap, np.int32)
+        va = np.empty(cap, np.float32)
+        n = self.L.ref_energy_history(self.h, _ptr(st, _i32p), _ptr(va, _f32p), cap)
+        return st[:n].copy(), va[:n].astype(np.float64)
+
+    @classmethod
+    def scatter_unitarity(cls):
+        return cls.lib().ref_scatter_unitarity()
+
+    @classmethod
+    def stub_unitarity(cls, epsr):
+        return cls.lib().ref_diel_unitarity(epsr)

@@ -1,0 +1,57 @@
+"""Small seeded grids for the golden vectors and the parity tests.
+
+They exercise every case of the step: all six outer faces with rho in
+{-1, 0, 0.3, 0.5, 1}, isolated and clustered PEC cells next to air and
+dielectric, overlapping lossy dielectric boxes, ports with three gap cells,
+a plane-wave source, all three standard waveforms and x extents that are not
+a multiple of the kernels' vector width.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from emsolver_b200 import workloads
+
+
+def small_cases():
+    """Small grids that exercise every face, PEC, dielectric and source case."""
+    cases = []
+
+    def boxes(rng, nx, ny, nz, nbox, pec_frac):
+        mat = np.zeros((nz, ny, nx), np.uint8)
+        table = []
+        for b in range(nbox):
+            lo = [int(rng.integers(0, d)) for d in (nz, ny, nx)]
+            hi = [int(rng.integers(l, d)) + 1 for l, d in zip(lo, (nz, ny, nx))]
+            mat[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = 2 + b
+            table.append((float(np.float32(rng.uniform(1, 10))), float(np.float32(rng.uniform(0, 0.05)))))
+        if pec_frac > 0:
+            mat[rng.random((nz, ny, nx)) < pec_frac] = 1
+        return mat.reshape(-1), table
+
+    specs = [
+        # name, dims, rho, nbox, pec, waveform, plane wave, steps, seed
+        ("pec_diel_rho0", (7, 6, 5), 0.0, 3, 0.08, 2, False, 80, 1),
+        ("pec_rho_m1_plane", (9, 8, 10), -1.0, 3, 0.08, 1, True, 80, 2),
+        ("diel_rho_half_cw", (12, 5, 7), 0.5, 2, 0.05, 0, False, 80, 3),
+        ("cube16_mixed", (16, 16, 16), 0.0, 4, 0.04, 2, True, 120, 4),
+        ("odd_x_rho_pmc", (13, 9, 11), 1.0, 2, 0.06, 2, False, 100, 5),
+        ("air_only_rho_03", (10, 12, 9), 0.3, 0, 0.0, 1, False, 90, 6),
+    ]
+    for name, (nx, ny, nz), rho, nbox, pec, wf, plane, steps, seed in specs:
+        rng = np.random.default_rng(seed)
+        mat, table = boxes(rng, nx, ny, nz, nbox, pec)
+        w = workloads.Workload("small_" + name, nx, ny, nz, mat, table, dl=1e-3, f0=3e10,
+                               waveform=wf, steps=steps, rho=rho)
+        kk, jj, ii = np.unravel_index(np.arange(mat.size), (nz, ny, nx))
+        inner = (ii > 0) & (ii < nx - 1) & (jj > 0) & (jj < ny - 1) & (kk > 0) & (kk < nz - 1)
+        air = np.flatnonzero((mat == 0) & inner)
+        for p in range(2):
+            cells = [int(c) for c in rng.choice(air, 3)]
+            w.ports.append((cells, int(rng.integers(0, 3)), float(np.float32(rng.uniform(-2, 2)))))
+        for q in range(3):
+            w.probes_cell.append(tuple(int(rng.integers(0, d)) for d in (nx, ny, nz)))
+        if plane:
+            w.meta["plane_wave"] = (2, nz // 2, 0, 0.7)
+        cases.append(w)
+    return cases

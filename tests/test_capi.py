@@ -1,0 +1,87 @@
+"""The C ABI library on a machine without a GPU: it loads, exports every
+symbol include/tlm_b200.h declares, its host-only math matches the
+reference bit for bit, and compute entry points fail loudly (no fallback)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from tests.conftest import ROOT
+from emsolver_b200 import _lib
+from oracle import Oracle, RefSolver, ref_available
+
+HEADER = os.path.join(ROOT, "include", "tlm_b200.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"TLM_API\s+[\w\s\*]+?\b(tlm_\w+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert len(names) >= 40
+    assert "tlm_setup" in names and "tlm_step" in names and "tlm_get_probe" in names
+
+
+@pytest.mark.parametrize("variant", ["", "checked"])
+def test_library_exports_every_declared_symbol(built, variant):
+    path = _lib.library_path(variant)
+    lib = C.CDLL(path)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+    # the Python binding covers the whole header
+    assert set(declared_symbols()) == set(_lib.SIGNATURES)
+
+
+def test_version_and_defaults(built):
+    L = _lib.load()
+    assert b"sm_100a" in L.tlm_version()
+    c = _lib.ConfigC()
+    L.tlm_config_default(C.byref(c))
+    # TlmConfig defaults (TlmSolver.h:113-123)
+    assert c.f0 == np.float32(1e9) and c.waveform == 0 and c.total_steps == 2000
+    assert c.settle_steps == 600 and c.boundary_rho == 0.0 and c.storage == _lib.STORE_F32
+
+
+def test_waveform_value_bitwise(built):
+    L = _lib.load()
+    out = C.c_float()
+    for wf in (0, 1, 2):
+        O = Oracle(False)
+        O.setup(4, 4, 4, np.zeros(64, np.uint8), [], dl=2.5e-3, f0=1.3e9, waveform=wf)
+        for n in (0, 3, 59, 60, 61, 499, 7999):
+            assert L.tlm_waveform_value(wf, 1.3e9, 2.5e-3, n, C.byref(out)) == 0
+            assert np.float32(out.value) == np.float32(O.waveform(n)), (wf, n)
+            if ref_available():
+                R = RefSolver()
+                R.setup(4, 4, 4, np.zeros(64, np.uint8), [], dl=2.5e-3, f0=1.3e9, waveform=wf)
+                assert np.float32(out.value) == np.float32(R.waveform(n))
+    assert L.tlm_waveform_value(9, 1e9, 1e-3, 0, C.byref(out)) == _lib.TLM_EINVAL
+
+
+def test_null_arguments_are_rejected(built):
+    L = _lib.load()
+    assert L.tlm_create(None, 0) == _lib.TLM_EINVAL
+    assert L.tlm_setup(None, None, None, 0, None, 0, None) == _lib.TLM_EINVAL
+    assert L.tlm_step(None, 1) == _lib.TLM_EINVAL
+    assert L.tlm_destroy(None) == _lib.TLM_OK
+    assert L.tlm_current_step(None) == -1
+    assert b"null" in L.tlm_last_error(None)
+
+
+def test_no_device_fails_loudly(built):
+    """Without a CUDA device every compute entry point refuses: there is no
+    CPU path to fall back to."""
+    L = _lib.load()
+    h = C.c_void_p()
+    st = L.tlm_create(C.byref(h), 0)
+    if st == _lib.TLM_OK:
+        L.tlm_destroy(h)
+        pytest.skip("a GPU is present")
+    assert st == _lib.TLM_ENODEV
+    assert L.tlm_last_error(None)
+    e = C.c_float()
+    assert L.tlm_scatter_unitarity_error(0, C.byref(e)) == _lib.TLM_ENODEV

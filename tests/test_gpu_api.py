@@ -1,0 +1,116 @@
+"""Behaviour of the C ABI around the time loop, on a B200: run / stop /
+resume, error statuses, the FP64 port DFT and the energy history."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from emsolver_b200 import MatProps, TlmConfig, TlmSolver, VoxelGridSpec, WaveformType, workloads
+from emsolver_b200._lib import TLM_EINVAL, TLM_ESTATE, TlmError
+from emsolver_b200.runner import build_solver, records
+from emsolver_b200.solver import s11_from_dft
+
+pytestmark = pytest.mark.gpu
+
+
+def small_dipole(steps=600):
+    return workloads.dipole(24, 20, 40, 21, slab=(2, 6, 3.0), steps=steps, nfreq=16)
+
+
+def test_run_to_total_steps(built):
+    w = small_dipole(300)
+    s = build_solver(w)
+    assert s.run() is True
+    assert s.currentStep() == 300 and s.isFinished() and not s.isRunning()
+    assert s.port(0).vRec.shape == (300,)
+    st, ev = s.getEnergyHistory()
+    assert np.array_equal(st, np.arange(0, 300, 16))
+    assert np.all(np.isfinite(ev)) and ev.max() > 0
+
+
+def test_stop_and_resume_equals_uninterrupted(built):
+    """requestStop from another thread ends run() between launch windows; the
+    stop flag stays set until the next setup (TlmSolver.h:219, :459), so a
+    second run() returns at once; stepping the rest gives exactly the
+    uninterrupted result."""
+    total = 20000
+    w = workloads.plain_free_space(n=96, steps=total)
+    ref = build_solver(w)
+    ref.run()
+    s = build_solver(w)
+    done = []
+    th = threading.Thread(target=lambda: done.append(s.run()))
+    th.start()
+    t0 = time.time()
+    while s.currentStep() == 0 and time.time() - t0 < 60:
+        time.sleep(0.001)
+    s.requestStop()
+    th.join(timeout=120)
+    assert done and done[0] is False
+    stopped_at = s.currentStep()
+    assert 0 < stopped_at < total
+    assert s.run() is False and s.currentStep() == stopped_at
+    s.step(total - stopped_at)
+    a, b = records(s, w), records(ref, w)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_errors_are_reported(built):
+    s = TlmSolver()
+    g = VoxelGridSpec(6, 6, 6)
+    mat = np.zeros(216, np.uint8)
+    mat[10] = 5  # id 5 -> table[3], table has 1 entry
+    with pytest.raises(TlmError) as e:
+        s.setup(g, mat, [MatProps(2.0, 0.0)], TlmConfig())
+    assert e.value.status == TLM_EINVAL
+    s.setup(g, np.zeros(216, np.uint8), [], TlmConfig(totalSteps=10))
+    with pytest.raises(TlmError) as e:
+        s.addPort([0], 2, 1.0)      # current loop leaves the grid
+    assert e.value.status == TLM_EINVAL
+    assert s.addProbe((1.0, 1.0, 1.0)) == -1   # outside: -1, like the reference
+    assert s.addPort([g.cellIndex(3, 3, 3)], 2, 1.0) == 0
+    assert s.addPort([1 + 6 * 3 + 36 * 3, 10 ** 9], 0, 1.0) == 1   # out-of-range cell dropped
+    s.step(3)
+    with pytest.raises(TlmError) as e:
+        s.addProbe((0.001, 0.001, 0.001))
+    assert e.value.status == TLM_ESTATE
+
+
+def test_port_dft_matches_record_dft(built):
+    w = small_dipole(800)
+    s = build_solver(w)
+    s.step(w.steps)
+    v, i = s.portDft(0)
+    port = s.port(0, f64=True)
+    dt = float(np.float32(s.timestep()))
+    n = np.arange(w.steps)
+    for fi, f in enumerate(w.dft_freqs):
+        e = np.exp(-1j * 2 * np.pi * f * dt * n)
+        vr = np.sum(port.vRec * e)
+        ir = np.sum(port.iRec * e)
+        assert abs(v[fi] - vr) <= 1e-9 * max(abs(vr), 1e-30)
+        assert abs(i[fi] - ir) <= 1e-9 * max(abs(ir), 1e-30)
+    z, s11 = s11_from_dft(v, i)
+    assert np.all(np.isfinite(z))
+
+
+def test_kernel_timing_counts_launches(built):
+    w = small_dipole(100)
+    s = build_solver(w)
+    s.setKernelTiming(True)
+    s.step(100)
+    ms, n = s.kernelTime()
+    assert n == 100 and ms > 0
+    assert s.deviceBytes() > 0
+
+
+def test_table_waveform_and_zero_steps(built):
+    w = workloads.heterogeneous(n=24, steps=40, nprobes=2)
+    s = build_solver(w)
+    s.step(0)
+    assert s.currentStep() == 0
+    s.step(40)
+    assert s.probe(0).ez.shape == (40,)
+    assert s.cfg().waveform == WaveformType.Table

@@ -1,0 +1,174 @@
+"""CUDA path vs the reference (through the C ABI), on a B200.
+
+Bar (FP32 storage): bitwise equality with the reference's own CPU step for
+pulses, stub pulses, port V/I and probe E records and the material tables;
+probe series of the full-size configurations within 1e-5 of their peak (the
+stated tolerance; in practice they are equal). Energy history (an FP64 sum
+whose order differs from the reference's per-thread chunks): relative 1e-6.
+FP64 storage mode vs the FP64 oracle: bitwise. BF16/FP16 storage vs the FP64
+oracle: bounded relative error (see the thresholds below).
+"""
+import numpy as np
+import pytest
+
+from tests.conftest import golden
+from emsolver_b200 import TlmSolver, workloads
+from emsolver_b200.runner import build_solver, records
+from emsolver_b200.solver import Storage
+from oracle import Oracle, drive
+from tests.golden.cases import small_cases
+
+pytestmark = pytest.mark.gpu
+
+CASES = small_cases()
+ENERGY_RTOL = 1e-6
+PROBE_TOL = 1e-5   # max |diff| relative to the series peak
+
+
+def run_gpu(w, storage=0, spl=0, variant=None, steps=None):
+    s = build_solver(w, storage=storage, steps_per_launch=spl, variant=variant)
+    s.step(w.steps if steps is None else steps)
+    return s
+
+
+def run_oracle(w, fp64=False, steps=None):
+    S = Oracle(fp64=fp64)
+    drive.setup(S, w)
+    if "plane_wave" in w.meta:
+        S.add_plane_wave(*w.meta["plane_wave"])
+    drive.advance(S, w, w.steps if steps is None else steps)
+    return S
+
+
+def assert_energy_close(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    assert a.shape == b.shape
+    scale = max(np.abs(b).max(), 1e-300)
+    assert np.abs(a - b).max() <= ENERGY_RTOL * scale
+
+
+def assert_series_close(a, b, tol=PROBE_TOL):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    assert a.shape == b.shape
+    peak = np.abs(b).max()
+    assert np.abs(a - b).max() <= tol * peak, (np.abs(a - b).max(), peak)
+
+
+def test_device_unitarity_kats_match_reference(built):
+    e = TlmSolver.ScatterUnitarityError()
+    d = TlmSolver.DielScatterUnitarityError(3.0)
+    assert e < 1e-5 and d < 1e-4
+    assert np.float32(e) == np.float32(Oracle.scatter_unitarity(False))
+    assert np.float32(d) == np.float32(Oracle.stub_unitarity(3.0, False))
+
+
+@pytest.mark.parametrize("variant", ["", "checked"])
+@pytest.mark.parametrize("w", CASES, ids=[w.name for w in CASES])
+def test_small_cases_bitwise(built, w, variant):
+    g = golden(w.name)
+    s = run_gpu(w, variant=variant)
+    assert np.array_equal(s.pulses(), g["pulses"])
+    assert np.array_equal(s.stubs()[: g["stubs"].size], g["stubs"]) if g["stubs"].size else True
+    y, gh = s.tables()
+    assert np.array_equal(y, g["yhat"]) and np.array_equal(gh, g["ghat"])
+    assert np.array_equal(s.materials(), w.mat)
+    rec = records(s, w)
+    for k, v in rec.items():
+        if k == "energy":
+            assert_energy_close(v, g[k])
+        elif k == "energy_steps":
+            assert np.array_equal(v, g[k])
+        else:
+            assert np.array_equal(v, g[k]), k
+
+
+@pytest.mark.parametrize("spl", [1, 5, 16, 100])
+def test_launch_window_does_not_change_results(built, spl):
+    w = CASES[3]
+    base = run_gpu(w, spl=64)
+    s = run_gpu(w, spl=spl)
+    assert np.array_equal(s.pulses(), base.pulses())
+    ra, rb = records(s, w), records(base, w)
+    for k in ra:
+        assert np.array_equal(ra[k], rb[k]), k
+
+
+def test_plain_free_space_vs_reference(built):
+    w = workloads.plain_free_space()
+    g = golden("plain_free_space")
+    s = run_gpu(w)
+    rec = records(s, w)
+    assert_series_close(rec["probe0_ez"], g["probe0_ez"])
+    assert np.array_equal(rec["probe0_ez"], g["probe0_ez"])
+    for k in ("probe0_ex", "probe0_ey", "port0_v", "port0_i"):
+        assert np.array_equal(rec[k], g[k]), k
+    assert_energy_close(rec["energy"], g["energy"])
+
+
+def test_heterogeneous_vs_reference(built):
+    w = workloads.heterogeneous()
+    g = golden("heterogeneous")
+    s = run_gpu(w)
+    y, gh = s.tables()
+    assert np.array_equal(y, g["yhat"]) and np.array_equal(gh, g["ghat"])
+    assert np.array_equal(s.materials(), w.mat)
+    rec = records(s, w)
+    for q in range(8):
+        for c in ("ex", "ey", "ez"):
+            assert_series_close(rec[f"probe{q}_{c}"], g[f"probe{q}_{c}"])
+    assert_series_close(rec["port0_v"], g["port0_v"])
+    assert_series_close(rec["port0_i"], g["port0_i"])
+    assert_energy_close(rec["energy"], g["energy"])
+
+
+def test_set_pulses_then_step_matches_oracle(built):
+    w = CASES[4]
+    rng = np.random.default_rng(3)
+    v0 = rng.standard_normal(w.ncells * 12).astype(np.float32)
+    v0.reshape(-1, 12)[w.mat == 1] = 0.0
+    s = build_solver(w)
+    s.setPulses(v0)
+    assert np.array_equal(s.pulses(), v0)
+    O = Oracle(False)
+    drive.setup(O, w)
+    O.set_pulses(v0)
+    s.step(25)
+    drive.advance(O, w, 25)
+    assert np.array_equal(s.pulses(), O.pulses())
+    ra, ro = records(s, w), drive.records(O, w)
+    for k in ra:
+        if k.startswith("energy"):
+            continue
+        assert np.array_equal(ra[k], ro[k]), k
+
+
+@pytest.mark.parametrize("w", CASES[:4], ids=[w.name for w in CASES[:4]])
+def test_fp64_storage_matches_fp64_oracle(built, w):
+    s = run_gpu(w, storage=Storage.F64)
+    O = run_oracle(w, fp64=True)
+    assert np.array_equal(s.pulses(f64=True), O.pulses())
+    ra, ro = records(s, w, f64=True), drive.records(O, w)
+    for k in ra:
+        if k == "energy":
+            assert_energy_close(ra[k], ro[k])
+        elif k != "energy_steps":
+            assert np.array_equal(ra[k], ro[k]), k
+
+
+@pytest.mark.parametrize("storage,tol", [(Storage.F16, 5e-3), (Storage.BF16, 3e-2)])
+def test_half_storage_error_vs_fp64_oracle(built, storage, tol):
+    """Pulses stored in FP16 / BF16 with FP32 arithmetic: probe series within
+    `tol` (max |diff| relative to the series peak) of the FP64 oracle."""
+    w = CASES[3]
+    s = run_gpu(w, storage=storage)
+    O = run_oracle(w, fp64=True)
+    ra, ro = records(s, w), drive.records(O, w)
+    worst = 0.0
+    for q in range(len(w.probes_cell)):
+        for c in ("ex", "ey", "ez"):
+            a = ra[f"probe{q}_{c}"].astype(np.float64)
+            b = ro[f"probe{q}_{c}"]
+            worst = max(worst, np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+    assert worst <= tol, worst
