@@ -58,6 +58,7 @@ SIGNATURES = {
                         _P(ConfigC)]),
     "tlm_add_port": (_st, [_h, _P(C.c_uint64), C.c_int, C.c_int, C.c_float, _P(C.c_int)]),
     "tlm_add_plane_wave": (_st, [_h, C.c_int, C.c_int, C.c_int, C.c_float]),
+    "tlm_add_source_cells": (_st, [_h, _P(C.c_uint64), C.c_int, C.c_int, C.c_float]),
     "tlm_add_probe": (_st, [_h, C.c_float, C.c_float, C.c_float, _P(C.c_int)]),
     "tlm_add_probe_cell": (_st, [_h, C.c_int, C.c_int, C.c_int, _P(C.c_int)]),
     "tlm_set_source_table": (_st, [_h, _P(C.c_float), C.c_int]),

@@ -938,6 +938,18 @@ tlm_status tlm_add_plane_wave(tlm_handle h, int prop_axis, int plane_index, int 
     return TLM_OK;
 }
 
+tlm_status tlm_add_source_cells(tlm_handle h, const uint64_t *cells, int n_cells, int pol_axis,
+                                float amp)
+{
+    TLM_TRY(checkAddable(h));
+    if (pol_axis < 0 || pol_axis > 2) return h->fail(TLM_EINVAL, "pol_axis must be 0, 1 or 2");
+    if (n_cells < 0 || (n_cells > 0 && !cells)) return h->fail(TLM_EINVAL, "bad cell list");
+    for (int t = 0; t < n_cells; ++t)
+        if (cells[t] < (uint64_t)h->ncell && h->mat[cells[t]] == TLM_MAT_AIR)
+            h->sources.push_back({ cells[t], pol_axis, amp });
+    return TLM_OK;
+}
+
 tlm_status tlm_add_probe(tlm_handle h, float x, float y, float z, int *out_idx)
 {
     TLM_TRY(checkAddable(h));

@@ -333,6 +333,10 @@ __global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
                 }
                 else
                 {
+                    // A PEC node's pulses are identically zero in the
+                    // reference (never scattered, never connected), so its
+                    // samples are zero; the gathered values are discarded.
+                    const bool on = (nodeLive >> c) & 1u;
                     R v[12];
 #pragma unroll
                     for (int s = 0; s < 12; ++s)
@@ -341,6 +345,7 @@ __global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
 #pragma unroll
                         for (int cc = 1; cc < V; ++cc)
                             if (cc == c) v[s] = inc[s][cc];
+                        v[s] = on ? v[s] : R(0);
                     }
                     R *dst = a.samples + (long long)se.arg * 6;
 #pragma unroll

@@ -194,6 +194,11 @@ class TlmSolver:
     def addPlaneWave(self, propAxis: int, planeIndex: int, polAxis: int, amp: float):
         self._c(self._L.tlm_add_plane_wave(self._h, propAxis, planeIndex, polAxis, amp))
 
+    def addSourceCells(self, cells, polAxis: int, amp: float):
+        """Soft sources cell by cell (the reference's SourceCell list)."""
+        arr = np.ascontiguousarray(cells, dtype=np.uint64).reshape(-1)
+        self._c(self._L.tlm_add_source_cells(self._h, _fp(arr, C.c_uint64), arr.size, polAxis, amp))
+
     def addProbe(self, worldPos) -> int:
         idx = C.c_int(-1)
         x, y, z = (float(v) for v in worldPos)

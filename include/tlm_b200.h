@@ -149,6 +149,12 @@ TLM_API tlm_status tlm_add_port(tlm_handle h, const uint64_t *cells, int n_cells
 TLM_API tlm_status tlm_add_plane_wave(tlm_handle h, int prop_axis, int plane_index,
                                       int pol_axis, float amp);
 
+/* Append soft sources one cell at a time: the reference's SourceCell list
+ * (TlmSolver.h:72-77, filled by addPlaneWave). For callers that hold that
+ * list, e.g. a RunGpuTlm seam (GpuTlm.h:15). Non-air cells are dropped. */
+TLM_API tlm_status tlm_add_source_cells(tlm_handle h, const uint64_t *cells, int n_cells,
+                                        int pol_axis, float amp);
+
 /* TlmSolver::addProbe (TlmSolver.cpp:377-391): *out_idx = -1 when the world
  * point is outside the grid (status TLM_OK, like the reference). */
 TLM_API tlm_status tlm_add_probe(tlm_handle h, float x, float y, float z, int *out_idx);
