@@ -98,6 +98,9 @@ SIGNATURES = {
     "tlm_waveform_value": (_st, [C.c_int, C.c_float, C.c_float, C.c_int, _P(C.c_float)]),
     "tlm_scatter_unitarity_error": (_st, [C.c_int, _P(C.c_float)]),
     "tlm_stub_unitarity_error": (_st, [C.c_int, C.c_float, _P(C.c_float)]),
+    "tlm_step_planes_noalloc": (_st, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
+                                      C.c_void_p, C.c_void_p]),
     "tlm_get_stream": (_st, [_h, _P(C.c_void_p)]),
     "tlm_device_bytes": (_st, [_h, _P(C.c_size_t)]),
     "tlm_set_kernel_timing": (_st, [_h, C.c_int]),

@@ -81,6 +81,10 @@ float pow2Ceil(float v)
 
 } // namespace
 
+// Lets other translation units of the library report a failure of a call
+// that has no handle through tlm_last_error(NULL).
+void tlmSetThreadError(const std::string &m) { g_threadError = m; }
+
 struct tlm_solver
 {
     int device = 0;

@@ -253,6 +253,44 @@ TLM_API tlm_status tlm_waveform_value(int waveform, float f0, float dl, int n, f
 TLM_API tlm_status tlm_scatter_unitarity_error(int device, float *err);
 TLM_API tlm_status tlm_stub_unitarity_error(int device, float epsr, float *err);
 
+/* ---- one step over caller-owned device memory, no allocation -------- */
+
+/* No counterpart in the reference. For callers that may not allocate device
+ * memory: a host application that reserves the GPU's memory in its own pool
+ * and hands this library only buffers it owns, or a time-critical loop that
+ * must not pay the device-wide synchronisation cudaMalloc/cudaFree can
+ * cause. It advances one FP32 step over planes the caller owns and calls no
+ * cudaMalloc, cudaFree or other allocating routine.
+ *
+ * Layout (all pointers are device pointers): px = nx rounded up to a
+ * multiple of 8, P = px*ny*nz; plane s (0..11, slot axis*4 + side*2 + pol)
+ * starts at element s*P; node (i,j,k) is element (k*ny + j)*px + i.
+ * mat has P bytes, padding columns (i >= nx) must be TLM_MAT_PEC and their
+ * pulses zero. in_planes holds the reflected pulses of the previous step
+ * (or, with input_is_incident != 0, incident pulses such as the reference's
+ * V re-laid out); out_planes (12*P floats, not aliasing in_planes) receives
+ * the reflected pulses of this step: pass it as in_planes of the next call.
+ * stubs: 3 planes read and written on dielectric nodes (NULL if mat has no
+ * id >= 2). yhat/ghat: per dielectric id (id - 2). No sources or monitors.
+ * energy_out (NULL to skip): the FP64 sum of the squares of all incident
+ * link pulses of this step. Planes 16-byte aligned, mat 4-byte aligned.
+ * Work is queued on `stream` (a cudaStream_t, NULL = default stream).
+ *
+ * Limits and sharing: its only scratch, one FP64 energy partial per thread
+ * block, is a fixed 512 KiB static device array that every GPU loading this
+ * library holds until the process exits; grids above 67,108,864 padded
+ * nodes are rejected with TLM_EINVAL. The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture. Every call shares the array, so calls that
+ * overlap on the GPU (other streams, other threads) race: serialise them.
+ * Each call overwrites the partials it uses; nothing needs clearing.
+ * Errors: status code, message in tlm_last_error(NULL). */
+TLM_API tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_planes,
+                                           float *stubs, const uint8_t *mat, const float *yhat,
+                                           const float *ghat, int nx, int ny, int nz, float rho,
+                                           int input_is_incident, double *energy_out,
+                                           void *stream);
+
 /* ---- bench / integration helpers ------------------------------------ */
 
 /* The handle's CUDA stream (cudaStream_t) for event timing by the caller. */
