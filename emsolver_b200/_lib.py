@@ -40,7 +40,8 @@ class ConfigC(C.Structure):
     _fields_ = [("f0", C.c_float), ("waveform", C.c_int), ("total_steps", C.c_int),
                 ("settle_steps", C.c_int), ("boundary_rho", C.c_float), ("huy_offset", C.c_int),
                 ("use_gpu", C.c_int), ("record_every", C.c_int), ("storage", C.c_int),
-                ("pulse_scale", C.c_float), ("steps_per_launch", C.c_int)]
+                ("pulse_scale", C.c_float), ("steps_per_launch", C.c_int),
+                ("kernel_variant", C.c_int), ("rounding", C.c_int)]
 
 
 _h = C.c_void_p
@@ -101,6 +102,8 @@ SIGNATURES = {
     "tlm_step_planes_noalloc": (_st, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
                                       C.c_void_p, C.c_void_p]),
+    "tlm_kernel_variants": (C.c_int, [C.c_int]),
+    "tlm_kernel_variant_info": (_st, [C.c_int, C.c_int, _P(C.c_int), _P(C.c_int)]),
     "tlm_get_stream": (_st, [_h, _P(C.c_void_p)]),
     "tlm_device_bytes": (_st, [_h, _P(C.c_size_t)]),
     "tlm_set_kernel_timing": (_st, [_h, C.c_int]),

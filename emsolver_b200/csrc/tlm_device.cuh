@@ -29,31 +29,42 @@ constexpr int kPadX = 8;     // row pitch multiple (every vector width divides i
 
 enum : uint8_t { kAir = 0, kPec = 1, kDiel0 = 2 };
 
-// Storage type S -> arithmetic type R, nodes per thread V (one aligned
-// vector load per plane), and whether stored values carry a per-grid scale.
+// Storage type S -> arithmetic type R, default nodes per thread V (one
+// aligned vector load per plane) and resident blocks per SM the default
+// kernel is compiled for, whether the default kernel scatters with the
+// warp-uniform select (else a per-node branch) -- the fastest choices
+// measured on B200 -- and whether stored values carry a per-grid scale.
 template <class S> struct Traits;
 template <> struct Traits<float>
 {
     using R = float;
     static constexpr int V = 4;
+    static constexpr int kMinBlocks = 3;
+    static constexpr bool kSelect = false;
     static constexpr bool kScaled = false;
 };
 template <> struct Traits<double>
 {
     using R = double;
-    static constexpr int V = 2;
+    static constexpr int V = 1;
+    static constexpr int kMinBlocks = 4;
+    static constexpr bool kSelect = true;
     static constexpr bool kScaled = false;
 };
 template <> struct Traits<__half>
 {
     using R = float;
     static constexpr int V = 4;
+    static constexpr int kMinBlocks = 3;
+    static constexpr bool kSelect = false;
     static constexpr bool kScaled = true;
 };
 template <> struct Traits<__nv_bfloat16>
 {
     using R = float;
     static constexpr int V = 4;
+    static constexpr int kMinBlocks = 3;
+    static constexpr bool kSelect = false;
     static constexpr bool kScaled = true;
 };
 
@@ -81,6 +92,53 @@ template <> __device__ __forceinline__ __nv_bfloat16 encode<__nv_bfloat16>(float
 }
 template <class S> __device__ __forceinline__ S encode(double v, double);
 template <> __device__ __forceinline__ double encode<double>(double v, double) { return v; }
+
+// 32-bit integer mixer (the MurmurHash3 finaliser): counter-based random
+// bits for stochastic rounding, a pure function of (node, slot, step).
+__host__ __device__ __forceinline__ unsigned mix32(unsigned h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// Stochastic rounding to the storage type: round the magnitude up with
+// probability equal to the fraction of the gap it covers, so the rounding
+// error has zero mean. r supplies 32 random bits.
+template <class S> __device__ __forceinline__ S encodeStochastic(float v, float inv, unsigned r);
+template <> __device__ __forceinline__ float encodeStochastic<float>(float v, float, unsigned)
+{
+    return v;
+}
+template <> __device__ __forceinline__ __nv_bfloat16 encodeStochastic<__nv_bfloat16>(float v, float inv,
+                                                                                     unsigned r)
+{
+    // bfloat16 keeps the upper 16 bits of the float: adding 16 random bits to
+    // the discarded half before truncating rounds the magnitude up with the
+    // right probability (a carry moves into the next binade correctly).
+    unsigned u = __float_as_uint(v * inv);
+    if ((u & 0x7f800000u) != 0x7f800000u) u += (r >> 16);
+    return __ushort_as_bfloat16((unsigned short)(u >> 16));
+}
+template <> __device__ __forceinline__ __half encodeStochastic<__half>(float v, float inv, unsigned r)
+{
+    const float x = v * inv;
+    const __half lo = __float2half_rz(x);  // toward zero
+    const float xl = __half2float(lo);
+    if (xl == x) return lo;
+    const __half hi = __ushort_as_half((unsigned short)(__half_as_ushort(lo) + 1));  // away from zero
+    const float xh = __half2float(hi);
+    const float frac = (x - xl) / (xh - xl);                 // in (0, 1)
+    const float u = (float)(r >> 8) * (1.0f / 16777216.0f);  // uniform in [0, 1)
+    return (u < frac) ? hi : lo;
+}
+template <> __device__ __forceinline__ double encodeStochastic<double>(float v, float, unsigned)
+{
+    return v;
+}
 
 // Slot helpers (compile-time after unrolling).
 __host__ __device__ constexpr int firstTransverse(int axis) { return axis == 0 ? 1 : 0; }
@@ -165,6 +223,33 @@ __device__ __forceinline__ void scatterStub(const R (&in)[12], R (&vs)[3], R yh,
     reflectLinks(in, Vn, ZI, out);
 #pragma unroll
     for (int j = 0; j < 3; ++j) vs[j] = Vn[j] - vs[j];
+}
+
+// Scatter of a node that may be air or stub-loaded, without a branch: the
+// node voltage is selected between the air formula (TlmSolver.cpp:46-52)
+// and the stub formula (TlmSolver.cpp:86-98), so each node gets exactly the
+// value its own formula rounds to; stubs are updated only when `diel`.
+template <class R>
+__device__ __forceinline__ void scatterSelect(const R (&in)[12], R (&vs)[3], R yh, R gh, bool diel,
+                                              R (&out)[12])
+{
+    R Vn[3], ZI[3];
+    const R den = (R(4) + yh) + gh;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+    {
+        const int a = (j == 0) ? 1 : 0;
+        const int b = (j == 2) ? 1 : 2;
+        const R sum4 = ((in[slotOf(a, 0, j)] + in[slotOf(a, 1, j)]) + in[slotOf(b, 0, j)]) +
+                       in[slotOf(b, 1, j)];
+        const R vStub = (R(2) * (sum4 + yh * vs[j])) / den;
+        Vn[j] = diel ? vStub : R(0.5) * sum4;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ZI[k] = circulation(in, k);
+    reflectLinks(in, Vn, ZI, out);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) vs[j] = diel ? Vn[j] - vs[j] : vs[j];
 }
 
 // A source or monitor attached to one node. Entries are sorted by node

@@ -1,0 +1,237 @@
+// tlm_internal.h -- internals shared by the translation units of the library
+// (the solver handle, its helpers); not part of the C ABI.
+#pragma once
+
+#include "tlm_b200.h"
+#include "tlm_device.cuh"
+
+#include <atomic>
+#include <string>
+#include <vector>
+
+namespace tlmi {
+struct PortInfo
+{
+    std::vector<uint64_t> cells;  // kept (air) cells, caller order
+    int pol = 2;
+    float amp = 1.0f;
+    long long nb[4] = { -1, -1, -1, -1 };  // reference linear indices of the current loop
+};
+struct SourceInfo
+{
+    uint64_t cell;
+    int pol;
+    float amp;
+};
+
+// Scoped device selection that restores the caller's current device.
+struct DeviceGuard
+{
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+inline size_t storageBytes(int storage)
+{
+    switch (storage)
+    {
+    case TLM_STORE_F64: return 8;
+    case TLM_STORE_BF16:
+    case TLM_STORE_F16: return 2;
+    default: return 4;
+    }
+}
+inline size_t realBytes(int storage) { return storage == TLM_STORE_F64 ? 8 : 4; }
+
+// Step-kernel tile shapes per storage mode: {nodes per thread, min blocks
+// per SM}. Entry 0 is the default; the autotuner and kernel_variant pick
+// among them.
+struct Shape
+{
+    int V, minb;
+    int select;  // 1: warp-uniform select between air and stub scatter; 0: per-node branch
+};
+constexpr Shape kShapesF32[] = { { 4, 3, 0 }, { 4, 3, 1 }, { 2, 4, 1 }, { 4, 2, 0 } };
+constexpr Shape kShapesF64[] = { { 1, 4, 1 }, { 1, 4, 0 }, { 2, 3, 0 } };
+constexpr Shape kShapesHalf[] = { { 4, 3, 0 }, { 4, 3, 1 }, { 2, 4, 1 }, { 8, 2, 0 } };
+
+inline int shapeCount(int storage)
+{
+    switch (storage)
+    {
+    case TLM_STORE_F64: return 3;
+    case TLM_STORE_BF16:
+    case TLM_STORE_F16: return 4;
+    case TLM_STORE_F32: return 4;
+    default: return 0;
+    }
+}
+inline Shape shapeOf(int storage, int variant)
+{
+    switch (storage)
+    {
+    case TLM_STORE_F64: return kShapesF64[variant];
+    case TLM_STORE_BF16:
+    case TLM_STORE_F16: return kShapesHalf[variant];
+    default: return kShapesF32[variant];
+    }
+}
+
+} // namespace tlmi
+
+struct tlm_solver
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    std::atomic<bool> running{ false };
+    std::atomic<bool> finished{ false };
+    std::atomic<bool> stopFlag{ false };
+    std::atomic<int> doneStep{ 0 };
+    std::atomic<float> energy{ 0.0f };
+
+    // configuration
+    bool configured = false;
+    tlm_grid g{};
+    tlm_config cfg{};
+    int storage = TLM_STORE_F32;
+    std::vector<uint8_t> mat;
+    std::vector<float> epsr, sigma;
+    std::vector<float> yhat32, ghat32;
+    std::vector<double> yhat64, ghat64;
+    int nx = 0, ny = 0, nz = 0, px = 0, V = 4, nq = 0;
+    long long P = 0, ncell = 0, nquads = 0;
+    int nblocks = 0;
+    bool anyDiel = false;
+    float dt32 = 0.0f;
+    double dt64 = 0.0;
+    float scale = 1.0f;
+    int window = 64;
+    int variant = 0;
+
+    // sources and monitors
+    std::vector<tlmi::SourceInfo> sources;
+    std::vector<tlmi::PortInfo> ports;
+    std::vector<uint64_t> probeCells;
+    std::vector<float> svTable;
+    std::vector<double> dftFreqs;
+    bool prepared = false;
+    int nsamp = 0;
+
+    // time-loop state
+    int curStep = 0;       // steps enqueued
+    int curBuf = 0;        // pulse buffer holding the current state
+    bool stateIncident = false;
+
+    // device memory
+    void *dPulses[2] = { nullptr, nullptr };
+    void *dStub = nullptr;
+    uint8_t *dMat = nullptr;
+    void *dYhat = nullptr, *dGhat = nullptr;
+    tlmk::SpecEntry *dSpec = nullptr;
+    int *dTile = nullptr;
+    void *dSamples = nullptr;
+    double *dEpart = nullptr;
+    int *dPortOff = nullptr, *dPortSlots = nullptr, *dPortPol = nullptr, *dPortNb = nullptr;
+    int *dProbeSlot = nullptr;
+    double *dVrec = nullptr, *dIrec = nullptr, *dPrec = nullptr;
+    long long recCap = 0;
+    double *dEhist = nullptr;
+    double *dElatest = nullptr;
+    double *dWdt = nullptr, *dDft = nullptr;
+    unsigned *dFault = nullptr;
+    size_t devBytes = 0;
+
+    // kernel timing
+    bool timing = false;
+    std::vector<cudaEvent_t> evs;
+    size_t evUsed = 0;
+
+    tlm_status fail(tlm_status s, const std::string &m)
+    {
+        err = m;
+        return s;
+    }
+    tlm_status cuda(cudaError_t e, const char *what)
+    {
+        if (e == cudaSuccess) return TLM_OK;
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? TLM_ENOMEM : TLM_ECUDA;
+    }
+};
+
+#define TLM_TRY(expr)                                  \
+    do                                                 \
+    {                                                  \
+        tlm_status _s = (expr);                        \
+        if (_s != TLM_OK) return _s;                   \
+    } while (0)
+#define TLM_CU(h, call) TLM_TRY((h)->cuda((call), #call))
+
+namespace tlmi {
+
+template <class T> tlm_status devAlloc(tlm_solver *h, T **p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) return TLM_OK;
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        return h->fail(TLM_ENOMEM, "cudaMalloc of " + std::to_string(bytes) +
+                                       " bytes failed: " + cudaGetErrorString(e));
+    }
+    h->devBytes += bytes;
+    *p = static_cast<T *>(q);
+    return TLM_OK;
+}
+
+// Short-lived buffers of one API call (not counted in the handle's bytes).
+template <class T> tlm_status tmpAlloc(tlm_solver *h, T **p, size_t bytes)
+{
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes > 0 ? bytes : 1);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        *p = nullptr;
+        return h->fail(TLM_ENOMEM, std::string("temporary cudaMalloc failed: ") + cudaGetErrorString(e));
+    }
+    *p = static_cast<T *>(q);
+    return TLM_OK;
+}
+
+template <class T> void devFree(tlm_solver *h, T *&p)
+{
+    (void)h;
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+// Defined in tlm_solver.cu.
+void setThreadError(const std::string &m);
+void freeMonitors(tlm_solver *h);
+void freeAll(tlm_solver *h);
+bool busy(tlm_solver *h);
+double sourceValue(const tlm_solver *h, int n);
+long long paddedNode(const tlm_solver *h, uint64_t cell);
+tlm_status prepare(tlm_solver *h);
+tlm_status ensureRecords(tlm_solver *h, long long need);
+tlm_status syncState(tlm_solver *h);
+tlm_status checkHandle(tlm_solver *h);
+tlm_status checkReady(tlm_solver *h);
+tlm_status chooseScale(tlm_solver *h);
+int gridBlocksFor(long long n);
+
+} // namespace tlmi

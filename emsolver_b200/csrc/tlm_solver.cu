@@ -4,6 +4,7 @@
 // setup -> add ports / probes / plane waves -> step or run -> read records.
 // All device state is owned here; there is no CPU execution path.
 #include "tlm_b200.h"
+#include "tlm_internal.h"
 
 #include "tlm_aux_kernels.cuh"
 #include "tlm_host_math.h"
@@ -16,60 +17,19 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using tlmk::kBlock;
 using tlmk::kPadX;
 using tlmk::SpecEntry;
+using namespace tlmi;
 
 namespace {
 
 thread_local std::string g_threadError;
 
 const char *kVersion = "tlm_b200 0.1.0 (sm_100a)";
-
-struct PortInfo
-{
-    std::vector<uint64_t> cells;  // kept (air) cells, caller order
-    int pol = 2;
-    float amp = 1.0f;
-    long long nb[4] = { -1, -1, -1, -1 };  // reference linear indices of the current loop
-};
-struct SourceInfo
-{
-    uint64_t cell;
-    int pol;
-    float amp;
-};
-
-// Scoped device selection that restores the caller's current device.
-struct DeviceGuard
-{
-    int prev = -1;
-    explicit DeviceGuard(int dev)
-    {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard()
-    {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
-
-size_t storageBytes(int storage)
-{
-    switch (storage)
-    {
-    case TLM_STORE_F64: return 8;
-    case TLM_STORE_BF16:
-    case TLM_STORE_F16: return 2;
-    default: return 4;
-    }
-}
-size_t realBytes(int storage) { return storage == TLM_STORE_F64 ? 8 : 4; }
-int vecWidth(int storage) { return storage == TLM_STORE_F64 ? 2 : 4; }
 
 float pow2Ceil(float v)
 {
@@ -84,134 +44,16 @@ float pow2Ceil(float v)
 // Lets other translation units of the library report a failure of a call
 // that has no handle through tlm_last_error(NULL).
 void tlmSetThreadError(const std::string &m) { g_threadError = m; }
+namespace tlmi {
+void setThreadError(const std::string &m) { g_threadError = m; }
+} // namespace tlmi
 
-struct tlm_solver
-{
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
 
-    std::atomic<bool> running{ false };
-    std::atomic<bool> finished{ false };
-    std::atomic<bool> stopFlag{ false };
-    std::atomic<int> doneStep{ 0 };
-    std::atomic<float> energy{ 0.0f };
+namespace tlmi {
 
-    // configuration
-    bool configured = false;
-    tlm_grid g{};
-    tlm_config cfg{};
-    int storage = TLM_STORE_F32;
-    std::vector<uint8_t> mat;
-    std::vector<float> epsr, sigma;
-    std::vector<float> yhat32, ghat32;
-    std::vector<double> yhat64, ghat64;
-    int nx = 0, ny = 0, nz = 0, px = 0, V = 4, nq = 0;
-    long long P = 0, ncell = 0, nquads = 0;
-    int nblocks = 0;
-    bool anyDiel = false;
-    float dt32 = 0.0f;
-    double dt64 = 0.0;
-    float scale = 1.0f;
-    int window = 64;
 
-    // sources and monitors
-    std::vector<SourceInfo> sources;
-    std::vector<PortInfo> ports;
-    std::vector<uint64_t> probeCells;
-    std::vector<float> svTable;
-    std::vector<double> dftFreqs;
-    bool prepared = false;
-    int nsamp = 0;
 
-    // time-loop state
-    int curStep = 0;       // steps enqueued
-    int curBuf = 0;        // pulse buffer holding the current state
-    bool stateIncident = false;
 
-    // device memory
-    void *dPulses[2] = { nullptr, nullptr };
-    void *dStub = nullptr;
-    uint8_t *dMat = nullptr;
-    void *dYhat = nullptr, *dGhat = nullptr;
-    SpecEntry *dSpec = nullptr;
-    int *dTile = nullptr;
-    void *dSamples = nullptr;
-    double *dEpart = nullptr;
-    int *dPortOff = nullptr, *dPortSlots = nullptr, *dPortPol = nullptr, *dPortNb = nullptr;
-    int *dProbeSlot = nullptr;
-    double *dVrec = nullptr, *dIrec = nullptr, *dPrec = nullptr;
-    long long recCap = 0;
-    double *dEhist = nullptr;
-    double *dElatest = nullptr;
-    double *dWdt = nullptr, *dDft = nullptr;
-    unsigned *dFault = nullptr;
-    size_t devBytes = 0;
-
-    // kernel timing
-    bool timing = false;
-    std::vector<cudaEvent_t> evs;
-    size_t evUsed = 0;
-
-    tlm_status fail(tlm_status s, const std::string &m)
-    {
-        err = m;
-        return s;
-    }
-    tlm_status cuda(cudaError_t e, const char *what)
-    {
-        if (e == cudaSuccess) return TLM_OK;
-        err = std::string(what) + ": " + cudaGetErrorString(e);
-        return e == cudaErrorMemoryAllocation ? TLM_ENOMEM : TLM_ECUDA;
-    }
-};
-
-#define TLM_TRY(expr)                                  \
-    do                                                 \
-    {                                                  \
-        tlm_status _s = (expr);                        \
-        if (_s != TLM_OK) return _s;                   \
-    } while (0)
-#define TLM_CU(h, call) TLM_TRY((h)->cuda((call), #call))
-
-namespace {
-
-template <class T> tlm_status devAlloc(tlm_solver *h, T **p, size_t bytes)
-{
-    *p = nullptr;
-    if (bytes == 0) return TLM_OK;
-    void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, bytes);
-    if (e != cudaSuccess)
-    {
-        cudaGetLastError();
-        return h->fail(TLM_ENOMEM, "cudaMalloc of " + std::to_string(bytes) +
-                                       " bytes failed: " + cudaGetErrorString(e));
-    }
-    h->devBytes += bytes;
-    *p = static_cast<T *>(q);
-    return TLM_OK;
-}
-// Short-lived buffers of one API call (not counted in the handle's bytes).
-template <class T> tlm_status tmpAlloc(tlm_solver *h, T **p, size_t bytes)
-{
-    void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, bytes > 0 ? bytes : 1);
-    if (e != cudaSuccess)
-    {
-        cudaGetLastError();
-        *p = nullptr;
-        return h->fail(TLM_ENOMEM, std::string("temporary cudaMalloc failed: ") + cudaGetErrorString(e));
-    }
-    *p = static_cast<T *>(q);
-    return TLM_OK;
-}
-template <class T> void devFree(tlm_solver *h, T *&p)
-{
-    (void)h;
-    if (p) cudaFree((void *)p);
-    p = nullptr;
-}
 
 void freeMonitors(tlm_solver *h)
 {
@@ -415,6 +257,47 @@ tlm_status ensureRecords(tlm_solver *h, long long need)
     return TLM_OK;
 }
 
+template <class S, int V, int MINB, bool SEL>
+void launchWithShape(const tlmk::StepArgs<S> &a, bool incident, int nblocks, cudaStream_t st)
+{
+    if (incident)
+        tlmk::stepKernelShaped<S, V, MINB, true, SEL><<<nblocks, kBlock, 0, st>>>(a);
+    else
+        tlmk::stepKernelShaped<S, V, MINB, false, SEL><<<nblocks, kBlock, 0, st>>>(a);
+}
+
+// Launch the step kernel in the tile shape `variant` of the storage type
+// (variant 0 is stepKernel's default shape; the table is tlmi::kShapes*).
+template <class S>
+void launchShaped(const tlmk::StepArgs<S> &a, int variant, bool incident, int nblocks, cudaStream_t st)
+{
+    if (variant == 0)
+    {
+        if (incident)
+            tlmk::stepKernel<S, true><<<nblocks, kBlock, 0, st>>>(a);
+        else
+            tlmk::stepKernel<S, false><<<nblocks, kBlock, 0, st>>>(a);
+        return;
+    }
+    if constexpr (std::is_same<S, double>::value)
+    {
+        if (variant == 1) launchWithShape<S, 1, 4, false>(a, incident, nblocks, st);
+        else launchWithShape<S, 2, 3, false>(a, incident, nblocks, st);
+    }
+    else if constexpr (std::is_same<S, float>::value)
+    {
+        if (variant == 1) launchWithShape<S, 4, 3, true>(a, incident, nblocks, st);
+        else if (variant == 2) launchWithShape<S, 2, 4, true>(a, incident, nblocks, st);
+        else launchWithShape<S, 4, 2, false>(a, incident, nblocks, st);
+    }
+    else
+    {
+        if (variant == 1) launchWithShape<S, 4, 3, true>(a, incident, nblocks, st);
+        else if (variant == 2) launchWithShape<S, 2, 4, true>(a, incident, nblocks, st);
+        else launchWithShape<S, 8, 2, false>(a, incident, nblocks, st);
+    }
+}
+
 template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long eFirst)
 {
     using R = typename tlmk::Traits<S>::R;
@@ -455,10 +338,9 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
         h->evUsed += 2;
         TLM_CU(h, cudaEventRecord(e0, h->stream));
     }
-    if (h->stateIncident)
-        tlmk::stepKernel<S, true><<<h->nblocks, kBlock, 0, h->stream>>>(a);
-    else
-        tlmk::stepKernel<S, false><<<h->nblocks, kBlock, 0, h->stream>>>(a);
+    a.round_seed = tlmk::mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
+    a.stochastic = h->cfg.rounding == 1 ? 1 : 0;
+    launchShaped<S>(a, h->variant, h->stateIncident, h->nblocks, h->stream);
     TLM_CU(h, cudaGetLastError());
     if (h->timing) TLM_CU(h, cudaEventRecord(e1, h->stream));
     h->stateIncident = false;
@@ -659,7 +541,9 @@ template <class S> static tlm_status setPulsesT(tlm_solver *h, const float *in)
     return TLM_OK;
 }
 
-} // namespace
+} // namespace tlmi
+
+using namespace tlmi;
 
 // ======================================================================
 extern "C" {
@@ -681,6 +565,24 @@ void tlm_config_default(tlm_config *c)
     c->storage = TLM_STORE_F32;
     c->pulse_scale = 0.0f;
     c->steps_per_launch = 0;
+    c->kernel_variant = 0;
+    c->rounding = 0;
+}
+
+int tlm_kernel_variants(int storage) { return shapeCount(storage); }
+
+tlm_status tlm_kernel_variant_info(int storage, int variant, int *nodes_per_thread,
+                                   int *min_blocks_per_sm)
+{
+    if (variant < 0 || variant >= shapeCount(storage))
+    {
+        g_threadError = "no such kernel variant";
+        return TLM_EINVAL;
+    }
+    const Shape sh = shapeOf(storage, variant);
+    if (nodes_per_thread) *nodes_per_thread = sh.V;
+    if (min_blocks_per_sm) *min_blocks_per_sm = sh.minb;
+    return TLM_OK;
 }
 
 tlm_status tlm_create(tlm_handle *out, int device)
@@ -782,6 +684,9 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     if (cfg->waveform < 0 || cfg->waveform > TLM_WAVE_TABLE)
         return h->fail(TLM_EINVAL, "unknown waveform");
     if (cfg->total_steps < 0) return h->fail(TLM_EINVAL, "total_steps must be >= 0");
+    if (cfg->kernel_variant < 0 || cfg->kernel_variant >= shapeCount(cfg->storage))
+        return h->fail(TLM_EINVAL, "kernel_variant out of range for this storage mode");
+    if (cfg->rounding < 0 || cfg->rounding > 1) return h->fail(TLM_EINVAL, "rounding must be 0 or 1");
     if (!std::isfinite(cfg->boundary_rho)) return h->fail(TLM_EINVAL, "boundary_rho not finite");
     bool anyDiel = false;
     for (long long c = 0; c < n; ++c)
@@ -806,7 +711,8 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     h->nx = grid->nx;
     h->ny = grid->ny;
     h->nz = grid->nz;
-    h->V = vecWidth(h->storage);
+    h->variant = cfg->kernel_variant;
+    h->V = shapeOf(h->storage, h->variant).V;
     h->px = (h->nx + kPadX - 1) / kPadX * kPadX;
     h->nq = h->px / h->V;
     h->P = (long long)h->px * h->ny * h->nz;
@@ -999,7 +905,9 @@ tlm_status tlm_set_port_dft(tlm_handle h, const double *freqs, int n_freq)
     return TLM_OK;
 }
 
-static tlm_status chooseScale(tlm_solver *h)
+} // extern "C"
+
+tlm_status tlmi::chooseScale(tlm_solver *h)
 {
     if (h->storage != TLM_STORE_F16 && h->storage != TLM_STORE_BF16)
     {
@@ -1027,6 +935,9 @@ static tlm_status chooseScale(tlm_solver *h)
     h->scale = h->storage == TLM_STORE_F16 ? pow2Ceil(peak) / 1024.0f : 1.0f;
     return TLM_OK;
 }
+
+extern "C" {
+
 
 tlm_status tlm_step_async(tlm_handle h, int n_steps)
 {

@@ -41,6 +41,8 @@ template <class S> struct StepArgs
     R *__restrict__ samples;       // [nsamp][6] of this step
     double *__restrict__ epart;    // [gridDim.x] energy partials (energy steps)
     unsigned int *__restrict__ fault;  // bounds-check record (checked builds)
+    unsigned int round_seed;       // per-step seed of stochastic rounding
+    int stochastic;                // BF16/F16: round stochastically
 };
 
 #ifdef TLM_CHECKED
@@ -76,17 +78,18 @@ template <int V> __device__ __forceinline__ unsigned pecMask(const uint8_t (&m)[
     return r;
 }
 
-// kIncident: the input planes hold INCIDENT pulses (state written by
-// tlm_set_pulses) instead of reflected ones; the gather is skipped.
-template <class S, bool kIncident>
-__global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
+// One tile of kBlock threads x V nodes: tile `tile` covers the V-node
+// groups [tile*kBlock, (tile+1)*kBlock). `red` is kBlock/32 doubles of
+// shared memory. kIncident: the input planes hold INCIDENT pulses (state
+// written by tlm_set_pulses) instead of reflected ones; the gather is
+// skipped.
+template <class S, int V, bool kIncident, bool kSelect = true>
+__device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double *red)
 {
     using R = typename Traits<S>::R;
-    constexpr int V = Traits<S>::V;
-    __shared__ double red[kBlock / 32];
 
     const int lane = threadIdx.x & 31;
-    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    const long long q = (long long)tile * kBlock + threadIdx.x;
     const bool live = q < a.nquads;
     const long long qq = live ? q : 0;
     const int xq = (int)(qq % a.nq);
@@ -301,7 +304,7 @@ __global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
     // ---- sources and monitor samples (rare: only blocks that hold one) ----
     if (a.tile_begin != nullptr)
     {
-        const int b0 = a.tile_begin[blockIdx.x], b1 = a.tile_begin[blockIdx.x + 1];
+        const int b0 = a.tile_begin[tile], b1 = a.tile_begin[tile + 1];
         if (b0 < b1 && live)
         {
             int lo = b0, hi = b1;
@@ -371,17 +374,27 @@ __global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
             }
         }
         const double tot = blockSumDouble(e, red);
-        if (threadIdx.x == 0) a.epart[blockIdx.x] = tot;
+        if (threadIdx.x == 0) a.epart[tile] = tot;
     }
 
     // ---- scatter and store ----
     R outv[12][V];
     R vs[3][V];
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj)
+    {
+#pragma unroll
+        for (int c = 0; c < V; ++c) vs[jj][c] = R(0);
+    }
     const bool anyDiel = a.stub != nullptr && live;
     unsigned dielMask = 0;
 #pragma unroll
     for (int c = 0; c < V; ++c) dielMask |= ((m[c] >= kDiel0) ? 1u : 0u) << c;
     dielMask &= nodeLive;
+    // Warp-uniform choice of scatter: all-air warps take the air scatter;
+    // a warp holding any dielectric node takes one branch-free path in
+    // which air nodes still use the air formula (selected, not diverged).
+    const bool warpDiel = kSelect ? __any_sync(0xffffffffu, anyDiel && dielMask != 0) : false;
     if (anyDiel && dielMask)
     {
 #pragma unroll
@@ -395,17 +408,31 @@ __global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
             }
         }
     }
+    const bool allOn = nodeLive == ((1u << V) - 1);
 #pragma unroll
     for (int c = 0; c < V; ++c)
     {
         R in1[12], o1[12];
 #pragma unroll
         for (int s = 0; s < 12; ++s) in1[s] = inc[s][c];
-        if ((dielMask >> c) & 1u)
+        if (!kSelect && ((dielMask >> c) & 1u))
         {
+            // per-node branch: stub formula only where the node is dielectric
             const int id = m[c] - kDiel0;
             R v3[3] = { vs[0][c], vs[1][c], vs[2][c] };
             scatterStub(in1, v3, a.yhat[id], a.ghat[id], o1);
+            vs[0][c] = v3[0];
+            vs[1][c] = v3[1];
+            vs[2][c] = v3[2];
+        }
+        else if (kSelect && warpDiel)
+        {
+            const bool isD = (dielMask >> c) & 1u;
+            const int id = isD ? m[c] - kDiel0 : 0;
+            const R yh = isD ? a.yhat[id] : R(0);
+            const R gh = isD ? a.ghat[id] : R(0);
+            R v3[3] = { vs[0][c], vs[1][c], vs[2][c] };
+            scatterSelect(in1, v3, yh, gh, isD, o1);
             vs[0][c] = v3[0];
             vs[1][c] = v3[1];
             vs[2][c] = v3[2];
@@ -414,7 +441,7 @@ __global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
             scatterAir(in1, o1);
         const bool on = (nodeLive >> c) & 1u;
 #pragma unroll
-        for (int s = 0; s < 12; ++s) outv[s][c] = on ? o1[s] : R(0);
+        for (int s = 0; s < 12; ++s) outv[s][c] = (allOn || on) ? o1[s] : R(0);
     }
     if (live)
     {
@@ -424,8 +451,19 @@ __global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
             if (TLM_GUARD(s * P + node0, 12 * P - V + 1, 12))
             {
                 Pack<S, V> p;
+                if (Traits<S>::kScaled && a.stochastic)
+                {
 #pragma unroll
-                for (int c = 0; c < V; ++c) p.v[c] = encode<S>(outv[s][c], a.inv_scale);
+                    for (int c = 0; c < V; ++c)
+                        p.v[c] = encodeStochastic<S>(
+                            outv[s][c], a.inv_scale,
+                            mix32((unsigned)((node0 + c) * 12 + s) ^ a.round_seed));
+                }
+                else
+                {
+#pragma unroll
+                    for (int c = 0; c < V; ++c) p.v[c] = encode<S>(outv[s][c], a.inv_scale);
+                }
                 *reinterpret_cast<Pack<S, V> *>(a.out + s * P + node0) = p;
             }
         }
@@ -444,6 +482,24 @@ __global__ void __launch_bounds__(kBlock, 2) stepKernel(const StepArgs<S> a)
             }
         }
     }
+}
+
+// Default tile shape of each storage type (Traits<S>::V nodes per thread,
+// Traits<S>::kMinBlocks resident blocks per SM).
+template <class S, bool kIncident>
+__global__ void __launch_bounds__(kBlock, Traits<S>::kMinBlocks) stepKernel(const StepArgs<S> a)
+{
+    __shared__ double red[kBlock / 32];
+    stepTile<S, Traits<S>::V, kIncident, Traits<S>::kSelect>(a, blockIdx.x, red);
+}
+
+// Other tile shapes, chosen by tlm_config.kernel_variant or the autotuner:
+// V nodes per thread, register budget for at least MINB blocks per SM.
+template <class S, int V, int MINB, bool kIncident, bool kSelect>
+__global__ void __launch_bounds__(kBlock, MINB) stepKernelShaped(const StepArgs<S> a)
+{
+    __shared__ double red[kBlock / 32];
+    stepTile<S, V, kIncident, kSelect>(a, blockIdx.x, red);
 }
 
 } // namespace tlmk

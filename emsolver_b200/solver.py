@@ -87,6 +87,8 @@ class TlmConfig:
     storage: int = Storage.F32
     pulseScale: float = 0.0
     stepsPerLaunch: int = 0
+    kernelVariant: int = 0
+    rounding: int = 0          # BF16/F16 storage: 0 nearest, 1 stochastic
 
     def to_c(self):
         c = _lib.ConfigC()
@@ -101,6 +103,8 @@ class TlmConfig:
         c.storage = int(self.storage)
         c.pulse_scale = self.pulseScale
         c.steps_per_launch = int(self.stepsPerLaunch)
+        c.kernel_variant = int(self.kernelVariant)
+        c.rounding = int(self.rounding)
         return c
 
 

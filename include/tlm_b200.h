@@ -103,6 +103,9 @@ typedef struct tlm_config {
     int storage;         /* tlm_storage */
     float pulse_scale;   /* BF16/F16 per-grid scale (0 = choose from sources) */
     int steps_per_launch;/* steps per monitor window; 0 = default (64) */
+    int kernel_variant;  /* thread-tile shape of the step kernel; 0 = default
+                            (tlm_kernel_variants lists the others) */
+    int rounding;        /* BF16/F16 storage: 0 round to nearest, 1 stochastic */
 } tlm_config;
 
 typedef struct tlm_solver *tlm_handle;
@@ -292,6 +295,13 @@ TLM_API tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_pl
                                            void *stream);
 
 /* ---- bench / integration helpers ------------------------------------ */
+
+/* Number of step-kernel tile shapes for a storage mode (valid values of
+ * tlm_config.kernel_variant are 0 .. n-1) and, for one of them, the nodes
+ * per thread and the minimum resident blocks per SM it is compiled for. */
+TLM_API int tlm_kernel_variants(int storage);
+TLM_API tlm_status tlm_kernel_variant_info(int storage, int variant, int *nodes_per_thread,
+                                           int *min_blocks_per_sm);
 
 /* The handle's CUDA stream (cudaStream_t) for event timing by the caller. */
 TLM_API tlm_status tlm_get_stream(tlm_handle h, void **stream);

@@ -67,6 +67,8 @@ struct TlmConfig  // TlmSolver.h:113-123 (+ storage, pulse scale, steps per laun
     Storage storage = Storage::F32;
     float pulseScale = 0.0f;
     int stepsPerLaunch = 0;
+    int kernelVariant = 0;
+    int rounding = 0;  // BF16/F16 storage: 0 nearest, 1 stochastic
 };
 
 struct TlmPort  // TlmSolver.h:81-87
@@ -115,6 +117,8 @@ public:
         c.storage = (int)cfg.storage;
         c.pulse_scale = cfg.pulseScale;
         c.steps_per_launch = cfg.stepsPerLaunch;
+        c.kernel_variant = cfg.kernelVariant;
+        c.rounding = cfg.rounding;
         check(tlm_setup(h_, &g, materials.data(), materials.size(), tab.data(), (int)tab.size(), &c));
         grid_ = grid;
         cfg_ = cfg;
