@@ -44,6 +44,11 @@ class ConfigC(C.Structure):
                 ("kernel_variant", C.c_int), ("rounding", C.c_int)]
 
 
+class BatchTuningC(C.Structure):
+    _fields_ = [("kernel_variant", C.c_int), ("steps_per_launch", C.c_int),
+                ("blocks_per_sm", C.c_int), ("use_graphs", C.c_int), ("ms_per_step", C.c_double)]
+
+
 _h = C.c_void_p
 _st = C.c_int
 _P = C.POINTER
@@ -104,6 +109,18 @@ SIGNATURES = {
                                       C.c_void_p, C.c_void_p]),
     "tlm_kernel_variants": (C.c_int, [C.c_int]),
     "tlm_kernel_variant_info": (_st, [C.c_int, C.c_int, _P(C.c_int), _P(C.c_int)]),
+    "tlm_batch_create": (_st, [_P(_h), C.c_int]),
+    "tlm_batch_destroy": (_st, [_h]),
+    "tlm_batch_attach": (_st, [_h, _h]),
+    "tlm_batch_detach": (_st, [_h, _h]),
+    "tlm_batch_size": (C.c_int, [_h]),
+    "tlm_batch_active": (C.c_int, [_h]),
+    "tlm_batch_step": (_st, [_h, C.c_int]),
+    "tlm_batch_run": (_st, [_h]),
+    "tlm_batch_set_tuning": (_st, [_h, _P(BatchTuningC)]),
+    "tlm_batch_get_tuning": (_st, [_h, _P(BatchTuningC)]),
+    "tlm_batch_autotune": (_st, [_h, C.c_int, _P(BatchTuningC)]),
+    "tlm_batch_get_stream": (_st, [_h, _P(C.c_void_p)]),
     "tlm_get_stream": (_st, [_h, _P(C.c_void_p)]),
     "tlm_device_bytes": (_st, [_h, _P(C.c_size_t)]),
     "tlm_set_kernel_timing": (_st, [_h, C.c_int]),

@@ -41,9 +41,10 @@ template <class R> struct EpilogueArgs
     double *elatest;        // last energy value (polled by the host)
 };
 
-template <class R> __global__ void __launch_bounds__(512) windowEpilogue(const EpilogueArgs<R> a)
+// Body of the window epilogue for one grid; run by one block (any size up to
+// 512 threads); `red` holds blockDim.x/32 doubles of shared memory.
+template <class R> __device__ __forceinline__ void epilogueBody(const EpilogueArgs<R> &a, double *red)
 {
-    __shared__ double red[16];
     const int nent = a.nports + a.nprobes;
     const long long total = (long long)a.w * nent;
     // 1. records (TlmSolver.cpp:677-713), float arithmetic in the
@@ -86,20 +87,30 @@ template <class R> __global__ void __launch_bounds__(512) windowEpilogue(const E
         }
     }
     __syncthreads();
-    // 2. FP64 running DFT: X(f) += x[n] exp(-j w n); the phasor is seeded
-    //    with sincos at the window start and rotated per step.
+    // 2. FP64 running DFT: X(f) += x[n] exp(-j w n). The phasor is a
+    //    function of the absolute step alone -- seeded exactly with sincos at
+    //    every multiple of 64 and rotated by exp(-j w) in between -- so the
+    //    result does not depend on how the steps were split into windows.
     for (int idx = threadIdx.x; idx < a.nports * a.nfreq; idx += blockDim.x)
     {
         const int p = idx / a.nfreq, f = idx % a.nfreq;
         const double w = a.wdt[f];
         double c, s, cw, sw;
-        sincos(w * (double)a.base, &s, &c);
         sincos(w, &sw, &cw);
+        const long long n0 = a.base / 64 * 64;
+        sincos(w * (double)n0, &s, &c);
+        for (long long n = n0; n < a.base; ++n)
+        {
+            const double c2 = c * cw - s * sw;
+            s = s * cw + c * sw;
+            c = c2;
+        }
         double *acc = a.dft + ((long long)p * a.nfreq + f) * 4;
         double vr = acc[0], vi = acc[1], ir = acc[2], ii = acc[3];
         for (int i = 0; i < a.w; ++i)
         {
             const long long n = a.base + i;
+            if (n % 64 == 0) sincos(w * (double)n, &s, &c);
             const double v = a.vrec[n * a.nports + p], cu = a.irec[n * a.nports + p];
             vr += v * c;
             vi -= v * s;
@@ -129,6 +140,12 @@ template <class R> __global__ void __launch_bounds__(512) windowEpilogue(const E
         }
         __syncthreads();
     }
+}
+
+template <class R> __global__ void __launch_bounds__(512) windowEpilogue(const EpilogueArgs<R> a)
+{
+    __shared__ double red[16];
+    epilogueBody(a, red);
 }
 
 // Connect applied to a reflected state: the incident pulses the next step
@@ -248,7 +265,7 @@ __global__ void aosToStubs(const R *__restrict__ in, long long P, int nx, int ny
 
 // Unitarity KATs (TlmSolver.cpp:116-169): max |S^T W S - W| with W = 1 on
 // the 12 links and yh on the 3 stubs (stub case).
-__global__ void unitarityKernel(float epsr, int withStubs, float *err)
+static __global__ void unitarityKernel(float epsr, int withStubs, float *err)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const int np = withStubs ? 15 : 12;

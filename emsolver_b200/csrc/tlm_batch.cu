@@ -1,0 +1,786 @@
+// tlm_batch.cu -- batched execution of many solver handles (C ABI
+// tlm_batch_*), with CUDA-graph launch windows and an autotuner.
+//
+// A batch drives handles that were set up as usual (tlm_setup, ports,
+// probes...). Handles of one storage mode and tile shape form a group; each
+// group's members advance together: per step, one launch of the batched step
+// kernel over the group's tile table; per window of W steps, one epilogue
+// launch. With graphs enabled the W step launches and the epilogue of every
+// group are captured once into a CUDA graph and replayed; member and tile
+// tables are device arrays with spare capacity, so members join and leave
+// between windows without a new capture. A member runs from its current
+// step to its total_steps; its results are read through the ordinary handle
+// getters and are bitwise those of the same handle stepped alone.
+#include "tlm_b200.h"
+#include "tlm_internal.h"
+
+#include "tlm_batch_kernels.cuh"
+#include "tlm_host_math.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+using namespace tlmi;
+using tlmk::kBlock;
+using tlmk::MemberDesc;
+
+namespace {
+
+struct Group
+{
+    int storage = TLM_STORE_F32;
+    int variant = 0;
+    std::vector<tlm_solver *> members;
+    void *dMembers = nullptr;   // MemberDesc<S>[capMembers]
+    int capMembers = 0;
+    int *dNMembers = nullptr;
+    int2 *dTiles = nullptr;
+    int capTiles = 0;
+    int *dNTiles = nullptr;
+    int gridBlocks = 0;         // resident blocks of the step kernel
+    size_t descBytes = 0;
+};
+
+int keyOf(int storage, int variant) { return storage * 16 + variant; }
+
+} // namespace
+
+struct tlm_batch_s
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int window = 64;
+    bool useGraph = true;
+    int blocksPerSm = 0;         // 0: as many as resident
+    std::map<int, Group> groups;
+    unsigned *dFault = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool graphDirty = true;
+    int smCount = 148;
+
+    tlm_status fail(tlm_status s, const std::string &m)
+    {
+        err = m;
+        setThreadError(m);
+        return s;
+    }
+    tlm_status cuda(cudaError_t e, const char *what)
+    {
+        if (e == cudaSuccess) return TLM_OK;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? TLM_ENOMEM : TLM_ECUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+    }
+};
+
+#define TLM_BCU(b, call) TLM_TRY((b)->cuda((call), #call))
+
+namespace {
+
+struct BatchDeviceGuard
+{
+    int prev = -1;
+    explicit BatchDeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~BatchDeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+size_t descSize(int storage)
+{
+    switch (storage)
+    {
+    case TLM_STORE_F64: return sizeof(MemberDesc<double>);
+    case TLM_STORE_BF16: return sizeof(MemberDesc<__nv_bfloat16>);
+    case TLM_STORE_F16: return sizeof(MemberDesc<__half>);
+    default: return sizeof(MemberDesc<float>);
+    }
+}
+
+template <class S> MemberDesc<S> makeDesc(tlm_solver *h)
+{
+    using R = typename tlmk::Traits<S>::R;
+    MemberDesc<S> d;
+    std::memset(&d, 0, sizeof(d));
+    d.buf[0] = static_cast<S *>(h->dPulses[0]);
+    d.buf[1] = static_cast<S *>(h->dPulses[1]);
+    d.stub = static_cast<R *>(h->dStub);
+    d.mat = h->dMat;
+    d.yhat = static_cast<const R *>(h->dYhat);
+    d.ghat = static_cast<const R *>(h->dGhat);
+    d.P = h->P;
+    d.nquads = h->nquads;
+    d.nx = h->nx;
+    d.ny = h->ny;
+    d.nz = h->nz;
+    d.px = h->px;
+    d.nq = h->nq;
+    d.rho = (R)h->cfg.boundary_rho;
+    d.scale = (R)h->scale;
+    d.inv_scale = (R)(1.0f / h->scale);
+    d.tile_begin = h->dTile;
+    d.spec = h->dSpec;
+    d.sv = static_cast<const R *>(h->dSv);
+    d.samples = static_cast<R *>(h->dSamples);
+    d.nsamp = h->nsamp;
+    d.epart = h->dEpart;
+    d.nblocks = h->nblocks;
+    d.stochastic = h->cfg.rounding == 1 ? 1 : 0;
+    d.base = h->curStep;
+    d.total = h->cfg.total_steps;
+    tlmk::EpilogueArgs<R> &a = d.epi;
+    a.samples = static_cast<const R *>(h->dSamples);
+    a.nsamp = h->nsamp;
+    a.nports = (int)h->ports.size();
+    a.port_off = h->dPortOff;
+    a.port_slots = h->dPortSlots;
+    a.port_pol = h->dPortPol;
+    a.port_nb = h->dPortNb;
+    a.nprobes = (int)h->probeCells.size();
+    a.probe_slot = h->dProbeSlot;
+    a.probe_scale = h->storage == TLM_STORE_F64 ? (R)tlmh::probe_scale_f64(h->g.dl)
+                                                : (R)tlmh::probe_scale_f32(h->g.dl);
+    a.eta0 = (R)tlmh::eta0_f32();
+    a.vrec = h->dVrec;
+    a.irec = h->dIrec;
+    a.prec = h->dPrec;
+    a.nfreq = h->dDft ? (int)h->dftFreqs.size() : 0;
+    a.wdt = h->dWdt;
+    a.dft = h->dDft;
+    a.epart = h->dEpart;
+    a.nblocks = h->nblocks;
+    a.ehist = h->dEhist;
+    a.elatest = h->dElatest;
+    return d;
+}
+
+tlm_status growBuffer(tlm_batch_s *b, void **p, int *cap, int need, size_t elem)
+{
+    if (need <= *cap && *p) return TLM_OK;
+    int c = std::max(need, std::max(16, *cap * 2));
+    void *q = nullptr;
+    TLM_BCU(b, cudaMalloc(&q, (size_t)c * elem));
+    if (*p) cudaFree(*p);
+    *p = q;
+    *cap = c;
+    b->graphDirty = true;  // kernels captured with the old address
+    return TLM_OK;
+}
+
+// Upload the group's member and tile tables (between windows).
+tlm_status syncGroupTables(tlm_batch_s *b, Group &g)
+{
+    const int nm = (int)g.members.size();
+    TLM_TRY(growBuffer(b, &g.dMembers, &g.capMembers, std::max(nm, 1), g.descBytes));
+    if (!g.dNMembers)
+    {
+        TLM_BCU(b, cudaMalloc(&g.dNMembers, sizeof(int)));
+        b->graphDirty = true;
+    }
+    if (!g.dNTiles)
+    {
+        TLM_BCU(b, cudaMalloc(&g.dNTiles, sizeof(int)));
+        b->graphDirty = true;
+    }
+    std::vector<char> descs((size_t)std::max(nm, 1) * g.descBytes, 0);
+    std::vector<int2> tiles;
+    for (int m = 0; m < nm; ++m)
+    {
+        tlm_solver *h = g.members[m];
+        char *dst = descs.data() + (size_t)m * g.descBytes;
+        switch (g.storage)
+        {
+        case TLM_STORE_F64: { auto d = makeDesc<double>(h); std::memcpy(dst, &d, sizeof(d)); break; }
+        case TLM_STORE_BF16: { auto d = makeDesc<__nv_bfloat16>(h); std::memcpy(dst, &d, sizeof(d)); break; }
+        case TLM_STORE_F16: { auto d = makeDesc<__half>(h); std::memcpy(dst, &d, sizeof(d)); break; }
+        default: { auto d = makeDesc<float>(h); std::memcpy(dst, &d, sizeof(d)); break; }
+        }
+        if (h->curStep < h->cfg.total_steps)
+            for (int t = 0; t < h->nblocks; ++t) tiles.push_back(make_int2(m, t));
+    }
+    int cap = g.capTiles;
+    void *tp = g.dTiles;
+    TLM_TRY(growBuffer(b, &tp, &cap, std::max((int)tiles.size(), 1), sizeof(int2)));
+    g.dTiles = static_cast<int2 *>(tp);
+    g.capTiles = cap;
+    const int ntiles = (int)tiles.size();
+    TLM_BCU(b, cudaMemcpyAsync(g.dMembers, descs.data(), (size_t)std::max(nm, 1) * g.descBytes,
+                               cudaMemcpyHostToDevice, b->stream));
+    if (ntiles)
+        TLM_BCU(b, cudaMemcpyAsync(g.dTiles, tiles.data(), tiles.size() * sizeof(int2),
+                                   cudaMemcpyHostToDevice, b->stream));
+    TLM_BCU(b, cudaMemcpyAsync(g.dNTiles, &ntiles, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    TLM_BCU(b, cudaMemcpyAsync(g.dNMembers, &nm, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    TLM_BCU(b, cudaStreamSynchronize(b->stream));
+    return TLM_OK;
+}
+
+template <class S, int V, int MINB, bool SEL>
+tlm_status launchGroupStep(tlm_batch_s *b, Group &g, int i, bool doLaunch)
+{
+    if (g.gridBlocks == 0)
+    {
+        int occ = 0;
+        TLM_BCU(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                       &occ, tlmk::batchStepKernel<S, V, MINB, SEL>, kBlock, 0));
+        occ = std::max(occ, 1);
+        if (b->blocksPerSm > 0) occ = std::min(occ, b->blocksPerSm);
+        g.gridBlocks = b->smCount * occ;
+    }
+    if (!doLaunch) return TLM_OK;
+    tlmk::batchStepKernel<S, V, MINB, SEL><<<g.gridBlocks, kBlock, 0, b->stream>>>(
+        static_cast<MemberDesc<S> *>(g.dMembers), g.dTiles, g.dNTiles, i, b->dFault);
+    return b->cuda(cudaGetLastError(), "batchStepKernel launch");
+}
+
+// The step launch of a group in its tile shape (the shape tables of
+// tlm_internal.h: variant 0 = Traits<S> default).
+template <class S> tlm_status launchShape(tlm_batch_s *b, Group &g, int i, bool go)
+{
+    constexpr int V0 = tlmk::Traits<S>::V;
+    constexpr int M0 = tlmk::Traits<S>::kMinBlocks;
+    constexpr bool S0 = tlmk::Traits<S>::kSelect;
+    if (g.variant == 0) return launchGroupStep<S, V0, M0, S0>(b, g, i, go);
+    if constexpr (std::is_same<S, double>::value)
+    {
+        if (g.variant == 1) return launchGroupStep<S, 1, 4, false>(b, g, i, go);
+        return launchGroupStep<S, 2, 3, false>(b, g, i, go);
+    }
+    else if constexpr (std::is_same<S, float>::value)
+    {
+        if (g.variant == 1) return launchGroupStep<S, 4, 3, true>(b, g, i, go);
+        if (g.variant == 2) return launchGroupStep<S, 2, 4, true>(b, g, i, go);
+        return launchGroupStep<S, 4, 2, false>(b, g, i, go);
+    }
+    else
+    {
+        if (g.variant == 1) return launchGroupStep<S, 4, 3, true>(b, g, i, go);
+        if (g.variant == 2) return launchGroupStep<S, 2, 4, true>(b, g, i, go);
+        return launchGroupStep<S, 8, 2, false>(b, g, i, go);
+    }
+}
+
+tlm_status launchStep(tlm_batch_s *b, Group &g, int i, bool go = true)
+{
+    switch (g.storage)
+    {
+    case TLM_STORE_F64: return launchShape<double>(b, g, i, go);
+    case TLM_STORE_BF16: return launchShape<__nv_bfloat16>(b, g, i, go);
+    case TLM_STORE_F16: return launchShape<__half>(b, g, i, go);
+    default: return launchShape<float>(b, g, i, go);
+    }
+}
+
+tlm_status launchEpilogue(tlm_batch_s *b, Group &g, int w)
+{
+    const int grid = std::max(g.capMembers, 1);
+    switch (g.storage)
+    {
+    case TLM_STORE_F64:
+        tlmk::batchEpilogue<double><<<grid, 512, 0, b->stream>>>(
+            static_cast<MemberDesc<double> *>(g.dMembers), g.dNMembers, w);
+        break;
+    case TLM_STORE_BF16:
+        tlmk::batchEpilogue<__nv_bfloat16><<<grid, 512, 0, b->stream>>>(
+            static_cast<MemberDesc<__nv_bfloat16> *>(g.dMembers), g.dNMembers, w);
+        break;
+    case TLM_STORE_F16:
+        tlmk::batchEpilogue<__half><<<grid, 512, 0, b->stream>>>(
+            static_cast<MemberDesc<__half> *>(g.dMembers), g.dNMembers, w);
+        break;
+    default:
+        tlmk::batchEpilogue<float><<<grid, 512, 0, b->stream>>>(
+            static_cast<MemberDesc<float> *>(g.dMembers), g.dNMembers, w);
+        break;
+    }
+    return b->cuda(cudaGetLastError(), "batchEpilogue launch");
+}
+
+// Queue one window of w steps for every group (not captured).
+tlm_status enqueueWindow(tlm_batch_s *b, int w)
+{
+    for (int i = 0; i < w; ++i)
+        for (auto &kv : b->groups)
+            if (!kv.second.members.empty()) TLM_TRY(launchStep(b, kv.second, i));
+    for (auto &kv : b->groups)
+        if (!kv.second.members.empty()) TLM_TRY(launchEpilogue(b, kv.second, w));
+    return TLM_OK;
+}
+
+tlm_status captureGraph(tlm_batch_s *b)
+{
+    if (b->graph)
+    {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    for (auto &kv : b->groups)  // occupancy queries stay outside the capture
+        if (!kv.second.members.empty()) TLM_TRY(launchStep(b, kv.second, 0, false));
+    cudaGraph_t g = nullptr;
+    TLM_BCU(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    tlm_status st = enqueueWindow(b, b->window);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (st != TLM_OK)
+    {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    TLM_BCU(b, e);
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    TLM_BCU(b, e);
+    b->graphDirty = false;
+    return TLM_OK;
+}
+
+// After a window of w steps: move every member's host mirror forward.
+void advanceMembers(tlm_batch_s *b, int w)
+{
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members)
+        {
+            const int next = std::min(h->curStep + w, std::max(h->cfg.total_steps, h->curStep));
+            h->curStep = next;
+            h->curBuf = next & 1;
+            h->doneStep.store(next);
+        }
+}
+
+int activeMembers(tlm_batch_s *b)
+{
+    int n = 0;
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members) n += h->curStep < h->cfg.total_steps;
+    return n;
+}
+
+// Make a handle ready to be driven by the batch.
+tlm_status readyMember(tlm_batch_s *b, tlm_solver *h)
+{
+    if (h->curStep == 0 && !h->prepared) TLM_TRY(chooseScale(h));
+    TLM_TRY(prepare(h));
+    TLM_TRY(setWindow(h, b->window));
+    TLM_TRY(ensureRecords(h, std::max(h->cfg.total_steps, 1)));
+    TLM_TRY(uploadSourceTable(h, std::max(h->cfg.total_steps, 1)));
+    return TLM_OK;
+}
+
+tlm_status refreshAll(tlm_batch_s *b)
+{
+    for (auto &kv : b->groups) TLM_TRY(syncGroupTables(b, kv.second));
+    return TLM_OK;
+}
+
+tlm_status runWindows(tlm_batch_s *b, int nsteps)
+{
+    int remaining = nsteps;
+    while (remaining > 0 && activeMembers(b) > 0)
+    {
+        const int w = std::min(remaining, b->window);
+        if (b->useGraph && w == b->window)
+        {
+            if (b->graphDirty || !b->graph) TLM_TRY(captureGraph(b));
+            TLM_BCU(b, cudaGraphLaunch(b->graph, b->stream));
+        }
+        else
+            TLM_TRY(enqueueWindow(b, w));
+        advanceMembers(b, w);
+        remaining -= w;
+        // members that just finished leave the tile table
+        bool finished = false;
+        for (auto &kv : b->groups)
+            for (tlm_solver *h : kv.second.members)
+                if (h->curStep >= h->cfg.total_steps && h->curStep - w < h->cfg.total_steps) finished = true;
+        if (finished)
+        {
+            TLM_BCU(b, cudaStreamSynchronize(b->stream));
+            TLM_TRY(refreshAll(b));
+        }
+    }
+    TLM_BCU(b, cudaStreamSynchronize(b->stream));
+    unsigned f = 0;
+    if (b->dFault)
+    {
+        TLM_BCU(b, cudaMemcpy(&f, b->dFault, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (f) return b->fail(TLM_ECUDA, "bounds check tripped in the batched kernel, mask " +
+                                             std::to_string(f));
+    }
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members)
+        {
+            double e = 0.0;
+            TLM_BCU(b, cudaMemcpy(&e, h->dElatest, sizeof(double), cudaMemcpyDeviceToHost));
+            h->energy.store((float)e);
+        }
+    return TLM_OK;
+}
+
+// ---- autotuner cache ----------------------------------------------------
+std::mutex g_tuneMutex;
+std::map<std::string, tlm_batch_tuning> g_tuneCache;
+
+std::string tuneKey(tlm_batch_s *b)
+{
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, b->device);
+    long long nodes = 0;
+    int members = 0;
+    std::ostringstream k;
+    k << prop.name;
+    for (auto &kv : b->groups)
+    {
+        for (tlm_solver *h : kv.second.members)
+        {
+            nodes += (long long)h->nx * h->ny * h->nz;
+            ++members;
+        }
+        k << "|s" << kv.second.storage;
+    }
+    int lg = 0;
+    while ((1LL << (lg + 1)) <= std::max(nodes, 1LL)) ++lg;
+    int lm = 0;
+    while ((1 << (lm + 1)) <= std::max(members, 1)) ++lm;
+    k << "|n2^" << lg << "|m2^" << lm;
+    return k.str();
+}
+
+void loadCacheFile()
+{
+    const char *path = std::getenv("TLM_AUTOTUNE_CACHE");
+    if (!path) return;
+    std::ifstream f(path);
+    std::string key;
+    tlm_batch_tuning t;
+    while (f >> std::quoted(key) >> t.kernel_variant >> t.steps_per_launch >> t.blocks_per_sm >>
+           t.use_graphs >> t.ms_per_step)
+        g_tuneCache[key] = t;
+}
+
+void saveCacheFile()
+{
+    const char *path = std::getenv("TLM_AUTOTUNE_CACHE");
+    if (!path) return;
+    std::ofstream f(path);
+    for (auto &kv : g_tuneCache)
+        f << std::quoted(kv.first) << ' ' << kv.second.kernel_variant << ' ' << kv.second.steps_per_launch
+          << ' ' << kv.second.blocks_per_sm << ' ' << kv.second.use_graphs << ' ' << kv.second.ms_per_step
+          << '\n';
+}
+
+tlm_status applyTuning(tlm_batch_s *b, const tlm_batch_tuning &t)
+{
+    b->window = t.steps_per_launch;
+    b->useGraph = t.use_graphs != 0;
+    b->blocksPerSm = t.blocks_per_sm;
+    std::map<int, Group> regrouped;
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members)
+        {
+            const int v = std::min(t.kernel_variant, shapeCount(h->storage) - 1);
+            TLM_TRY(reshape(h, v));
+            TLM_TRY(readyMember(b, h));
+            Group &g = regrouped[keyOf(h->storage, h->variant)];
+            g.storage = h->storage;
+            g.variant = h->variant;
+            g.descBytes = descSize(h->storage);
+            g.members.push_back(h);
+        }
+    for (auto &kv : b->groups)
+    {
+        Group &g = kv.second;
+        if (g.dMembers) cudaFree(g.dMembers);
+        if (g.dTiles) cudaFree(g.dTiles);
+        if (g.dNTiles) cudaFree(g.dNTiles);
+        if (g.dNMembers) cudaFree(g.dNMembers);
+    }
+    b->groups = std::move(regrouped);
+    b->graphDirty = true;
+    return refreshAll(b);
+}
+
+} // namespace
+
+extern "C" {
+
+tlm_status tlm_batch_create(tlm_batch *out, int device)
+{
+    if (!out)
+    {
+        setThreadError("null output pointer");
+        return TLM_EINVAL;
+    }
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+    {
+        cudaGetLastError();
+        setThreadError("no such CUDA device");
+        return TLM_ENODEV;
+    }
+    tlm_batch_s *b = new tlm_batch_s();
+    b->device = device;
+    BatchDeviceGuard dg(device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) b->smCount = prop.multiProcessorCount;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+#ifdef TLM_CHECKED
+    if (e == cudaSuccess) e = cudaMalloc(&b->dFault, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(b->dFault, 0, sizeof(unsigned));
+#endif
+    if (e != cudaSuccess)
+    {
+        setThreadError(std::string("batch creation: ") + cudaGetErrorString(e));
+        if (b->stream) cudaStreamDestroy(b->stream);
+        delete b;
+        return TLM_ECUDA;
+    }
+    *out = b;
+    return TLM_OK;
+}
+
+tlm_status tlm_batch_destroy(tlm_batch b)
+{
+    if (!b) return TLM_OK;
+    BatchDeviceGuard dg(b->device);
+    cudaStreamSynchronize(b->stream);
+    for (auto &kv : b->groups)
+    {
+        for (tlm_solver *h : kv.second.members) h->batch = nullptr;
+        Group &g = kv.second;
+        if (g.dMembers) cudaFree(g.dMembers);
+        if (g.dTiles) cudaFree(g.dTiles);
+        if (g.dNTiles) cudaFree(g.dNTiles);
+        if (g.dNMembers) cudaFree(g.dNMembers);
+    }
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->dFault) cudaFree(b->dFault);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return TLM_OK;
+}
+
+tlm_status tlm_batch_attach(tlm_batch b, tlm_handle h)
+{
+    if (!b || !h)
+    {
+        setThreadError("null batch or handle");
+        return TLM_EINVAL;
+    }
+    if (h->batch) return b->fail(TLM_ESTATE, "the handle is already attached to a batch");
+    if (!h->configured) return b->fail(TLM_ESTATE, "tlm_setup has not been called on the handle");
+    if (h->running.load()) return b->fail(TLM_EBUSY, "the handle is running");
+    if (h->device != b->device) return b->fail(TLM_EINVAL, "handle and batch are on different devices");
+    if (h->stateIncident)
+        return b->fail(TLM_ESTATE, "a state set by tlm_set_pulses must be stepped once before batching");
+    BatchDeviceGuard dg(b->device);
+    cudaStreamSynchronize(h->stream);
+    tlm_status st = readyMember(b, h);
+    if (st != TLM_OK) return b->fail(st, std::string("attach: ") + h->err);
+    Group &g = b->groups[keyOf(h->storage, h->variant)];
+    g.storage = h->storage;
+    g.variant = h->variant;
+    g.descBytes = descSize(h->storage);
+    g.members.push_back(h);
+    h->batch = b;
+    return syncGroupTables(b, g);
+}
+
+tlm_status tlm_batch_detach(tlm_batch b, tlm_handle h)
+{
+    if (!b || !h || h->batch != b)
+    {
+        setThreadError("the handle is not attached to this batch");
+        return TLM_EINVAL;
+    }
+    BatchDeviceGuard dg(b->device);
+    TLM_BCU(b, cudaStreamSynchronize(b->stream));
+    Group &g = b->groups[keyOf(h->storage, h->variant)];
+    g.members.erase(std::remove(g.members.begin(), g.members.end(), h), g.members.end());
+    h->batch = nullptr;
+    return syncGroupTables(b, g);
+}
+
+int tlm_batch_size(tlm_batch b)
+{
+    if (!b) return 0;
+    int n = 0;
+    for (auto &kv : b->groups) n += (int)kv.second.members.size();
+    return n;
+}
+
+int tlm_batch_active(tlm_batch b) { return b ? activeMembers(b) : 0; }
+
+tlm_status tlm_batch_step(tlm_batch b, int n_steps)
+{
+    if (!b || n_steps < 0)
+    {
+        setThreadError("null batch or negative step count");
+        return TLM_EINVAL;
+    }
+    BatchDeviceGuard dg(b->device);
+    return runWindows(b, n_steps);
+}
+
+tlm_status tlm_batch_run(tlm_batch b)
+{
+    if (!b)
+    {
+        setThreadError("null batch");
+        return TLM_EINVAL;
+    }
+    BatchDeviceGuard dg(b->device);
+    int most = 0;
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members) most = std::max(most, h->cfg.total_steps - h->curStep);
+    return runWindows(b, most);
+}
+
+tlm_status tlm_batch_set_tuning(tlm_batch b, const tlm_batch_tuning *t)
+{
+    if (!b || !t || t->steps_per_launch < 1 || t->steps_per_launch > 1024 || t->blocks_per_sm < 0 ||
+        t->kernel_variant < 0)
+    {
+        setThreadError("bad batch tuning");
+        return TLM_EINVAL;
+    }
+    BatchDeviceGuard dg(b->device);
+    TLM_BCU(b, cudaStreamSynchronize(b->stream));
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members)
+            if (h->variant != std::min(t->kernel_variant, shapeCount(h->storage) - 1) && h->curStep != 0)
+                return b->fail(TLM_ESTATE, "the tile shape can only change before the first step");
+    return applyTuning(b, *t);
+}
+
+tlm_status tlm_batch_get_tuning(tlm_batch b, tlm_batch_tuning *t)
+{
+    if (!b || !t)
+    {
+        setThreadError("null argument");
+        return TLM_EINVAL;
+    }
+    int v = 0;
+    for (auto &kv : b->groups)
+        if (!kv.second.members.empty()) v = kv.second.variant;
+    t->kernel_variant = v;
+    t->steps_per_launch = b->window;
+    t->blocks_per_sm = b->blocksPerSm;
+    t->use_graphs = b->useGraph ? 1 : 0;
+    t->ms_per_step = 0.0;
+    return TLM_OK;
+}
+
+tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *out)
+{
+    if (!b || trial_windows < 1)
+    {
+        setThreadError("null batch or no trial windows");
+        return TLM_EINVAL;
+    }
+    BatchDeviceGuard dg(b->device);
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members)
+            if (h->curStep != 0) return b->fail(TLM_ESTATE, "autotune runs before the first step");
+    if (tlm_batch_size(b) == 0) return b->fail(TLM_ESTATE, "the batch has no members");
+    const std::string key = tuneKey(b);
+    {
+        std::lock_guard<std::mutex> lk(g_tuneMutex);
+        if (g_tuneCache.empty()) loadCacheFile();
+        auto it = g_tuneCache.find(key);
+        if (it != g_tuneCache.end())
+        {
+            if (out) *out = it->second;
+            return applyTuning(b, it->second);
+        }
+    }
+    int nvar = 1 << 30;
+    for (auto &kv : b->groups)
+        if (!kv.second.members.empty()) nvar = std::min(nvar, shapeCount(kv.second.storage));
+    cudaEvent_t e0, e1;
+    TLM_BCU(b, cudaEventCreate(&e0));
+    TLM_BCU(b, cudaEventCreate(&e1));
+    auto trial = [&](const tlm_batch_tuning &t, double *msPerStep) -> tlm_status {
+        for (auto &kv : b->groups)
+            for (tlm_solver *h : kv.second.members) TLM_TRY(rewind(h));
+        TLM_TRY(applyTuning(b, t));
+        TLM_TRY(runWindows(b, t.steps_per_launch));  // warm-up (graph capture)
+        TLM_BCU(b, cudaEventRecord(e0, b->stream));
+        TLM_TRY(runWindows(b, t.steps_per_launch * trial_windows));
+        TLM_BCU(b, cudaEventRecord(e1, b->stream));
+        TLM_BCU(b, cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        TLM_BCU(b, cudaEventElapsedTime(&ms, e0, e1));
+        *msPerStep = ms / (t.steps_per_launch * trial_windows);
+        return TLM_OK;
+    };
+    tlm_batch_tuning best{ 0, 64, 0, 1, 1e30 };
+    tlm_status st = TLM_OK;
+    for (int v = 0; v < nvar && st == TLM_OK; ++v)
+    {
+        tlm_batch_tuning t{ v, 64, 0, 1, 0.0 };
+        double ms = 0.0;
+        st = trial(t, &ms);
+        if (st == TLM_OK && ms < best.ms_per_step)
+        {
+            best = t;
+            best.ms_per_step = ms;
+        }
+    }
+    for (int w : { 16, 32, 128 })
+    {
+        if (st != TLM_OK) break;
+        tlm_batch_tuning t = best;
+        t.steps_per_launch = w;
+        double ms = 0.0;
+        st = trial(t, &ms);
+        if (st == TLM_OK && ms < best.ms_per_step)
+        {
+            best = t;
+            best.ms_per_step = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != TLM_OK) return st;
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members) TLM_TRY(rewind(h));
+    TLM_TRY(applyTuning(b, best));
+    {
+        std::lock_guard<std::mutex> lk(g_tuneMutex);
+        g_tuneCache[key] = best;
+        saveCacheFile();
+    }
+    if (out) *out = best;
+    return TLM_OK;
+}
+
+tlm_status tlm_batch_get_stream(tlm_batch b, void **stream)
+{
+    if (!b)
+    {
+        setThreadError("null batch");
+        return TLM_EINVAL;
+    }
+    if (stream) *stream = (void *)b->stream;
+    return TLM_OK;
+}
+
+} // extern "C"

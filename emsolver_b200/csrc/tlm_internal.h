@@ -152,6 +152,12 @@ struct tlm_solver
     unsigned *dFault = nullptr;
     size_t devBytes = 0;
 
+    // batched execution (tlm_batch_*): the batch that drives this handle, and
+    // the per-step source values the batched kernel reads from device memory
+    struct tlm_batch_s *batch = nullptr;
+    void *dSv = nullptr;
+    long long svCount = 0;
+
     // kernel timing
     bool timing = false;
     std::vector<cudaEvent_t> evs;
@@ -233,5 +239,10 @@ tlm_status checkHandle(tlm_solver *h);
 tlm_status checkReady(tlm_solver *h);
 tlm_status chooseScale(tlm_solver *h);
 int gridBlocksFor(long long n);
+// Batched execution support (defined in tlm_solver.cu).
+tlm_status uploadSourceTable(tlm_solver *h, long long steps);
+tlm_status setWindow(tlm_solver *h, int window);
+tlm_status rewind(tlm_solver *h);
+tlm_status reshape(tlm_solver *h, int variant);
 
 } // namespace tlmi

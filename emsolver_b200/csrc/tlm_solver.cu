@@ -79,6 +79,8 @@ void freeMonitors(tlm_solver *h)
 void freeAll(tlm_solver *h)
 {
     freeMonitors(h);
+    devFree(h, h->dSv);
+    h->svCount = 0;
     devFree(h, h->dPulses[0]);
     devFree(h, h->dPulses[1]);
     devFree(h, h->dStub);
@@ -471,9 +473,91 @@ tlm_status checkReady(tlm_solver *h)
 tlm_status checkAddable(tlm_solver *h)
 {
     TLM_TRY(checkReady(h));
+    if (h->batch) return h->fail(TLM_ESTATE, "the handle is attached to a batch");
     if (h->curStep > 0)
         return h->fail(TLM_ESTATE, "sources and monitors must be added before the first step");
     h->prepared = false;
+    return TLM_OK;
+}
+
+// Per-step source values on the device (the batched kernel reads them there
+// instead of taking them as a launch argument): sourceValue for [0, steps).
+tlm_status uploadSourceTable(tlm_solver *h, long long steps)
+{
+    const size_t rb = realBytes(h->storage);
+    if (h->dSv && h->svCount >= steps) return TLM_OK;
+    devFree(h, h->dSv);
+    h->svCount = 0;
+    TLM_TRY(devAlloc(h, &h->dSv, (size_t)std::max<long long>(steps, 1) * rb));
+    std::vector<double> v64((size_t)std::max<long long>(steps, 1), 0.0);
+    for (long long n = 0; n < steps; ++n) v64[(size_t)n] = sourceValue(h, (int)n);
+    if (h->storage == TLM_STORE_F64)
+    {
+        TLM_CU(h, cudaMemcpy(h->dSv, v64.data(), v64.size() * 8, cudaMemcpyHostToDevice));
+    }
+    else
+    {
+        std::vector<float> v32(v64.size());
+        for (size_t t = 0; t < v64.size(); ++t) v32[t] = (float)v64[t];
+        TLM_CU(h, cudaMemcpy(h->dSv, v32.data(), v32.size() * 4, cudaMemcpyHostToDevice));
+    }
+    h->svCount = steps;
+    return TLM_OK;
+}
+
+// Steps per launch window: the per-window sample and energy-partial buffers
+// are resized; records and DFT accumulators are kept.
+tlm_status setWindow(tlm_solver *h, int window)
+{
+    TLM_TRY(prepare(h));
+    if (window == h->window) return TLM_OK;
+    const size_t rb = realBytes(h->storage);
+    devFree(h, h->dSamples);
+    devFree(h, h->dEpart);
+    h->window = window;
+    TLM_TRY(devAlloc(h, &h->dSamples, (size_t)h->window * std::max(h->nsamp, 1) * 6 * rb));
+    TLM_TRY(devAlloc(h, &h->dEpart, (size_t)(h->window / 16 + 1) * h->nblocks * sizeof(double)));
+    return TLM_OK;
+}
+
+// Back to step 0 with zero fields (the state after setup), keeping the
+// sources, monitors and device allocations.
+tlm_status rewind(tlm_solver *h)
+{
+    const size_t sb = storageBytes(h->storage), rb = realBytes(h->storage);
+    TLM_CU(h, cudaStreamSynchronize(h->stream));
+    TLM_CU(h, cudaMemsetAsync(h->dPulses[0], 0, 12 * (size_t)h->P * sb, h->stream));
+    TLM_CU(h, cudaMemsetAsync(h->dPulses[1], 0, 12 * (size_t)h->P * sb, h->stream));
+    if (h->dStub) TLM_CU(h, cudaMemsetAsync(h->dStub, 0, 3 * (size_t)h->P * rb, h->stream));
+    if (h->dDft)
+        TLM_CU(h, cudaMemsetAsync(h->dDft, 0,
+                                  h->ports.size() * h->dftFreqs.size() * 4 * sizeof(double), h->stream));
+    TLM_CU(h, cudaMemsetAsync(h->dElatest, 0, sizeof(double), h->stream));
+    TLM_CU(h, cudaStreamSynchronize(h->stream));
+    h->curStep = 0;
+    h->curBuf = 0;
+    h->stateIncident = false;
+    h->doneStep.store(0);
+    h->energy.store(0.0f);
+    h->finished.store(false);
+    return TLM_OK;
+}
+
+// Switch the step-kernel tile shape of a handle that is at step 0.
+tlm_status reshape(tlm_solver *h, int variant)
+{
+    if (h->curStep != 0) return h->fail(TLM_ESTATE, "the tile shape can only change at step 0");
+    if (variant < 0 || variant >= shapeCount(h->storage)) return h->fail(TLM_EINVAL, "no such variant");
+    if (variant == h->variant && h->prepared) return TLM_OK;
+    const long long cap = h->recCap;
+    h->variant = variant;
+    h->V = shapeOf(h->storage, variant).V;
+    h->nq = h->px / h->V;
+    h->nquads = (long long)h->nq * h->ny * h->nz;
+    h->nblocks = (int)((h->nquads + kBlock - 1) / kBlock);
+    h->prepared = false;
+    TLM_TRY(prepare(h));
+    if (cap > 0) TLM_TRY(ensureRecords(h, cap));
     return TLM_OK;
 }
 
@@ -646,6 +730,7 @@ tlm_status tlm_destroy(tlm_handle h)
 {
     if (!h) return TLM_OK;
     if (busy(h)) return h->fail(TLM_EBUSY, "cannot destroy a running handle");
+    if (h->batch) return h->fail(TLM_EBUSY, "detach the handle from its batch first");
     DeviceGuard dg(h->device);
     cudaStreamSynchronize(h->stream);
     freeAll(h);
@@ -668,6 +753,7 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
 {
     TLM_TRY(checkHandle(h));
     if (busy(h)) return h->fail(TLM_EBUSY, "the handle is running");
+    if (h->batch) return h->fail(TLM_ESTATE, "the handle is attached to a batch");
     if (!grid || !mat || !cfg) return h->fail(TLM_EINVAL, "null grid, material map or config");
     if (grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0)
         return h->fail(TLM_EINVAL, "grid dimensions must be positive");
@@ -942,6 +1028,7 @@ extern "C" {
 tlm_status tlm_step_async(tlm_handle h, int n_steps)
 {
     TLM_TRY(checkReady(h));
+    if (h->batch) return h->fail(TLM_ESTATE, "the handle is attached to a batch: step the batch");
     if (n_steps < 0) return h->fail(TLM_EINVAL, "n_steps must be >= 0");
     DeviceGuard dg(h->device);
     if (h->curStep == 0 && !h->prepared) TLM_TRY(chooseScale(h));
@@ -965,6 +1052,7 @@ tlm_status tlm_step(tlm_handle h, int n_steps)
 tlm_status tlm_run(tlm_handle h)
 {
     TLM_TRY(checkReady(h));
+    if (h->batch) return h->fail(TLM_ESTATE, "the handle is attached to a batch: step the batch");
     DeviceGuard dg(h->device);
     bool expected = false;
     if (!h->running.compare_exchange_strong(expected, true))
@@ -1144,6 +1232,7 @@ tlm_status tlm_get_pulses_f64(tlm_handle h, double *out, size_t cap) { return ge
 tlm_status tlm_set_pulses(tlm_handle h, const float *in, size_t n)
 {
     TLM_TRY(checkReady(h));
+    if (h->batch) return h->fail(TLM_ESTATE, "the handle is attached to a batch");
     if (!in || n != (size_t)h->ncell * 12)
         return h->fail(TLM_EINVAL, "pulse array must hold 12 values per cell");
     DeviceGuard dg(h->device);

@@ -256,6 +256,50 @@ TLM_API tlm_status tlm_waveform_value(int waveform, float f0, float dl, int n, f
 TLM_API tlm_status tlm_scatter_unitarity_error(int device, float *err);
 TLM_API tlm_status tlm_stub_unitarity_error(int device, float epsr, float *err);
 
+/* ---- batched execution of many grids -------------------------------- */
+
+/* No single counterpart in the reference, whose UI runs one TlmSolver at a
+ * time (MainUnit.cpp:872-991). A batch advances many handles -- each set up
+ * as usual with tlm_setup / tlm_add_port / tlm_add_probe ... -- with one
+ * kernel launch per step for all of them (per storage mode and tile shape),
+ * in windows of steps_per_launch steps captured as CUDA graphs. Each member
+ * runs from its current step to its own total_steps and stops there. While
+ * attached, a handle is stepped only by its batch (tlm_step/tlm_run on it
+ * return TLM_ESTATE); its results are read with the ordinary getters and are
+ * bitwise those it would get stepped alone. */
+typedef struct tlm_batch_s *tlm_batch;
+
+typedef struct tlm_batch_tuning {
+    int kernel_variant;    /* step-kernel tile shape (see tlm_kernel_variants) */
+    int steps_per_launch;  /* steps per window (graph) */
+    int blocks_per_sm;     /* resident step-kernel blocks per SM, 0 = all that fit */
+    int use_graphs;        /* 1: replay windows as CUDA graphs */
+    double ms_per_step;    /* autotuner: measured time per step of the batch */
+} tlm_batch_tuning;
+
+TLM_API tlm_status tlm_batch_create(tlm_batch *out, int device);
+/* Detaches every member (the handles stay valid) and frees the batch. */
+TLM_API tlm_status tlm_batch_destroy(tlm_batch b);
+TLM_API tlm_status tlm_batch_attach(tlm_batch b, tlm_handle h);
+TLM_API tlm_status tlm_batch_detach(tlm_batch b, tlm_handle h);
+/* Attached handles, and those not yet at their total_steps. */
+TLM_API int tlm_batch_size(tlm_batch b);
+TLM_API int tlm_batch_active(tlm_batch b);
+/* Advance every member by up to n_steps (none past its total_steps) and
+ * wait for the device. */
+TLM_API tlm_status tlm_batch_step(tlm_batch b, int n_steps);
+/* Advance until every member has reached its total_steps. */
+TLM_API tlm_status tlm_batch_run(tlm_batch b);
+TLM_API tlm_status tlm_batch_set_tuning(tlm_batch b, const tlm_batch_tuning *t);
+TLM_API tlm_status tlm_batch_get_tuning(tlm_batch b, tlm_batch_tuning *t);
+/* Time trial_windows windows of every tile shape (then of steps-per-launch
+ * 16/32/64/128 for the best shape) on the batch's own members, keep the
+ * fastest, and rewind every member to step 0 (fields zero). Call before the
+ * first step. Results are cached per (GPU, storage modes, size class), in
+ * the file named by TLM_AUTOTUNE_CACHE when that variable is set. */
+TLM_API tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *out);
+TLM_API tlm_status tlm_batch_get_stream(tlm_batch b, void **stream);
+
 /* ---- one step over caller-owned device memory, no allocation -------- */
 
 /* No counterpart in the reference. For callers that may not allocate device
