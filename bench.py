@@ -40,7 +40,15 @@ def parse():
     p.add_argument("--warmup", type=int, default=20)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="heterogeneous",
-                   choices=["heterogeneous", "plain", "precision"])
+                   choices=["heterogeneous", "plain", "precision", "batched", "served"])
+    p.add_argument("--instances", type=int, default=256, help="batched: number of instances")
+    p.add_argument("--requests", type=int, default=200, help="served: number of requests")
+    p.add_argument("--rate", type=float, default=200.0, help="served: mean arrivals per second")
+    p.add_argument("--edge-max", type=int, default=128,
+                   help="served: largest cubic edge (the full stream goes to 256)")
+    p.add_argument("--steps-max", type=int, default=2000,
+                   help="served: most steps per request (the full stream goes to 8000)")
+    p.add_argument("--autotune", action="store_true", help="batched: run the autotuner first")
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64"])
     p.add_argument("--steps-per-launch", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
@@ -306,10 +314,165 @@ def run_ours(args):
     dist.close()
 
 
+def sequential_solves(ws):
+    """Each instance alone through the plain API, one after the other:
+    setup, all steps, port DFT back to the host, free. Returns per-solve
+    seconds."""
+    from emsolver_b200.runner import build_solver
+    times = []
+    for w in ws:
+        t0 = time.perf_counter()
+        s = build_solver(w)
+        s.step(w.steps)
+        s.portDft(0)
+        s.close()
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def run_batched(args):
+    """256 independent dipole instances, edges U{24..96}, 1000 steps each."""
+    import torch
+    from emsolver_b200 import Batch, workloads
+    from emsolver_b200.runner import build_solver
+    ws = workloads.batched_instances(count=args.instances, steps=1000)
+    nodes = sum(w.ncells for w in ws)
+    work = sum(w.ncells * w.steps for w in ws)
+    bytes_all = sum(w.bytes_per_step() * w.steps for w in ws)
+    sequential_solves(ws[:4])                        # warm-up (context, kernels)
+    seq = sequential_solves(ws)
+    t0 = time.perf_counter()
+    solvers = [build_solver(w) for w in ws]
+    b = Batch()
+    for s in solvers:
+        b.attach(s)
+    tuning = b.autotune(trial_windows=2) if args.autotune else b.get_tuning()
+    t1 = time.perf_counter()
+    ext = torch.cuda.ExternalStream(b.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    b.run()
+    e1.record(ext)
+    torch.cuda.synchronize()
+    gpu_ms = e0.elapsed_time(e1)
+    for s in solvers:
+        s.portDft(0)
+    t2 = time.perf_counter()
+    b.close()
+    for s in solvers:
+        s.close()
+    t3 = time.perf_counter()
+    batched_s = t3 - t0
+    peak, kind = peaks()
+    line = {
+        "metric": "batched solves/s", "value": len(ws) / batched_s, "unit": "solves/s",
+        "n_gpus": 1, "steps": 1000, "warmup": 4, "ms_per_step": gpu_ms / 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"batched: {len(ws)} dipole instances, edges U{{24..96}}, 1000 steps",
+                   "nodes": nodes, "tuning": tuning.__dict__,
+                   "includes": "setup of every instance, all steps, port DFT read-back, free"},
+        "sequential_plain_gpu": {"value": len(ws) / sum(seq), "unit": "solves/s",
+                                 "seconds": sum(seq), "p50_s": float(np.percentile(seq, 50)),
+                                 "p99_s": float(np.percentile(seq, 99))},
+        "speedup_vs_sequential": sum(seq) / batched_s,
+        "batched_gpu": {"node_updates_per_s": work / (gpu_ms / 1e3), "seconds": gpu_ms / 1e3,
+                        "setup_s": t1 - t0, "readback_s": t2 - t1 - gpu_ms / 1e3,
+                        "hbm_frac": bytes_all / (gpu_ms / 1e3) / 1e9 / peak, "peak_kind": kind},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_served(args):
+    """Poisson arrivals of dipole solves (edge log-uniform, steps uniform,
+    FP32 or BF16 storage with probability 0.5), scaled by --edge-max and
+    --steps-max; latency percentiles beside solves/s, against the same
+    stream served one solve at a time by the plain API."""
+    import threading
+    from emsolver_b200 import Server, workloads
+    from emsolver_b200.runner import build_solver
+    from emsolver_b200.solver import s11_from_dft
+    stream = workloads.request_stream(count=args.requests, rate=args.rate, edge_hi=args.edge_max,
+                                      steps_hi=args.steps_max)
+    arrivals = [t for t, _ in stream]
+    ws = [w for _, w in stream]
+    for w in ws:
+        w.dft_freqs = w.dft_freqs[:16]
+    sequential_solves([ws[0]])
+    seq = sequential_solves(ws)
+    # plain FIFO single-solve server on the same arrival stream
+    done = 0.0
+    plain_lat = []
+    for a, svc in zip(arrivals, seq):
+        done = max(done, a) + svc
+        plain_lat.append(done - a)
+    plain_span = done - arrivals[0]
+    srv = Server(steps_per_launch=64)
+    ids = [None] * len(ws)
+    t0 = time.perf_counter()
+
+    def feeder():
+        for k, (a, w) in enumerate(zip(arrivals, ws)):
+            now = time.perf_counter() - t0
+            if a > now:
+                time.sleep(a - now)
+            ids[k] = srv.submit(w)
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    for rid in ids:
+        srv.wait(rid, -1.0)
+    t1 = time.perf_counter()
+    lat = []
+    for rid in ids:
+        lat.append(srv.result(rid)[2])
+    st = srv.stats()
+    # S11 of sampled requests against the FP64 storage mode
+    errs = {}
+    for k in range(min(4, len(ws))):
+        w = ws[k]
+        v, i, _ = srv.result(ids[k])
+        r = build_solver(w, storage=3)
+        r.step(w.steps)
+        rv, ri = r.portDft(0)
+        r.close()
+        s_srv, s_ref = s11_from_dft(v, i)[1], s11_from_dft(rv, ri)[1]
+        errs[f"{w.name}_{'bf16' if w.storage == 1 else 'f32'}"] = float(
+            np.max(np.abs(s_srv - s_ref) / np.abs(s_ref)))
+    srv.close()
+    span = t1 - t0
+    work = sum(w.ncells * w.steps for w in ws)
+    line = {
+        "metric": "served solves/s", "value": len(ws) / span, "unit": "solves/s", "n_gpus": 1,
+        "steps": len(ws), "warmup": 1, "ms_per_step": 1000.0 * span / len(ws),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 or bf16 storage per request", "data": "synthetic (seeded Poisson stream)",
+        "config": {"workload": f"served: {len(ws)} requests, Poisson {args.rate}/s, cubic edge "
+                               f"log-U[32,{args.edge_max}], steps U[500,{args.steps_max}]",
+                   "node_updates": work},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "mean": float(np.mean(lat))},
+        "plain_sequential": {"solves_per_s": len(ws) / plain_span,
+                             "latency_p50_s": float(np.percentile(plain_lat, 50)),
+                             "latency_p99_s": float(np.percentile(plain_lat, 99)),
+                             "busy_s": sum(seq)},
+        "speedup_vs_plain": plain_span / span,
+        "node_updates_per_s": work / span,
+        "s11_rel_err_vs_fp64": errs,
+        "server": st,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "batched":
+        run_batched(args)
+    elif args.workload == "served":
+        run_served(args)
     else:
         run_ours(args)
 

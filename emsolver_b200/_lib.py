@@ -49,6 +49,26 @@ class BatchTuningC(C.Structure):
                 ("blocks_per_sm", C.c_int), ("use_graphs", C.c_int), ("ms_per_step", C.c_double)]
 
 
+class RequestC(C.Structure):
+    _fields_ = [("grid", Grid), ("mat", C.POINTER(C.c_uint8)), ("n_cells", C.c_size_t),
+                ("table", C.POINTER(MatPropsC)), ("n_table", C.c_int), ("cfg", ConfigC),
+                ("source_table", C.POINTER(C.c_float)), ("n_source", C.c_int),
+                ("n_ports", C.c_int), ("port_cells", C.POINTER(C.c_uint64)),
+                ("port_ncells", C.POINTER(C.c_int)), ("port_pol", C.POINTER(C.c_int)),
+                ("port_amp", C.POINTER(C.c_float)), ("n_probes", C.c_int),
+                ("probe_ijk", C.POINTER(C.c_int)), ("n_freq", C.c_int),
+                ("freqs", C.POINTER(C.c_double))]
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = [("completed", C.c_longlong), ("failed", C.c_longlong), ("cancelled", C.c_longlong),
+                ("queued", C.c_longlong), ("running", C.c_longlong),
+                ("latency_p50_s", C.c_double), ("latency_p99_s", C.c_double),
+                ("latency_mean_s", C.c_double), ("solves_per_s", C.c_double),
+                ("hbm_used_bytes", C.c_size_t), ("hbm_budget_bytes", C.c_size_t),
+                ("windows", C.c_longlong), ("busy_s", C.c_double)]
+
+
 _h = C.c_void_p
 _st = C.c_int
 _P = C.POINTER
@@ -117,10 +137,26 @@ SIGNATURES = {
     "tlm_batch_active": (C.c_int, [_h]),
     "tlm_batch_step": (_st, [_h, C.c_int]),
     "tlm_batch_run": (_st, [_h]),
+    "tlm_batch_launch_window": (_st, [_h, _P(C.c_int)]),
+    "tlm_batch_sync": (_st, [_h]),
     "tlm_batch_set_tuning": (_st, [_h, _P(BatchTuningC)]),
     "tlm_batch_get_tuning": (_st, [_h, _P(BatchTuningC)]),
     "tlm_batch_autotune": (_st, [_h, C.c_int, _P(BatchTuningC)]),
     "tlm_batch_get_stream": (_st, [_h, _P(C.c_void_p)]),
+    "tlm_server_create": (_st, [_P(_h), C.c_int, C.c_size_t, C.c_int]),
+    "tlm_server_destroy": (_st, [_h]),
+    "tlm_server_submit": (_st, [_h, _P(RequestC), _P(C.c_uint64)]),
+    "tlm_server_poll": (_st, [_h, C.c_uint64, _P(C.c_int)]),
+    "tlm_server_wait": (_st, [_h, C.c_uint64, C.c_double, _P(C.c_int)]),
+    "tlm_server_cancel": (_st, [_h, C.c_uint64]),
+    "tlm_server_result": (_st, [_h, C.c_uint64, C.c_int, _P(C.c_double), _P(C.c_double),
+                                _P(C.c_double), _P(C.c_double), C.c_int, _P(C.c_int),
+                                _P(C.c_double)]),
+    "tlm_server_port_records": (_st, [_h, C.c_uint64, C.c_int, _P(C.c_float), _P(C.c_float),
+                                      C.c_int, _P(C.c_int)]),
+    "tlm_server_release": (_st, [_h, C.c_uint64]),
+    "tlm_server_stats": (_st, [_h, _P(ServerStatsC)]),
+    "tlm_request_footprint": (_st, [_P(RequestC), _P(C.c_size_t)]),
     "tlm_get_stream": (_st, [_h, _P(C.c_void_p)]),
     "tlm_device_bytes": (_st, [_h, _P(C.c_size_t)]),
     "tlm_set_kernel_timing": (_st, [_h, C.c_int]),

@@ -50,6 +50,7 @@ struct Group
     int *dNTiles = nullptr;
     int gridBlocks = 0;         // resident blocks of the step kernel
     size_t descBytes = 0;
+    bool dirty = true;          // host tables changed since the last upload
 };
 
 int keyOf(int storage, int variant) { return storage * 16 + variant; }
@@ -385,12 +386,30 @@ tlm_status readyMember(tlm_batch_s *b, tlm_solver *h)
 
 tlm_status refreshAll(tlm_batch_s *b)
 {
-    for (auto &kv : b->groups) TLM_TRY(syncGroupTables(b, kv.second));
+    for (auto &kv : b->groups)
+    {
+        TLM_TRY(syncGroupTables(b, kv.second));
+        kv.second.dirty = false;
+    }
+    return TLM_OK;
+}
+
+// Upload the tables of groups whose membership changed (attach / detach are
+// cheap; the upload happens once before the next window).
+tlm_status refreshDirty(tlm_batch_s *b)
+{
+    for (auto &kv : b->groups)
+        if (kv.second.dirty)
+        {
+            TLM_TRY(syncGroupTables(b, kv.second));
+            kv.second.dirty = false;
+        }
     return TLM_OK;
 }
 
 tlm_status runWindows(tlm_batch_s *b, int nsteps)
 {
+    TLM_TRY(refreshDirty(b));
     int remaining = nsteps;
     while (remaining > 0 && activeMembers(b) > 0)
     {
@@ -538,8 +557,9 @@ tlm_status tlm_batch_create(tlm_batch *out, int device)
     tlm_batch_s *b = new tlm_batch_s();
     b->device = device;
     BatchDeviceGuard dg(device);
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) b->smCount = prop.multiProcessorCount;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+        b->smCount = sms;
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
 #ifdef TLM_CHECKED
     if (e == cudaSuccess) e = cudaMalloc(&b->dFault, sizeof(unsigned));
@@ -599,8 +619,9 @@ tlm_status tlm_batch_attach(tlm_batch b, tlm_handle h)
     g.variant = h->variant;
     g.descBytes = descSize(h->storage);
     g.members.push_back(h);
+    g.dirty = true;
     h->batch = b;
-    return syncGroupTables(b, g);
+    return TLM_OK;
 }
 
 tlm_status tlm_batch_detach(tlm_batch b, tlm_handle h)
@@ -614,8 +635,9 @@ tlm_status tlm_batch_detach(tlm_batch b, tlm_handle h)
     TLM_BCU(b, cudaStreamSynchronize(b->stream));
     Group &g = b->groups[keyOf(h->storage, h->variant)];
     g.members.erase(std::remove(g.members.begin(), g.members.end(), h), g.members.end());
+    g.dirty = true;
     h->batch = nullptr;
-    return syncGroupTables(b, g);
+    return TLM_OK;
 }
 
 int tlm_batch_size(tlm_batch b)
@@ -637,6 +659,54 @@ tlm_status tlm_batch_step(tlm_batch b, int n_steps)
     }
     BatchDeviceGuard dg(b->device);
     return runWindows(b, n_steps);
+}
+
+tlm_status tlm_batch_launch_window(tlm_batch b, int *n_steps)
+{
+    if (!b)
+    {
+        setThreadError("null batch");
+        return TLM_EINVAL;
+    }
+    if (n_steps) *n_steps = 0;
+    BatchDeviceGuard dg(b->device);
+    TLM_TRY(refreshDirty(b));
+    if (activeMembers(b) == 0) return TLM_OK;
+    if (b->useGraph)
+    {
+        if (b->graphDirty || !b->graph) TLM_TRY(captureGraph(b));
+        TLM_BCU(b, cudaGraphLaunch(b->graph, b->stream));
+    }
+    else
+        TLM_TRY(enqueueWindow(b, b->window));
+    advanceMembers(b, b->window);
+    // members that finished in this window leave the tile table at the next
+    // upload (until then their tiles are skipped on the device)
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members)
+            if (h->curStep >= h->cfg.total_steps && h->curStep - b->window < h->cfg.total_steps)
+                kv.second.dirty = true;
+    if (n_steps) *n_steps = b->window;
+    return TLM_OK;
+}
+
+tlm_status tlm_batch_sync(tlm_batch b)
+{
+    if (!b)
+    {
+        setThreadError("null batch");
+        return TLM_EINVAL;
+    }
+    BatchDeviceGuard dg(b->device);
+    TLM_BCU(b, cudaStreamSynchronize(b->stream));
+    for (auto &kv : b->groups)
+        for (tlm_solver *h : kv.second.members)
+        {
+            double e = 0.0;
+            TLM_BCU(b, cudaMemcpy(&e, h->dElatest, sizeof(double), cudaMemcpyDeviceToHost));
+            h->energy.store((float)e);
+        }
+    return TLM_OK;
 }
 
 tlm_status tlm_batch_run(tlm_batch b)
@@ -700,6 +770,7 @@ tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *
         for (tlm_solver *h : kv.second.members)
             if (h->curStep != 0) return b->fail(TLM_ESTATE, "autotune runs before the first step");
     if (tlm_batch_size(b) == 0) return b->fail(TLM_ESTATE, "the batch has no members");
+    TLM_TRY(refreshDirty(b));
     const std::string key = tuneKey(b);
     {
         std::lock_guard<std::mutex> lk(g_tuneMutex);

@@ -92,6 +92,7 @@ struct tlm_solver
 {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
     std::string err;
 
     std::atomic<bool> running{ false };
@@ -186,42 +187,43 @@ struct tlm_solver
 
 namespace tlmi {
 
+// Device memory of a handle comes from a per-device stream-ordered pool that
+// keeps freed blocks for reuse (no device-wide synchronisation and no
+// driver round trip per allocation), ordered on the handle's stream.
 template <class T> tlm_status devAlloc(tlm_solver *h, T **p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) return TLM_OK;
     void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, bytes);
+    cudaError_t e = cudaMallocFromPoolAsync(&q, bytes, h->pool, h->stream);
     if (e != cudaSuccess)
     {
         cudaGetLastError();
-        return h->fail(TLM_ENOMEM, "cudaMalloc of " + std::to_string(bytes) +
+        return h->fail(TLM_ENOMEM, "device allocation of " + std::to_string(bytes) +
                                        " bytes failed: " + cudaGetErrorString(e));
     }
     h->devBytes += bytes;
     *p = static_cast<T *>(q);
     return TLM_OK;
 }
-
 // Short-lived buffers of one API call (not counted in the handle's bytes).
 template <class T> tlm_status tmpAlloc(tlm_solver *h, T **p, size_t bytes)
 {
     void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, bytes > 0 ? bytes : 1);
+    cudaError_t e = cudaMallocFromPoolAsync(&q, bytes > 0 ? bytes : 1, h->pool, h->stream);
     if (e != cudaSuccess)
     {
         cudaGetLastError();
         *p = nullptr;
-        return h->fail(TLM_ENOMEM, std::string("temporary cudaMalloc failed: ") + cudaGetErrorString(e));
+        return h->fail(TLM_ENOMEM, std::string("temporary device allocation failed: ") +
+                                       cudaGetErrorString(e));
     }
     *p = static_cast<T *>(q);
     return TLM_OK;
 }
-
 template <class T> void devFree(tlm_solver *h, T *&p)
 {
-    (void)h;
-    if (p) cudaFree((void *)p);
+    if (p) cudaFreeAsync((void *)p, h->stream);
     p = nullptr;
 }
 
@@ -244,5 +246,9 @@ tlm_status uploadSourceTable(tlm_solver *h, long long steps);
 tlm_status setWindow(tlm_solver *h, int window);
 tlm_status rewind(tlm_solver *h);
 tlm_status reshape(tlm_solver *h, int variant);
+// The library's memory pool on a device (created on first use) and the
+// bytes it could hand out: free device memory plus blocks it keeps for reuse.
+cudaMemPool_t devicePool(int device);
+size_t poolAvailable(int device);
 
 } // namespace tlmi

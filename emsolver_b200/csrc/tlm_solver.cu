@@ -493,13 +493,15 @@ tlm_status uploadSourceTable(tlm_solver *h, long long steps)
     for (long long n = 0; n < steps; ++n) v64[(size_t)n] = sourceValue(h, (int)n);
     if (h->storage == TLM_STORE_F64)
     {
-        TLM_CU(h, cudaMemcpy(h->dSv, v64.data(), v64.size() * 8, cudaMemcpyHostToDevice));
+        TLM_CU(h, cudaMemcpyAsync(h->dSv, v64.data(), v64.size() * 8, cudaMemcpyHostToDevice, h->stream));
+        TLM_CU(h, cudaStreamSynchronize(h->stream));
     }
     else
     {
         std::vector<float> v32(v64.size());
         for (size_t t = 0; t < v64.size(); ++t) v32[t] = (float)v64[t];
-        TLM_CU(h, cudaMemcpy(h->dSv, v32.data(), v32.size() * 4, cudaMemcpyHostToDevice));
+        TLM_CU(h, cudaMemcpyAsync(h->dSv, v32.data(), v32.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        TLM_CU(h, cudaStreamSynchronize(h->stream));
     }
     h->svCount = steps;
     return TLM_OK;
@@ -561,6 +563,51 @@ tlm_status reshape(tlm_solver *h, int variant)
     return TLM_OK;
 }
 
+cudaMemPool_t devicePool(int device)
+{
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)pools.size() <= device) pools.resize(device + 1, nullptr);
+    if (!pools[device])
+    {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = UINT64_MAX;  // keep freed blocks for reuse
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
+size_t poolAvailable(int device)
+{
+    size_t freeB = 0, totalB = 0;
+    if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaMemPool_t pool = devicePool(device);
+    uint64_t reserved = 0, used = 0;
+    if (pool)
+    {
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    }
+    return freeB + (size_t)(reserved > used ? reserved - used : 0);
+}
+
 int gridBlocksFor(long long n)
 {
     long long b = (n + 255) / 256;
@@ -585,7 +632,7 @@ template <class S, class O> static tlm_status pulsesToHost(tlm_solver *h, O *out
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, need * sizeof(O), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(d);
+    cudaFreeAsync(d, h->stream);
     return h->cuda(e, "incident state export");
 }
 
@@ -619,7 +666,7 @@ template <class S> static tlm_status setPulsesT(tlm_solver *h, const float *in)
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(d);
+    cudaFreeAsync(d, h->stream);
     TLM_CU(h, e);
     h->stateIncident = true;
     return TLM_OK;
@@ -691,17 +738,26 @@ tlm_status tlm_create(tlm_handle *out, int device)
         g_threadError = "device index out of range";
         return TLM_EINVAL;
     }
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10)
+    int major = 0, minor = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device) != cudaSuccess ||
+        major < 10)
     {
         cudaGetLastError();
         g_threadError = "the kernels are built for sm_100a; device " + std::to_string(device) +
-                        " is sm_" + std::to_string(prop.major) + std::to_string(prop.minor);
+                        " is sm_" + std::to_string(major) + std::to_string(minor);
         return TLM_ENODEV;
     }
     tlm_solver *h = new tlm_solver();
     h->device = device;
     DeviceGuard dg(device);
+    h->pool = devicePool(device);
+    if (!h->pool)
+    {
+        g_threadError = "could not create the device memory pool";
+        delete h;
+        return TLM_ECUDA;
+    }
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess)
     {
@@ -709,12 +765,13 @@ tlm_status tlm_create(tlm_handle *out, int device)
         delete h;
         return TLM_ECUDA;
     }
-    e = cudaMalloc(&h->dElatest, sizeof(double));
-    if (e == cudaSuccess) e = cudaMemset(h->dElatest, 0, sizeof(double));
+    e = cudaMallocFromPoolAsync((void **)&h->dElatest, sizeof(double), h->pool, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->dElatest, 0, sizeof(double), h->stream);
 #ifdef TLM_CHECKED
-    if (e == cudaSuccess) e = cudaMalloc(&h->dFault, sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMemset(h->dFault, 0, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&h->dFault, sizeof(unsigned), h->pool, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->dFault, 0, sizeof(unsigned), h->stream);
 #endif
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess)
     {
         g_threadError = std::string("cudaMalloc: ") + cudaGetErrorString(e);
@@ -734,8 +791,8 @@ tlm_status tlm_destroy(tlm_handle h)
     DeviceGuard dg(h->device);
     cudaStreamSynchronize(h->stream);
     freeAll(h);
-    if (h->dElatest) cudaFree(h->dElatest);
-    if (h->dFault) cudaFree(h->dFault);
+    if (h->dElatest) cudaFreeAsync(h->dElatest, h->stream);
+    if (h->dFault) cudaFreeAsync(h->dFault, h->stream);
     for (cudaEvent_t ev : h->evs) cudaEventDestroy(ev);
     cudaStreamDestroy(h->stream);
     delete h;
@@ -845,8 +902,7 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     const size_t sb = storageBytes(h->storage), rb = realBytes(h->storage);
     const size_t need = 2 * 12 * (size_t)h->P * sb + (anyDiel ? 3 * (size_t)h->P * rb : 0) +
                         (size_t)h->P + (size_t)h->nblocks * 8 * 8;
-    size_t freeB = 0, totalB = 0;
-    TLM_CU(h, cudaMemGetInfo(&freeB, &totalB));
+    const size_t freeB = poolAvailable(h->device);
     if (need + (size_t)(256u << 20) > freeB)
         return h->fail(TLM_ENOMEM, "grid needs " + std::to_string(need >> 20) + " MiB of HBM, " +
                                        std::to_string(freeB >> 20) + " MiB free");
@@ -874,15 +930,20 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     TLM_TRY(devAlloc(h, &h->dGhat, h->ghat32.size() * rb));
     if (h->storage == TLM_STORE_F64)
     {
-        TLM_CU(h, cudaMemcpy(h->dYhat, h->yhat64.data(), h->yhat64.size() * 8, cudaMemcpyHostToDevice));
-        TLM_CU(h, cudaMemcpy(h->dGhat, h->ghat64.data(), h->ghat64.size() * 8, cudaMemcpyHostToDevice));
+        TLM_CU(h, cudaMemcpyAsync(h->dYhat, h->yhat64.data(), h->yhat64.size() * 8,
+                                  cudaMemcpyHostToDevice, h->stream));
+        TLM_CU(h, cudaMemcpyAsync(h->dGhat, h->ghat64.data(), h->ghat64.size() * 8,
+                                  cudaMemcpyHostToDevice, h->stream));
     }
     else
     {
-        TLM_CU(h, cudaMemcpy(h->dYhat, h->yhat32.data(), h->yhat32.size() * 4, cudaMemcpyHostToDevice));
-        TLM_CU(h, cudaMemcpy(h->dGhat, h->ghat32.data(), h->ghat32.size() * 4, cudaMemcpyHostToDevice));
+        TLM_CU(h, cudaMemcpyAsync(h->dYhat, h->yhat32.data(), h->yhat32.size() * 4,
+                                  cudaMemcpyHostToDevice, h->stream));
+        TLM_CU(h, cudaMemcpyAsync(h->dGhat, h->ghat32.data(), h->ghat32.size() * 4,
+                                  cudaMemcpyHostToDevice, h->stream));
     }
-    TLM_CU(h, cudaMemset(h->dElatest, 0, sizeof(double)));
+    TLM_CU(h, cudaMemsetAsync(h->dElatest, 0, sizeof(double), h->stream));
+    TLM_CU(h, cudaStreamSynchronize(h->stream));
     h->configured = true;
     return TLM_OK;
 }
@@ -1270,7 +1331,7 @@ tlm_status tlm_get_stubs(tlm_handle h, float *out, size_t cap)
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, need * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(d);
+    cudaFreeAsync(d, h->stream);
     return h->cuda(e, "stub export");
 }
 

@@ -290,6 +290,12 @@ TLM_API int tlm_batch_active(tlm_batch b);
 TLM_API tlm_status tlm_batch_step(tlm_batch b, int n_steps);
 /* Advance until every member has reached its total_steps. */
 TLM_API tlm_status tlm_batch_run(tlm_batch b);
+/* Queue one window (steps_per_launch steps) without waiting, so the caller
+ * can prepare new members while the GPU works; *n_steps gets the window
+ * length (0 when no member is active). Follow with tlm_batch_sync before
+ * attaching, detaching or reading members. */
+TLM_API tlm_status tlm_batch_launch_window(tlm_batch b, int *n_steps);
+TLM_API tlm_status tlm_batch_sync(tlm_batch b);
 TLM_API tlm_status tlm_batch_set_tuning(tlm_batch b, const tlm_batch_tuning *t);
 TLM_API tlm_status tlm_batch_get_tuning(tlm_batch b, tlm_batch_tuning *t);
 /* Time trial_windows windows of every tile shape (then of steps-per-launch
@@ -299,6 +305,75 @@ TLM_API tlm_status tlm_batch_get_tuning(tlm_batch b, tlm_batch_tuning *t);
  * the file named by TLM_AUTOTUNE_CACHE when that variable is set. */
 TLM_API tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *out);
 TLM_API tlm_status tlm_batch_get_stream(tlm_batch b, void **stream);
+
+/* ---- continuous-batching request server ------------------------------ */
+
+/* No counterpart in the reference (a desktop application running one solve
+ * at a time). Requests are complete solves; a worker thread admits queued
+ * requests in arrival order while their device footprint fits the HBM
+ * budget, keeps their state resident on the GPU, advances all running
+ * requests together in a batch one window at a time, and retires each at its
+ * total_steps. Requests that arrive while others run join the batch at the
+ * next window. Each result equals the same solve run alone with
+ * tlm_setup/tlm_run. */
+typedef struct tlm_server_s *tlm_server;
+
+enum { TLM_REQ_QUEUED = 0, TLM_REQ_RUNNING = 1, TLM_REQ_DONE = 2, TLM_REQ_FAILED = 3,
+       TLM_REQ_CANCELLED = 4 };
+
+typedef struct tlm_request {
+    tlm_grid grid;
+    const uint8_t *mat;             /* n_cells = nx*ny*nz material ids */
+    size_t n_cells;
+    const tlm_matprops *table;      /* n_table dielectric entries */
+    int n_table;
+    tlm_config cfg;                 /* waveform, total_steps, rho, storage ... */
+    const float *source_table;      /* for TLM_WAVE_TABLE, n_source values */
+    int n_source;
+    int n_ports;                    /* ports: cells concatenated, count per port */
+    const uint64_t *port_cells;
+    const int *port_ncells;
+    const int *port_pol;
+    const float *port_amp;
+    int n_probes;                   /* probes: i,j,k per probe */
+    const int *probe_ijk;
+    int n_freq;                     /* port DFT frequencies (Hz) */
+    const double *freqs;
+} tlm_request;
+
+typedef struct tlm_server_stats_t {
+    long long completed, failed, cancelled, queued, running;
+    double latency_p50_s, latency_p99_s, latency_mean_s;  /* submit -> done */
+    double solves_per_s;            /* completed / (last completion - start) */
+    size_t hbm_used_bytes, hbm_budget_bytes;
+    long long windows;
+    double busy_s;                  /* time spent stepping */
+} tlm_server_stats_t;
+
+/* hbm_budget_bytes 0 = 80% of the device's free memory; steps_per_launch 0
+ * = 64 (the admission / retirement granularity). */
+TLM_API tlm_status tlm_server_create(tlm_server *out, int device, size_t hbm_budget_bytes,
+                                     int steps_per_launch);
+/* Stops the worker; queued and running requests end CANCELLED. */
+TLM_API tlm_status tlm_server_destroy(tlm_server s);
+/* Copies the request and queues it; TLM_ENOMEM if it can never fit. */
+TLM_API tlm_status tlm_server_submit(tlm_server s, const tlm_request *req, uint64_t *id);
+TLM_API tlm_status tlm_server_poll(tlm_server s, uint64_t id, int *state);
+/* Wait until the request ends (timeout_s < 0: no limit); TLM_ETIMEOUT if it
+ * has not ended in time. */
+TLM_API tlm_status tlm_server_wait(tlm_server s, uint64_t id, double timeout_s, int *state);
+TLM_API tlm_status tlm_server_cancel(tlm_server s, uint64_t id);
+/* FP64 DFT of a finished request's port (and its latency). */
+TLM_API tlm_status tlm_server_result(tlm_server s, uint64_t id, int port, double *v_re,
+                                     double *v_im, double *i_re, double *i_im, int cap,
+                                     int *n_freq, double *latency_s);
+TLM_API tlm_status tlm_server_port_records(tlm_server s, uint64_t id, int port, float *v,
+                                           float *i, int cap, int *n_out);
+/* Forget a finished request (frees its results). */
+TLM_API tlm_status tlm_server_release(tlm_server s, uint64_t id);
+TLM_API tlm_status tlm_server_stats(tlm_server s, tlm_server_stats_t *out);
+/* Device bytes a request holds while it runs (what admission counts). */
+TLM_API tlm_status tlm_request_footprint(const tlm_request *req, size_t *bytes);
 
 /* ---- one step over caller-owned device memory, no allocation -------- */
 

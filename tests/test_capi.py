@@ -85,3 +85,16 @@ def test_no_device_fails_loudly(built):
     assert L.tlm_last_error(None)
     e = C.c_float()
     assert L.tlm_scatter_unitarity_error(0, C.byref(e)) == _lib.TLM_ENODEV
+
+
+def test_request_footprint_without_device(built):
+    """Admission arithmetic is host-only: FP32 pulses take twice the bytes of
+    BF16, and a dielectric adds the stub planes."""
+    from emsolver_b200 import workloads
+    from emsolver_b200.server import footprint
+    w = workloads.dipole(32, 32, 48, 21, steps=500)
+    f32, bf16 = footprint(w, storage=0), footprint(w, storage=1)
+    P = 32 * 32 * 48
+    assert f32 - bf16 == 2 * 12 * P * 2
+    w2 = workloads.dipole(32, 32, 48, 21, slab=(2, 6, 3.0), steps=500)
+    assert footprint(w2, storage=0) - f32 == 3 * P * 4
