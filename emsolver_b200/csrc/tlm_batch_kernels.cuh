@@ -5,8 +5,9 @@
 // ordinary solver handle). A tile table lists (member, tile) pairs, one tile
 // = kBlock threads x V nodes of one member, exactly the tiles the single-grid
 // kernel would launch as blocks. The step kernel runs a fixed grid of
-// resident blocks that stride over the tile table; the member table and the
-// tile count live in device memory, so a CUDA graph of W steps captured once
+// resident blocks, each walking a contiguous chunk of the tile table; the
+// member table and the tile count live in device memory, so a CUDA graph of
+// W steps captured once
 // stays valid while members join and leave between windows. Each member
 // advances from its own current step `base + i` and stops at its own
 // `total`. The per-tile arithmetic is stepTile, the same code as the
@@ -50,47 +51,64 @@ __global__ void __launch_bounds__(kBlock, MINB)
     __shared__ double red[kBlock / 32];
     __shared__ StepArgs<S> sa;
     __shared__ int skip;
+    // Each block walks a contiguous chunk of the tile table: consecutive
+    // tiles mostly belong to the same member (its arguments are rebuilt only
+    // when the member changes) and are spatial neighbours (shared rows and
+    // planes stay in L2).
     const int nt = *ntiles;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x)
+    const int chunk = (nt + gridDim.x - 1) / gridDim.x;
+    const int t0 = blockIdx.x * chunk;
+    const int t1 = min(t0 + chunk, nt);
+    int current = -1;
+    for (int t = t0; t < t1; ++t)
     {
         const int2 tl = tiles[t];
-        if (threadIdx.x == 0)
+        if (tl.x != current)
         {
-            const MemberDesc<S> &d = members[tl.x];
-            const long long n = d.base + i;
-            skip = n >= d.total;
-            if (!skip)
+            __syncthreads();  // every thread is done with the previous member's arguments
+            if (threadIdx.x == 0)
             {
-                const long long eFirst = (d.base + 15) / 16 * 16;
-                sa.in = d.buf[n & 1];
-                sa.out = d.buf[(n + 1) & 1];
-                sa.stub = d.stub;
-                sa.mat = d.mat;
-                sa.yhat = d.yhat;
-                sa.ghat = d.ghat;
-                sa.P = d.P;
-                sa.nquads = d.nquads;
-                sa.nx = d.nx;
-                sa.ny = d.ny;
-                sa.nz = d.nz;
-                sa.px = d.px;
-                sa.nq = d.nq;
-                sa.rho = d.rho;
-                sa.scale = d.scale;
-                sa.inv_scale = d.inv_scale;
-                sa.tile_begin = d.tile_begin;
-                sa.spec = d.spec;
-                sa.sv = d.sv[n];
-                sa.samples = d.samples + (long long)i * d.nsamp * 6;
-                sa.epart = (n % 16 == 0) ? d.epart + ((n - eFirst) / 16) * d.nblocks : nullptr;
-                sa.fault = fault;
-                sa.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
-                sa.stochastic = d.stochastic;
+                const MemberDesc<S> &d = members[tl.x];
+                const long long n = d.base + i;
+                skip = n >= d.total;
+                if (!skip)
+                {
+                    const long long eFirst = (d.base + 15) / 16 * 16;
+                    sa.in = d.buf[n & 1];
+                    sa.out = d.buf[(n + 1) & 1];
+                    sa.stub = d.stub;
+                    sa.mat = d.mat;
+                    sa.yhat = d.yhat;
+                    sa.ghat = d.ghat;
+                    sa.P = d.P;
+                    sa.nquads = d.nquads;
+                    sa.nx = d.nx;
+                    sa.ny = d.ny;
+                    sa.nz = d.nz;
+                    sa.px = d.px;
+                    sa.nq = d.nq;
+                    sa.rho = d.rho;
+                    sa.scale = d.scale;
+                    sa.inv_scale = d.inv_scale;
+                    sa.tile_begin = d.tile_begin;
+                    sa.spec = d.spec;
+                    sa.sv = d.sv[n];
+                    sa.samples = d.samples + (long long)i * d.nsamp * 6;
+                    sa.epart = (n % 16 == 0) ? d.epart + ((n - eFirst) / 16) * d.nblocks : nullptr;
+                    sa.fault = fault;
+                    sa.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
+                    sa.stochastic = d.stochastic;
+                }
             }
+            __syncthreads();
+            current = tl.x;
         }
-        __syncthreads();
-        if (!skip) stepTile<S, V, false, SEL>(sa, tl.y, red);
-        __syncthreads();
+        if (!skip)
+        {
+            stepTile<S, V, false, SEL>(sa, tl.y, red);
+            // energy steps reduce through `red`: finish before the next tile reuses it
+            if (sa.epart != nullptr) __syncthreads();
+        }
     }
 }
 

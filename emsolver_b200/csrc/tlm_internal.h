@@ -68,10 +68,10 @@ inline int shapeCount(int storage)
 {
     switch (storage)
     {
-    case TLM_STORE_F64: return 3;
+    case TLM_STORE_F64: return (int)(sizeof(kShapesF64) / sizeof(Shape));
     case TLM_STORE_BF16:
-    case TLM_STORE_F16: return 4;
-    case TLM_STORE_F32: return 4;
+    case TLM_STORE_F16: return (int)(sizeof(kShapesHalf) / sizeof(Shape));
+    case TLM_STORE_F32: return (int)(sizeof(kShapesF32) / sizeof(Shape));
     default: return 0;
     }
 }
