@@ -1,7 +1,7 @@
 """Throughput of the B200 SCN TLM step (node-updates/s and % of HBM roofline).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload heterogeneous|plain|precision] [--storage f32|bf16|f16|f64]
+                    [--workload heterogeneous|plain|precision] [--storage f32|bf16|f16|f64|bfp16]
 
 A "step" is one TLM time step (inject, monitors, scatter, connect) of the
 whole grid. Default workload: 192^3 heterogeneous grid (16 lossy dielectric
@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--steps-max", type=int, default=2000,
                    help="served: most steps per request (the full stream goes to 8000)")
     p.add_argument("--autotune", action="store_true", help="batched: run the autotuner first")
-    p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64"])
+    p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64", "bfp16"])
     p.add_argument("--steps-per-launch", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -65,9 +65,10 @@ def make_workload(name, steps):
     return workloads.heterogeneous(steps=2000)
 
 
-STORAGE = {"f32": (0, 4, 4), "bf16": (1, 2, 4), "f16": (2, 2, 4), "f64": (3, 8, 8)}
+STORAGE = {"f32": (0, 4, 4), "bf16": (1, 2, 4), "f16": (2, 2, 4), "f64": (3, 8, 8), "bfp16": (4, 2, 4)}
 DTYPE = {"f32": "f32", "bf16": "bf16 storage / f32 arithmetic",
-         "f16": "f16 storage / f32 arithmetic", "f64": "f64"}
+         "f16": "f16 storage / f32 arithmetic", "f64": "f64",
+         "bfp16": "16-bit block floating point storage / f32 arithmetic"}
 
 
 # ---------------------------------------------------------------- distributed

@@ -17,7 +17,7 @@ TLM_OK, TLM_EINVAL, TLM_ENOMEM, TLM_ECUDA, TLM_ETIMEOUT, TLM_ESTOPPED, TLM_ESTAT
 STATUS_NAMES = {0: "TLM_OK", 1: "TLM_EINVAL", 2: "TLM_ENOMEM", 3: "TLM_ECUDA", 4: "TLM_ETIMEOUT",
                 5: "TLM_ESTOPPED", 6: "TLM_ESTATE", 7: "TLM_ENODEV", 8: "TLM_EBUSY"}
 
-STORE_F32, STORE_BF16, STORE_F16, STORE_F64 = range(4)
+STORE_F32, STORE_BF16, STORE_F16, STORE_F64, STORE_BFP16 = range(5)
 WAVE_CW_RAMPED, WAVE_GAUSSIAN_SINE, WAVE_GAUSSIAN_PULSE, WAVE_TABLE = range(4)
 
 

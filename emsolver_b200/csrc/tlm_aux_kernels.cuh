@@ -9,7 +9,7 @@
 //    with the device scatter functions.
 #pragma once
 
-#include "tlm_device.cuh"
+#include "tlm_step_kernel.cuh"
 
 namespace tlmk {
 
@@ -177,14 +177,14 @@ __global__ void incidentToAos(const S *__restrict__ refl, const uint8_t *__restr
         {
             const int ax = s >> 2, side = (s >> 1) & 1;
             const int qn = co[ax] + (side ? 1 : -1);
-            const R own = decode(refl[s * P + node], scale);
+            const R own = loadOne<S>(refl, s * P + node, scale);
             R v;
             if (qn < 0 || qn >= dims[ax])
                 v = rho * own;
             else
             {
                 const long long nb = node + (side ? st[ax] : -st[ax]);
-                v = (mat[nb] == kPec) ? -own : decode(refl[(s ^ 2) * P + nb], scale);
+                v = (mat[nb] == kPec) ? -own : loadOne<S>(refl, (s ^ 2) * P + nb, scale);
             }
             dst[s] = (O)v;
         }
@@ -204,29 +204,37 @@ __global__ void planesToAos(const S *__restrict__ planes, long long P, int nx, i
         const int j = (int)((c / nx) % ny);
         const int k = (int)(c / ((long long)nx * ny));
         const long long node = ((long long)k * ny + j) * px + i;
-        for (int s = 0; s < 12; ++s) out[c * 12 + s] = (O)decode(planes[s * P + node], scale);
+        for (int s = 0; s < 12; ++s) out[c * 12 + s] = (O)loadOne<S>(planes, s * P + node, scale);
     }
 }
 
-// Incident AoS state -> incident planes (PEC and padding nodes get 0).
+// Incident AoS state -> incident planes (PEC and padding nodes get 0), one
+// aligned group of 4 nodes per thread iteration (the unit of every storage
+// type, block floating point included).
 template <class S, class I>
 __global__ void aosToIncident(const I *__restrict__ in, const uint8_t *__restrict__ mat, long long P,
                               int nx, int ny, int nz, int px, typename Traits<S>::R inv_scale,
                               S *__restrict__ planes)
 {
     using R = typename Traits<S>::R;
-    for (long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x; node < P;
-         node += (long long)gridDim.x * blockDim.x)
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < P / 4;
+         g += (long long)gridDim.x * blockDim.x)
     {
-        const int i = (int)(node % px);
-        const long long r = node / px;
+        const long long node0 = g * 4;
+        const int i0 = (int)(node0 % px);
+        const long long r = node0 / px;
         const int j = (int)(r % ny), k = (int)(r / ny);
-        const bool real = i < nx && k < nz;
-        const long long c = ((long long)k * ny + j) * nx + i;
         for (int s = 0; s < 12; ++s)
         {
-            R v = (real && mat[node] != kPec) ? (R)in[c * 12 + s] : R(0);
-            planes[s * P + node] = encode<S>(v, inv_scale);
+            R v[4];
+            for (int c = 0; c < 4; ++c)
+            {
+                const int i = i0 + c;
+                const bool real = i < nx && k < nz && mat[node0 + c] != kPec;
+                const long long cell = ((long long)k * ny + j) * nx + i;
+                v[c] = real ? (R)in[cell * 12 + s] : R(0);
+            }
+            storeVec<S, 4>(planes, s * P + node0, v, inv_scale, false, 0u, s);
         }
     }
 }

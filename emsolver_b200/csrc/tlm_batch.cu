@@ -112,6 +112,7 @@ size_t descSize(int storage)
     case TLM_STORE_F64: return sizeof(MemberDesc<double>);
     case TLM_STORE_BF16: return sizeof(MemberDesc<__nv_bfloat16>);
     case TLM_STORE_F16: return sizeof(MemberDesc<__half>);
+    case TLM_STORE_BFP16: return sizeof(MemberDesc<tlmk::Bfp4>);
     default: return sizeof(MemberDesc<float>);
     }
 }
@@ -212,6 +213,7 @@ tlm_status syncGroupTables(tlm_batch_s *b, Group &g)
         case TLM_STORE_F64: { auto d = makeDesc<double>(h); std::memcpy(dst, &d, sizeof(d)); break; }
         case TLM_STORE_BF16: { auto d = makeDesc<__nv_bfloat16>(h); std::memcpy(dst, &d, sizeof(d)); break; }
         case TLM_STORE_F16: { auto d = makeDesc<__half>(h); std::memcpy(dst, &d, sizeof(d)); break; }
+        case TLM_STORE_BFP16: { auto d = makeDesc<tlmk::Bfp4>(h); std::memcpy(dst, &d, sizeof(d)); break; }
         default: { auto d = makeDesc<float>(h); std::memcpy(dst, &d, sizeof(d)); break; }
         }
         if (h->curStep < h->cfg.total_steps)
@@ -271,6 +273,11 @@ template <class S> tlm_status launchShape(tlm_batch_s *b, Group &g, int i, bool 
         if (g.variant == 2) return launchGroupStep<S, 2, 4, true>(b, g, i, go);
         return launchGroupStep<S, 4, 2, false>(b, g, i, go);
     }
+    else if constexpr (std::is_same<S, tlmk::Bfp4>::value)
+    {
+        if (g.variant == 1) return launchGroupStep<S, 4, 3, true>(b, g, i, go);
+        return launchGroupStep<S, 4, 2, false>(b, g, i, go);
+    }
     else
     {
         if (g.variant == 1) return launchGroupStep<S, 4, 3, true>(b, g, i, go);
@@ -286,6 +293,7 @@ tlm_status launchStep(tlm_batch_s *b, Group &g, int i, bool go = true)
     case TLM_STORE_F64: return launchShape<double>(b, g, i, go);
     case TLM_STORE_BF16: return launchShape<__nv_bfloat16>(b, g, i, go);
     case TLM_STORE_F16: return launchShape<__half>(b, g, i, go);
+    case TLM_STORE_BFP16: return launchShape<tlmk::Bfp4>(b, g, i, go);
     default: return launchShape<float>(b, g, i, go);
     }
 }
@@ -306,6 +314,10 @@ tlm_status launchEpilogue(tlm_batch_s *b, Group &g, int w)
     case TLM_STORE_F16:
         tlmk::batchEpilogue<__half><<<grid, 512, 0, b->stream>>>(
             static_cast<MemberDesc<__half> *>(g.dMembers), g.dNMembers, w);
+        break;
+    case TLM_STORE_BFP16:
+        tlmk::batchEpilogue<tlmk::Bfp4><<<grid, 512, 0, b->stream>>>(
+            static_cast<MemberDesc<tlmk::Bfp4> *>(g.dMembers), g.dNMembers, w);
         break;
     default:
         tlmk::batchEpilogue<float><<<grid, 512, 0, b->stream>>>(

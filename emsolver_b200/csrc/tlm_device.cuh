@@ -68,10 +68,110 @@ template <> struct Traits<__nv_bfloat16>
     static constexpr bool kScaled = true;
 };
 
+// 32-bit integer mixer (the MurmurHash3 finaliser): counter-based random
+// bits for stochastic rounding, a pure function of (node, slot, step).
+__host__ __device__ __forceinline__ unsigned mix32(unsigned h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// Block floating point, 16 bits per pulse: one 64-bit word holds an aligned
+// group of 4 consecutive x-nodes of one plane -- four 14-bit two's-complement
+// mantissas (bits 0-13, 14-27, 28-41, 42-55) and the group's biased binary
+// exponent (bits 56-63). Value = mantissa * 2^(E - 13), E = exponent - 127,
+// chosen so the group's largest magnitude uses the full 13 bits. Exponent 0
+// encodes an all-zero group.
+struct Bfp4
+{
+    unsigned long long w;
+};
+template <> struct Traits<Bfp4>
+{
+    using R = float;
+    static constexpr int V = 4;
+    static constexpr int kMinBlocks = 3;
+    static constexpr bool kSelect = false;
+    static constexpr bool kScaled = false;
+};
+
 template <class S, int V> struct alignas(sizeof(S) * V) Pack
 {
     S v[V];
 };
+
+__device__ __forceinline__ float bfpUnit(int biasedExp)
+{
+    // 2^(E - 13) for E = biasedExp - 127 (exponents below 2^-112 are flushed
+    // to zero by the encoder, so the result is a normal float)
+    return __int_as_float((biasedExp - 13) << 23);
+}
+
+__device__ __forceinline__ void bfpDecode(unsigned long long w, float (&v)[4])
+{
+    const int e = (int)(w >> 56);
+    const float unit = e ? bfpUnit(e) : 0.0f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+    {
+        const long long m = ((long long)(w << (50 - 14 * c))) >> 50;  // sign-extend 14 bits
+        v[c] = (float)(int)m * unit;
+    }
+}
+
+__device__ __forceinline__ float bfpDecodeOne(unsigned long long w, int c)
+{
+    const int e = (int)(w >> 56);
+    const long long m = ((long long)(w << (50 - 14 * c))) >> 50;
+    return e ? (float)(int)m * bfpUnit(e) : 0.0f;
+}
+
+// Encode 4 values; `r` (when stochastic) supplies random bits for unbiased
+// rounding of each mantissa.
+__device__ __forceinline__ unsigned long long bfpEncode(const float (&v)[4], bool stochastic,
+                                                        unsigned r)
+{
+    float M = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) M = fmaxf(M, fabsf(v[c]));
+    if (!(M > 0x1p-112f) || !(M < 0x1p126f)) return 0ull;  // zero, tiny, or not finite
+    int e = (int)((__float_as_uint(M) >> 23) & 0xff) + 1;       // biased E with M < 2^E
+    unsigned long long w = 0;
+#pragma unroll 1
+    for (int attempt = 0; attempt < 2; ++attempt)
+    {
+        const float q = __int_as_float((127 + 127 + 13 - e) << 23);  // 2^(13 - E)
+        int m[4];
+        int big = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+        {
+            const float x = v[c] * q;  // exact power-of-two scaling
+            if (stochastic)
+            {
+                const float u = (float)(mix32(r + (unsigned)c) >> 8) * (1.0f / 16777216.0f);  // [0, 1)
+                m[c] = __float2int_rd(x + u);
+            }
+            else
+                m[c] = __float2int_rn(x);
+            big = max(big, abs(m[c]));
+        }
+        if (big > 8191 && attempt == 0)
+        {
+            ++e;  // rounding reached 2^13: use the next binade
+            continue;
+        }
+        w = (unsigned long long)e << 56;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) w |= ((unsigned long long)(m[c] & 0x3fff)) << (14 * c);
+        break;
+    }
+    return w;
+}
 
 __device__ __forceinline__ float decode(float s, float) { return s; }
 __device__ __forceinline__ double decode(double s, double) { return s; }
@@ -92,18 +192,6 @@ template <> __device__ __forceinline__ __nv_bfloat16 encode<__nv_bfloat16>(float
 }
 template <class S> __device__ __forceinline__ S encode(double v, double);
 template <> __device__ __forceinline__ double encode<double>(double v, double) { return v; }
-
-// 32-bit integer mixer (the MurmurHash3 finaliser): counter-based random
-// bits for stochastic rounding, a pure function of (node, slot, step).
-__host__ __device__ __forceinline__ unsigned mix32(unsigned h)
-{
-    h ^= h >> 16;
-    h *= 0x85ebca6bu;
-    h ^= h >> 13;
-    h *= 0xc2b2ae35u;
-    h ^= h >> 16;
-    return h;
-}
 
 // Stochastic rounding to the storage type: round the magnitude up with
 // probability equal to the fraction of the gap it covers, so the rounding

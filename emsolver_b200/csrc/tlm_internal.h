@@ -46,7 +46,8 @@ inline size_t storageBytes(int storage)
     {
     case TLM_STORE_F64: return 8;
     case TLM_STORE_BF16:
-    case TLM_STORE_F16: return 2;
+    case TLM_STORE_F16:
+    case TLM_STORE_BFP16: return 2;
     default: return 4;
     }
 }
@@ -63,6 +64,8 @@ struct Shape
 constexpr Shape kShapesF32[] = { { 4, 3, 0 }, { 4, 3, 1 }, { 2, 4, 1 }, { 4, 2, 0 } };
 constexpr Shape kShapesF64[] = { { 1, 4, 1 }, { 1, 4, 0 }, { 2, 3, 0 } };
 constexpr Shape kShapesHalf[] = { { 4, 3, 0 }, { 4, 3, 1 }, { 2, 4, 1 }, { 8, 2, 0 } };
+// block floating point: a thread owns one 4-node group
+constexpr Shape kShapesBfp[] = { { 4, 3, 0 }, { 4, 3, 1 }, { 4, 2, 0 } };
 
 inline int shapeCount(int storage)
 {
@@ -71,6 +74,7 @@ inline int shapeCount(int storage)
     case TLM_STORE_F64: return (int)(sizeof(kShapesF64) / sizeof(Shape));
     case TLM_STORE_BF16:
     case TLM_STORE_F16: return (int)(sizeof(kShapesHalf) / sizeof(Shape));
+    case TLM_STORE_BFP16: return (int)(sizeof(kShapesBfp) / sizeof(Shape));
     case TLM_STORE_F32: return (int)(sizeof(kShapesF32) / sizeof(Shape));
     default: return 0;
     }
@@ -82,6 +86,7 @@ inline Shape shapeOf(int storage, int variant)
     case TLM_STORE_F64: return kShapesF64[variant];
     case TLM_STORE_BF16:
     case TLM_STORE_F16: return kShapesHalf[variant];
+    case TLM_STORE_BFP16: return kShapesBfp[variant];
     default: return kShapesF32[variant];
     }
 }

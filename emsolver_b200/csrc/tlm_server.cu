@@ -105,7 +105,7 @@ size_t footprintOf(const tlm_grid &g, const std::vector<uint8_t> &mat, const tlm
 {
     const size_t px = (size_t)((g.nx + 7) / 8 * 8);
     const size_t P = px * g.ny * g.nz;
-    const size_t sb = cfg.storage == TLM_STORE_F64 ? 8 : (cfg.storage == TLM_STORE_F32 ? 4 : 2);
+    const size_t sb = tlmi::storageBytes(cfg.storage);
     const size_t rb = cfg.storage == TLM_STORE_F64 ? 8 : 4;
     bool diel = false;
     for (uint8_t v : mat)

@@ -292,6 +292,11 @@ void launchShaped(const tlmk::StepArgs<S> &a, int variant, bool incident, int nb
         else if (variant == 2) launchWithShape<S, 2, 4, true>(a, incident, nblocks, st);
         else launchWithShape<S, 4, 2, false>(a, incident, nblocks, st);
     }
+    else if constexpr (std::is_same<S, tlmk::Bfp4>::value)
+    {
+        if (variant == 1) launchWithShape<S, 4, 3, true>(a, incident, nblocks, st);
+        else launchWithShape<S, 4, 2, false>(a, incident, nblocks, st);
+    }
     else
     {
         if (variant == 1) launchWithShape<S, 4, 3, true>(a, incident, nblocks, st);
@@ -410,6 +415,7 @@ tlm_status enqueueSteps(tlm_solver *h, int nsteps, bool honourStop, bool *stoppe
             case TLM_STORE_F64: TLM_TRY(launchStep<double>(h, n, i, eFirst)); break;
             case TLM_STORE_BF16: TLM_TRY(launchStep<__nv_bfloat16>(h, n, i, eFirst)); break;
             case TLM_STORE_F16: TLM_TRY(launchStep<__half>(h, n, i, eFirst)); break;
+            case TLM_STORE_BFP16: TLM_TRY(launchStep<tlmk::Bfp4>(h, n, i, eFirst)); break;
             default: TLM_TRY(launchStep<float>(h, n, i, eFirst)); break;
             }
         }
@@ -647,6 +653,7 @@ template <class O> static tlm_status getPulsesImpl(tlm_solver *h, O *out, size_t
     case TLM_STORE_F64: return pulsesToHost<double, O>(h, out, cap);
     case TLM_STORE_BF16: return pulsesToHost<__nv_bfloat16, O>(h, out, cap);
     case TLM_STORE_F16: return pulsesToHost<__half, O>(h, out, cap);
+    case TLM_STORE_BFP16: return pulsesToHost<tlmk::Bfp4, O>(h, out, cap);
     default: return pulsesToHost<float, O>(h, out, cap);
     }
 }
@@ -822,7 +829,7 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
                                        " cells, the grid has " + std::to_string(n));
     if (n_table < 0 || n_table > 254 || (n_table > 0 && !table))
         return h->fail(TLM_EINVAL, "material table must have 0..254 entries");
-    if (cfg->storage < TLM_STORE_F32 || cfg->storage > TLM_STORE_F64)
+    if (cfg->storage < TLM_STORE_F32 || cfg->storage > TLM_STORE_BFP16)
         return h->fail(TLM_EINVAL, "unknown pulse storage mode");
     if (cfg->waveform < 0 || cfg->waveform > TLM_WAVE_TABLE)
         return h->fail(TLM_EINVAL, "unknown waveform");
@@ -1303,6 +1310,7 @@ tlm_status tlm_set_pulses(tlm_handle h, const float *in, size_t n)
     case TLM_STORE_F64: return setPulsesT<double>(h, in);
     case TLM_STORE_BF16: return setPulsesT<__nv_bfloat16>(h, in);
     case TLM_STORE_F16: return setPulsesT<__half>(h, in);
+    case TLM_STORE_BFP16: return setPulsesT<tlmk::Bfp4>(h, in);
     default: return setPulsesT<float>(h, in);
     }
 }

@@ -18,6 +18,8 @@
 
 #include "tlm_device.cuh"
 
+#include <type_traits>
+
 namespace tlmk {
 
 template <class S> struct StepArgs
@@ -52,14 +54,69 @@ template <class S> struct StepArgs
 #define TLM_GUARD(idx, limit, code) true
 #endif
 
+// Plane access by node index, for every storage type. Element storage
+// (float, double, half, bfloat16) is read and written as aligned vectors of
+// V nodes; block floating point (Bfp4) as one word per aligned 4-node group.
 template <class S, int V>
-__device__ __forceinline__ void loadPack(const S *__restrict__ base, long long idx,
-                                         typename Traits<S>::R (&dst)[V],
-                                         typename Traits<S>::R scale)
+__device__ __forceinline__ void loadVec(const S *__restrict__ base, long long node,
+                                        typename Traits<S>::R (&dst)[V], typename Traits<S>::R scale)
 {
-    const Pack<S, V> p = *reinterpret_cast<const Pack<S, V> *>(base + idx);
+    if constexpr (std::is_same<S, Bfp4>::value)
+    {
+        static_assert(V == 4, "block floating point groups hold 4 nodes");
+        float v[4];
+        bfpDecode(base[node >> 2].w, v);
 #pragma unroll
-    for (int c = 0; c < V; ++c) dst[c] = decode(p.v[c], scale);
+        for (int c = 0; c < 4; ++c) dst[c] = v[c];
+    }
+    else
+    {
+        const Pack<S, V> p = *reinterpret_cast<const Pack<S, V> *>(base + node);
+#pragma unroll
+        for (int c = 0; c < V; ++c) dst[c] = decode(p.v[c], scale);
+    }
+}
+
+template <class S>
+__device__ __forceinline__ typename Traits<S>::R loadOne(const S *__restrict__ base, long long node,
+                                                         typename Traits<S>::R scale)
+{
+    if constexpr (std::is_same<S, Bfp4>::value)
+        return bfpDecodeOne(base[node >> 2].w, (int)(node & 3));
+    else
+        return decode(base[node], scale);
+}
+
+// Store V nodes of plane slot `salt`; with stochastic rounding the random
+// bits are a function of (node, slot, step seed).
+template <class S, int V>
+__device__ __forceinline__ void storeVec(S *__restrict__ base, long long node,
+                                         const typename Traits<S>::R (&src)[V],
+                                         typename Traits<S>::R inv, bool stochastic, unsigned seed,
+                                         int salt)
+{
+    if constexpr (std::is_same<S, Bfp4>::value)
+    {
+        static_assert(V == 4, "block floating point groups hold 4 nodes");
+        float v[4] = { src[0], src[1], src[2], src[3] };
+        base[node >> 2].w = bfpEncode(v, stochastic, mix32((unsigned)(node * 12 + salt) ^ seed));
+    }
+    else
+    {
+        Pack<S, V> p;
+        if (Traits<S>::kScaled && stochastic)
+        {
+#pragma unroll
+            for (int c = 0; c < V; ++c)
+                p.v[c] = encodeStochastic<S>(src[c], inv, mix32((unsigned)((node + c) * 12 + salt) ^ seed));
+        }
+        else
+        {
+#pragma unroll
+            for (int c = 0; c < V; ++c) p.v[c] = encode<S>(src[c], inv);
+        }
+        *reinterpret_cast<Pack<S, V> *>(base + node) = p;
+    }
 }
 
 template <int V> __device__ __forceinline__ void loadMat(const uint8_t *__restrict__ m, long long idx,
@@ -122,7 +179,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
         for (int s = 0; s < 12; ++s)
         {
             if (live && TLM_GUARD(s * P + node0, 12 * P - V + 1, 2))
-                loadPack<S, V>(a.in, s * P + node0, inc[s], a.scale);
+                loadVec<S, V>(a.in, s * P + node0, inc[s], a.scale);
             else
             {
 #pragma unroll
@@ -175,7 +232,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
         for (int s = 0; s < 4; ++s)
         {
             if (live && TLM_GUARD(s * P + node0, 12 * P - V + 1, 5))
-                loadPack<S, V>(a.in, s * P + node0, ox[s], a.scale);
+                loadVec<S, V>(a.in, s * P + node0, ox[s], a.scale);
             else
             {
 #pragma unroll
@@ -194,14 +251,14 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
 #pragma unroll
             for (int t = 0; t < 2; ++t)
                 if (TLM_GUARD((2 + t) * P + node0 - 1, 12 * P, 6))
-                    prevX[t] = decode(a.in[(2 + t) * P + node0 - 1], a.scale);
+                    prevX[t] = loadOne<S>(a.in, (2 + t) * P + node0 - 1, a.scale);
         }
         if (lane == 31 && needNext)
         {
 #pragma unroll
             for (int t = 0; t < 2; ++t)
                 if (TLM_GUARD(t * P + node0 + V, 12 * P, 6))
-                    nextX[t] = decode(a.in[t * P + node0 + V], a.scale);
+                    nextX[t] = loadOne<S>(a.in, t * P + node0 + V, a.scale);
         }
 #pragma unroll
         for (int c = 0; c < V; ++c)
@@ -245,7 +302,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                 {
                     const long long idx = atLo ? sLo * P + node0 : sHi * P + node0 - st;
                     if (live && TLM_GUARD(idx, 12 * P - V + 1, 7))
-                        loadPack<S, V>(a.in, idx, vLo, a.scale);
+                        loadVec<S, V>(a.in, idx, vLo, a.scale);
                     else
                     {
 #pragma unroll
@@ -260,7 +317,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                     {
                         R own[V];
                         if (TLM_GUARD(sLo * P + node0, 12 * P - V + 1, 8))
-                            loadPack<S, V>(a.in, sLo * P + node0, own, a.scale);
+                            loadVec<S, V>(a.in, sLo * P + node0, own, a.scale);
 #pragma unroll
                         for (int c = 0; c < V; ++c)
                             if ((pm >> c) & 1u) vLo[c] = -own[c];
@@ -270,7 +327,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                 {
                     const long long idx = atHi ? sHi * P + node0 : sLo * P + node0 + st;
                     if (live && TLM_GUARD(idx, 12 * P - V + 1, 9))
-                        loadPack<S, V>(a.in, idx, vHi, a.scale);
+                        loadVec<S, V>(a.in, idx, vHi, a.scale);
                     else
                     {
 #pragma unroll
@@ -285,7 +342,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                     {
                         R own[V];
                         if (TLM_GUARD(sHi * P + node0, 12 * P - V + 1, 10))
-                            loadPack<S, V>(a.in, sHi * P + node0, own, a.scale);
+                            loadVec<S, V>(a.in, sHi * P + node0, own, a.scale);
 #pragma unroll
                         for (int c = 0; c < V; ++c)
                             if ((pp >> c) & 1u) vHi[c] = -own[c];
@@ -450,21 +507,8 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
         {
             if (TLM_GUARD(s * P + node0, 12 * P - V + 1, 12))
             {
-                Pack<S, V> p;
-                if (Traits<S>::kScaled && a.stochastic)
-                {
-#pragma unroll
-                    for (int c = 0; c < V; ++c)
-                        p.v[c] = encodeStochastic<S>(
-                            outv[s][c], a.inv_scale,
-                            mix32((unsigned)((node0 + c) * 12 + s) ^ a.round_seed));
-                }
-                else
-                {
-#pragma unroll
-                    for (int c = 0; c < V; ++c) p.v[c] = encode<S>(outv[s][c], a.inv_scale);
-                }
-                *reinterpret_cast<Pack<S, V> *>(a.out + s * P + node0) = p;
+                storeVec<S, V>(a.out, s * P + node0, outv[s], a.inv_scale, a.stochastic != 0,
+                               a.round_seed, s);
             }
         }
         if (anyDiel && dielMask)

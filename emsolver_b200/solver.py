@@ -34,6 +34,7 @@ class Storage(IntEnum):
     BF16 = _lib.STORE_BF16
     F16 = _lib.STORE_F16
     F64 = _lib.STORE_F64
+    BFP16 = _lib.STORE_BFP16
 
 
 MAT_AIR, MAT_PEC, MAT_DIEL0 = 0, 1, 2

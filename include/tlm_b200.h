@@ -67,13 +67,17 @@ typedef enum tlm_waveform {
     TLM_WAVE_TABLE = 3
 } tlm_waveform;
 
-/* Pulse storage. Scatter arithmetic is FP32 for F32/BF16/F16 and FP64 for
- * F64 (the on-device FP64 oracle mode). BF16/F16 store pulse/scale. */
+/* Pulse storage. Scatter arithmetic is FP32 for F32/BF16/F16/BFP16 and FP64
+ * for F64 (the on-device FP64 oracle mode). BF16/F16 store pulse/scale.
+ * BFP16 is block floating point at 16 bits per pulse: each aligned group of
+ * 4 x-neighbours of one link plane shares an 8-bit exponent and keeps a
+ * 14-bit signed mantissa per pulse (13 bits below the group maximum). */
 typedef enum tlm_storage {
     TLM_STORE_F32 = 0,
     TLM_STORE_BF16 = 1,
     TLM_STORE_F16 = 2,
-    TLM_STORE_F64 = 3
+    TLM_STORE_F64 = 3,
+    TLM_STORE_BFP16 = 4
 } tlm_storage;
 
 /* VoxelGridSpec (Geometry.h:85-113). */

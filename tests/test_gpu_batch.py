@@ -89,8 +89,8 @@ def test_members_join_and_leave_mid_run(built):
 
 
 def test_mixed_storage_batch(built):
-    ws = instances(4, seed=3)
-    modes = [Storage.F32, Storage.BF16, Storage.F16, Storage.F64]
+    ws = instances(5, seed=3)
+    modes = [Storage.F32, Storage.BF16, Storage.F16, Storage.F64, Storage.BFP16]
     refs = [alone(w, m) for w, m in zip(ws, modes)]
     solvers = [build_solver(w, storage=m) for w, m in zip(ws, modes)]
     with Batch() as b:

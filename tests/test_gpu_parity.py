@@ -158,7 +158,8 @@ def test_fp64_storage_matches_fp64_oracle(built, w):
 
 
 @pytest.mark.parametrize("storage,rounding,tol", [(Storage.F16, 0, 4e-2), (Storage.BF16, 0, 0.3),
-                                                  (Storage.F16, 1, 4e-2), (Storage.BF16, 1, 0.3)])
+                                                  (Storage.F16, 1, 4e-2), (Storage.BF16, 1, 0.3),
+                                                  (Storage.BFP16, 0, 1e-2), (Storage.BFP16, 1, 1e-2)])
 def test_half_storage_error_vs_fp64_oracle(built, storage, rounding, tol):
     """Regression guard for pulses stored in FP16 / BF16 (FP32 arithmetic):
     probe series of a small resonant PEC/dielectric box (16^3, 120 steps)
@@ -186,7 +187,7 @@ def test_dipole_s11_precision_modes(built):
     from emsolver_b200.solver import s11_from_dft
     w = workloads.dipole(48, 48, 64, 31, slab=(4, 12, 3.0), steps=1500, nfreq=32)
     out = {}
-    for st in (Storage.F64, Storage.F32, Storage.F16, Storage.BF16):
+    for st in (Storage.F64, Storage.F32, Storage.F16, Storage.BF16, Storage.BFP16):
         s = build_solver(w, storage=st)
         s.step(w.steps)
         v, i = s.portDft(0)
@@ -196,9 +197,10 @@ def test_dipole_s11_precision_modes(built):
     assert rel[Storage.F32] <= 1e-5, rel
     assert rel[Storage.F16] <= 5e-2, rel
     assert rel[Storage.BF16] <= 2e-1, rel
+    assert rel[Storage.BFP16] <= 1e-2, rel
 
 
-@pytest.mark.parametrize("storage", [Storage.F32, Storage.BF16, Storage.F16, Storage.F64])
+@pytest.mark.parametrize("storage", [Storage.F32, Storage.BF16, Storage.F16, Storage.F64, Storage.BFP16])
 def test_every_kernel_shape_gives_identical_results(built, storage):
     """The tile shapes (nodes per thread, blocks per SM) only change how the
     work is laid out: every shape must produce bit-identical state."""
@@ -217,3 +219,30 @@ def test_every_kernel_shape_gives_identical_results(built, storage):
                 assert_energy_close(r[k], ref_r[k])
             else:
                 assert np.array_equal(r[k], ref_r[k]), (v, k)
+
+
+def test_bfp16_storage_quantisation_bound(built):
+    """Block floating point storage: a pulse written by tlm_set_pulses and
+    read back differs from the written value by at most 2^-13 of the largest
+    magnitude in its group (4 x-neighbours of one link plane); zero groups and
+    PEC nodes read back as 0."""
+    w = CASES[3]
+    s = build_solver(w, storage=Storage.BFP16)
+    nx, ny, nz = w.nx, w.ny, w.nz
+    rng = np.random.default_rng(5)
+    # magnitudes spread over many binades, with some all-zero groups
+    x = (rng.standard_normal((nz, ny, nx, 12)) * 10.0 ** rng.uniform(-6, 3, (nz, ny, nx, 1)))
+    x = x.astype(np.float32)
+    x[:, :, :4, 3] = 0.0
+    s.setPulses(x.reshape(-1))
+    got = s.pulses().reshape(nz, ny, nx, 12).astype(np.float64)
+    live = (np.asarray(w.mat).reshape(nz, ny, nx) != 1)[..., None]
+    want = np.where(live, x.astype(np.float64), 0.0)
+    px = (nx + 7) // 8 * 8
+    pad = np.zeros((nz, ny, px, 12))
+    pad[:, :, :nx] = want
+    gmax = np.abs(pad).reshape(nz, ny, px // 4, 4, 12).max(axis=3)
+    bound = np.repeat(gmax, 4, axis=2)[:, :, :nx] * 2.0 ** -13 * (1 + 1e-6)
+    assert np.all(np.abs(got - want) <= bound)
+    assert np.all(got[:, :, :4, 3] == 0.0)
+    assert np.all(got[~np.broadcast_to(live, got.shape)] == 0.0)
