@@ -41,7 +41,7 @@ class ConfigC(C.Structure):
                 ("settle_steps", C.c_int), ("boundary_rho", C.c_float), ("huy_offset", C.c_int),
                 ("use_gpu", C.c_int), ("record_every", C.c_int), ("storage", C.c_int),
                 ("pulse_scale", C.c_float), ("steps_per_launch", C.c_int),
-                ("kernel_variant", C.c_int), ("rounding", C.c_int)]
+                ("kernel_variant", C.c_int), ("rounding", C.c_int), ("general_tiles", C.c_int)]
 
 
 class BatchTuningC(C.Structure):

@@ -135,11 +135,15 @@ template <class S> MemberDesc<S> makeDesc(tlm_solver *h)
     d.nz = h->nz;
     d.px = h->px;
     d.nq = h->nq;
+    d.div_nq = tlmk::makeFastDiv((unsigned)h->nq);
+    d.div_ny = tlmk::makeFastDiv((unsigned)h->ny);
     d.rho = (R)h->cfg.boundary_rho;
     d.scale = (R)h->scale;
     d.inv_scale = (R)(1.0f / h->scale);
     d.tile_begin = h->dTile;
     d.spec = h->dSpec;
+    d.tile_flags = h->dTileFlags;
+    d.neg_zero = -0.0f;
     d.sv = static_cast<const R *>(h->dSv);
     d.samples = static_cast<R *>(h->dSamples);
     d.nsamp = h->nsamp;

@@ -29,9 +29,12 @@ template <class S> struct MemberDesc
     const R *ghat;
     long long P, nquads;
     int nx, ny, nz, px, nq;
+    FastDiv div_nq, div_ny;
     R rho, scale, inv_scale;
     const int *tile_begin;
     const SpecEntry *spec;
+    const uint8_t *tile_flags;
+    float neg_zero;          // -0.0f (see mul2)
     const R *sv;             // source value per absolute step, [total]
     R *samples;              // [window][nsamp][6]
     int nsamp;
@@ -87,11 +90,15 @@ __global__ void __launch_bounds__(kBlock, MINB)
                     sa.nz = d.nz;
                     sa.px = d.px;
                     sa.nq = d.nq;
+                    sa.div_nq = d.div_nq;
+                    sa.div_ny = d.div_ny;
                     sa.rho = d.rho;
                     sa.scale = d.scale;
                     sa.inv_scale = d.inv_scale;
                     sa.tile_begin = d.tile_begin;
                     sa.spec = d.spec;
+                    sa.tile_flags = d.tile_flags;
+                    sa.neg_zero = d.neg_zero;
                     sa.sv = d.sv[n];
                     sa.samples = d.samples + (long long)i * d.nsamp * 6;
                     sa.epart = (n % 16 == 0) ? d.epart + ((n - eFirst) / 16) * d.nblocks : nullptr;

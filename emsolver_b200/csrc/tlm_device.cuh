@@ -68,6 +68,29 @@ template <> struct Traits<__nv_bfloat16>
     static constexpr bool kScaled = true;
 };
 
+// Division of n < 2^31 by a divisor d >= 1 that is fixed for a launch,
+// through a multiply-high (Granlund and Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994): with shift = ceil(log2 d) and
+// mul = floor(2^32 (2^shift - d) / d) + 1, n / d = (umulhi(n, mul) + n) >> shift
+// (the sum stays below 2^32 because n < 2^31).
+struct FastDiv
+{
+    unsigned mul;
+    int shift;
+};
+
+inline FastDiv makeFastDiv(unsigned d)
+{
+    int l = 0;
+    while (l < 32 && (1ull << l) < d) ++l;
+    FastDiv f;
+    f.mul = (unsigned)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    f.shift = l;
+    return f;
+}
+
+__device__ __forceinline__ unsigned fastDiv(unsigned n, FastDiv f) { return (__umulhi(n, f.mul) + n) >> f.shift; }
+
 // 32-bit integer mixer (the MurmurHash3 finaliser): counter-based random
 // bits for stochastic rounding, a pure function of (node, slot, step).
 __host__ __device__ __forceinline__ unsigned mix32(unsigned h)
@@ -81,14 +104,19 @@ __host__ __device__ __forceinline__ unsigned mix32(unsigned h)
 }
 
 // Block floating point, 16 bits per pulse: one 64-bit word holds an aligned
-// group of 4 consecutive x-nodes of one plane -- four 14-bit two's-complement
-// mantissas (bits 0-13, 14-27, 28-41, 42-55) and the group's biased binary
-// exponent (bits 56-63). Value = mantissa * 2^(E - 13), E = exponent - 127,
-// chosen so the group's largest magnitude uses the full 13 bits. Exponent 0
-// encodes an all-zero group.
-struct Bfp4
+// group of 4 consecutive x-nodes of one plane. Each pulse keeps a 14-bit
+// offset-binary mantissa u (value m = u - 8192, |m| <= 8191); the group shares
+// an 8-bit exponent e: pulse = m * 2^(e - 140). Layout, as two 32-bit halves:
+//   lo = u0 | u1 << 14 | (e & 15) << 28,   hi = u2 | u3 << 14 | (e >> 4) << 28.
+// e = 0 encodes an all-zero group (a zero-filled buffer decodes to zeros).
+// The encoder picks e so that the group's largest magnitude uses 13 bits.
+// Conversions between the integer mantissas and floats go through the
+// float-bits identity bits(2^23 + 2^22 + k) = 0x4B400000 + k (0 <= k < 2^22),
+// so neither direction needs an int<->float conversion instruction, and both
+// are exact: m * 2^(e-140) is a float, and x * 2^(153-e) is an exact scaling.
+struct __align__(8) Bfp4
 {
-    unsigned long long w;
+    unsigned lo, hi;
 };
 template <> struct Traits<Bfp4>
 {
@@ -104,72 +132,75 @@ template <class S, int V> struct alignas(sizeof(S) * V) Pack
     S v[V];
 };
 
-__device__ __forceinline__ float bfpUnit(int biasedExp)
+constexpr unsigned kBfpMagic = 0x4B400000u;  // bits of 2^23 + 2^22
+constexpr float kBfpBias = 12591104.0f;      // 2^23 + 2^22 + 8192: float of (magic | u) minus m
+
+__device__ __forceinline__ int bfpExp(const Bfp4 &w) { return (int)((w.lo >> 28) | ((w.hi >> 24) & 0xf0u)); }
+
+// 2^(e - 140), or 0 for e = 0 (the encoder never writes 1 <= e <= 15)
+__device__ __forceinline__ float bfpUnit(int e) { return __int_as_float(max((e - 13) << 23, 0)); }
+
+__device__ __forceinline__ float bfpValue(unsigned field, float unit, float bias)
 {
-    // 2^(E - 13) for E = biasedExp - 127 (exponents below 2^-112 are flushed
-    // to zero by the encoder, so the result is a normal float)
-    return __int_as_float((biasedExp - 13) << 23);
+    // (2^23 + 2^22 + u) * unit - (2^23 + 2^22 + 8192) * unit, one rounding of
+    // an exactly representable result
+    return __fmaf_rn(__uint_as_float((field & 0x3fffu) | kBfpMagic), unit, bias);
 }
 
-__device__ __forceinline__ void bfpDecode(unsigned long long w, float (&v)[4])
+__device__ __forceinline__ void bfpDecode(const Bfp4 &w, float (&v)[4])
 {
-    const int e = (int)(w >> 56);
-    const float unit = e ? bfpUnit(e) : 0.0f;
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
+    const float unit = bfpUnit(bfpExp(w));
+    const float bias = __fmul_rn(-kBfpBias, unit);
+    v[0] = bfpValue(w.lo, unit, bias);
+    v[1] = bfpValue(w.lo >> 14, unit, bias);
+    v[2] = bfpValue(w.hi, unit, bias);
+    v[3] = bfpValue(w.hi >> 14, unit, bias);
+}
+
+__device__ __forceinline__ float bfpDecodeOne(const Bfp4 &w, int c)
+{
+    const float unit = bfpUnit(bfpExp(w));
+    const unsigned half = (c & 2) ? w.hi : w.lo;
+    return bfpValue((c & 1) ? half >> 14 : half, unit, __fmul_rn(-kBfpBias, unit));
+}
+
+// Encode 4 values (round to nearest even, or stochastically with the random
+// bits `r`). Groups whose largest magnitude is below 2^-112 (or not finite,
+// or above 2^125) are stored as zero.
+__device__ __forceinline__ Bfp4 bfpEncode(const float (&v)[4], bool stochastic, unsigned r)
+{
+    const float M = fmaxf(fmaxf(fabsf(v[0]), fabsf(v[1])), fmaxf(fabsf(v[2]), fabsf(v[3])));
+    // exponent of M * (1 + 2^-12): M * 2^(153 - e) <= 8190 + 2^-11, so neither
+    // rounding mode can carry a mantissa past 8191
+    const float Madj = __fmaf_rn(M, 0x1p-12f, M);
+    const int e = (__float_as_int(Madj) >> 23) + 1;           // Madj < 2^(e - 127)
+    const float q = __int_as_float((267 - e) << 23);           // 2^(13 - (e - 127))
+    unsigned u[4];
+    if (stochastic)
     {
-        const long long m = ((long long)(w << (50 - 14 * c))) >> 50;  // sign-extend 14 bits
-        v[c] = (float)(int)m * unit;
-    }
-}
-
-__device__ __forceinline__ float bfpDecodeOne(unsigned long long w, int c)
-{
-    const int e = (int)(w >> 56);
-    const long long m = ((long long)(w << (50 - 14 * c))) >> 50;
-    return e ? (float)(int)m * bfpUnit(e) : 0.0f;
-}
-
-// Encode 4 values; `r` (when stochastic) supplies random bits for unbiased
-// rounding of each mantissa.
-__device__ __forceinline__ unsigned long long bfpEncode(const float (&v)[4], bool stochastic,
-                                                        unsigned r)
-{
-    float M = 0.0f;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) M = fmaxf(M, fabsf(v[c]));
-    if (!(M > 0x1p-112f) || !(M < 0x1p126f)) return 0ull;  // zero, tiny, or not finite
-    int e = (int)((__float_as_uint(M) >> 23) & 0xff) + 1;       // biased E with M < 2^E
-    unsigned long long w = 0;
-#pragma unroll 1
-    for (int attempt = 0; attempt < 2; ++attempt)
-    {
-        const float q = __int_as_float((127 + 127 + 13 - e) << 23);  // 2^(13 - E)
-        int m[4];
-        int big = 0;
+        const unsigned h0 = mix32(r), h1 = mix32(r ^ 0x5bd1e995u);
+        const unsigned bits[4] = { h0 << 7, h0 >> 9, h1 << 7, h1 >> 9 };
 #pragma unroll
         for (int c = 0; c < 4; ++c)
         {
-            const float x = v[c] * q;  // exact power-of-two scaling
-            if (stochastic)
-            {
-                const float u = (float)(mix32(r + (unsigned)c) >> 8) * (1.0f / 16777216.0f);  // [0, 1)
-                m[c] = __float2int_rd(x + u);
-            }
-            else
-                m[c] = __float2int_rn(x);
-            big = max(big, abs(m[c]));
+            // y = x*q + d, d uniform in [1, 2) (16 random bits); floor(y - 1)
+            // through a round-down add into the magic range
+            const float d = __uint_as_float(0x3f800000u | (bits[c] & 0x7fff80u));
+            const float y = __fmaf_rn(v[c], q, d);
+            u[c] = __float_as_uint(__fadd_rd(y, kBfpBias - 1.0f));
         }
-        if (big > 8191 && attempt == 0)
-        {
-            ++e;  // rounding reached 2^13: use the next binade
-            continue;
-        }
-        w = (unsigned long long)e << 56;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) w |= ((unsigned long long)(m[c] & 0x3fff)) << (14 * c);
-        break;
     }
+    else
+    {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) u[c] = __float_as_uint(__fmaf_rn(v[c], q, kBfpBias));
+    }
+    Bfp4 w;
+    w.lo = (u[0] & 0x3fffu) | ((u[1] & 0x3fffu) << 14) | ((unsigned)e << 28);
+    w.hi = (u[2] & 0x3fffu) | ((u[3] & 0x3fffu) << 14) | (((unsigned)e >> 4) << 28);
+    const bool keep = (M > 0x1p-112f) && (Madj < 0x1p125f);
+    w.lo = keep ? w.lo : 0u;
+    w.hi = keep ? w.hi : 0u;
     return w;
 }
 
@@ -338,6 +369,102 @@ __device__ __forceinline__ void scatterSelect(const R (&in)[12], R (&vs)[3], R y
     reflectLinks(in, Vn, ZI, out);
 #pragma unroll
     for (int j = 0; j < 3; ++j) vs[j] = diel ? Vn[j] - vs[j] : vs[j];
+}
+
+// ---- two nodes at once: packed FP32x2 arithmetic ----
+// Each lane is rounded exactly like the scalar operation. The code generator
+// fuses a packed multiply into a following packed add even when fused
+// multiply-add is disabled, which would round a*b + c once instead of twice.
+// Products are therefore formed as fma(a, b, z) with z = -0.0 supplied at run
+// time (a kernel argument the compiler cannot see through): fma(a, b, -0) is
+// the correctly rounded product (signed zeros included) and an FMA cannot be
+// fused again, so the packed scatter below is bitwise the scalar one.
+#define TLM_F32X2_OP(name, op)                                                                   \
+    __device__ __forceinline__ float2 name(float2 a, float2 b)                                   \
+    {                                                                                            \
+        float2 r;                                                                                \
+        asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t" \
+            op " pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"                                       \
+            : "=f"(r.x), "=f"(r.y)                                                               \
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                           \
+        return r;                                                                                \
+    }
+TLM_F32X2_OP(add2, "add.rn.f32x2")
+TLM_F32X2_OP(sub2, "sub.rn.f32x2")
+#undef TLM_F32X2_OP
+
+// a * b, correctly rounded per lane; z must be (-0.0, -0.0) from run time
+__device__ __forceinline__ float2 mul2(float2 a, float2 b, float2 z)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pz, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "mov.b64 pz, {%6, %7};\n\tfma.rn.f32x2 pd, pa, pb, pz;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(z.x), "f"(z.y));
+    return r;
+}
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ float2 nodeVoltage2(const float2 (&v)[12], int j, float2 z)
+{
+    const int a = (j == 0) ? 1 : 0;
+    const int b = (j == 2) ? 1 : 2;
+    return mul2(splat2(0.5f),
+                add2(add2(add2(v[slotOf(a, 0, j)], v[slotOf(a, 1, j)]), v[slotOf(b, 0, j)]), v[slotOf(b, 1, j)]),
+                z);
+}
+__device__ __forceinline__ float2 circulation2(const float2 (&v)[12], int k, float2 z)
+{
+    const int p = (k + 1) % 3, q = (k + 2) % 3;
+    return mul2(splat2(0.5f),
+                add2(sub2(sub2(v[slotOf(p, 0, q)], v[slotOf(p, 1, q)]), v[slotOf(q, 0, p)]), v[slotOf(q, 1, p)]),
+                z);
+}
+__device__ __forceinline__ void reflectLinks2(const float2 (&in)[12], const float2 (&Vn)[3],
+                                              const float2 (&ZI)[3], float2 (&out)[12])
+{
+#pragma unroll
+    for (int s = 0; s < 12; ++s)
+    {
+        const int i = s >> 2, side = (s >> 1) & 1;
+        const int j = fieldOfSlot(s);
+        const int k = 3 - i - j;
+        const bool plus = ((j == (i + 1) % 3) == (side == 1));
+        const float2 base = plus ? add2(Vn[j], ZI[k]) : sub2(Vn[j], ZI[k]);
+        out[s] = sub2(base, in[s ^ 2]);
+    }
+}
+// scatterAir for a pair of air nodes
+__device__ __forceinline__ void scatterAir2(const float2 (&in)[12], float2 (&out)[12], float2 z)
+{
+    float2 Vn[3], ZI[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) Vn[j] = nodeVoltage2(in, j, z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ZI[k] = circulation2(in, k, z);
+    reflectLinks2(in, Vn, ZI, out);
+}
+// scatterStub for a pair of stub-loaded nodes (the divides stay scalar)
+__device__ __forceinline__ void scatterStub2(const float2 (&in)[12], float2 (&vs)[3], float2 yh, float2 gh,
+                                             float2 (&out)[12], float2 z)
+{
+    float2 Vn[3], ZI[3];
+    const float2 den = add2(add2(splat2(4.0f), yh), gh);
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+    {
+        const int a = (j == 0) ? 1 : 0;
+        const int b = (j == 2) ? 1 : 2;
+        const float2 sum4 =
+            add2(add2(add2(in[slotOf(a, 0, j)], in[slotOf(a, 1, j)]), in[slotOf(b, 0, j)]), in[slotOf(b, 1, j)]);
+        const float2 num = mul2(splat2(2.0f), add2(sum4, mul2(yh, vs[j], z)), z);
+        Vn[j] = make_float2(__fdiv_rn(num.x, den.x), __fdiv_rn(num.y, den.y));
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ZI[k] = circulation2(in, k, z);
+    reflectLinks2(in, Vn, ZI, out);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) vs[j] = sub2(Vn[j], vs[j]);
 }
 
 // A source or monitor attached to one node. Entries are sorted by node

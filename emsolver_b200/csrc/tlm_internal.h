@@ -146,6 +146,7 @@ struct tlm_solver
     void *dYhat = nullptr, *dGhat = nullptr;
     tlmk::SpecEntry *dSpec = nullptr;
     int *dTile = nullptr;
+    uint8_t *dTileFlags = nullptr;  // per step-kernel tile: tlmk::kTileGeneral / kTileDiel
     void *dSamples = nullptr;
     double *dEpart = nullptr;
     int *dPortOff = nullptr, *dPortSlots = nullptr, *dPortPol = nullptr, *dPortNb = nullptr;

@@ -146,11 +146,15 @@ tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_planes, fl
     a.nz = nz;
     a.px = (int)px;
     a.nq = (int)nq;
+    a.div_nq = tlmk::makeFastDiv((unsigned)nq);
+    a.div_ny = tlmk::makeFastDiv((unsigned)ny);
     a.rho = rho;
     a.scale = 1.0f;
     a.inv_scale = 1.0f;
     a.tile_begin = nullptr;
     a.spec = nullptr;
+    a.tile_flags = nullptr;  // every tile takes the general body
+    a.neg_zero = -0.0f;
     a.sv = 0.0f;
     a.samples = nullptr;
     a.epart = energy_out ? scratch : nullptr;

@@ -59,6 +59,7 @@ void freeMonitors(tlm_solver *h)
 {
     devFree(h, h->dSpec);
     devFree(h, h->dTile);
+    devFree(h, h->dTileFlags);
     devFree(h, h->dSamples);
     devFree(h, h->dEpart);
     devFree(h, h->dPortOff);
@@ -110,6 +111,52 @@ long long paddedNode(const tlm_solver *h, uint64_t cell)
     return r * h->px + i;
 }
 
+// Per-tile flags of the step kernel (tlmk::kTileGeneral, tlmk::kTileDiel):
+// a tile is general when it is the partial last tile, holds a source or
+// monitor entry (tileBegin ranges), covers a row on a y or z face of the
+// grid, or holds a node that is PEC or next to a PEC node.
+std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tileBegin)
+{
+    const long long T = (long long)kBlock * h->V;
+    const int nb = h->nblocks;
+    std::vector<uint8_t> f((size_t)nb, h->cfg.general_tiles ? tlmk::kTileGeneral : 0);
+    auto mark = [&](long long node, uint8_t bit) {
+        if (node >= 0 && node < h->P) f[(size_t)(node / T)] |= bit;
+    };
+    if (h->nquads % kBlock) f[(size_t)nb - 1] |= tlmk::kTileGeneral;
+    for (int b = 0; b < nb; ++b)
+        if (tileBegin[b + 1] > tileBegin[b]) f[(size_t)b] |= tlmk::kTileGeneral;
+    for (int k = 0; k < h->nz; ++k)
+        for (int j = 0; j < h->ny; ++j)
+        {
+            if (!(j == 0 || j == h->ny - 1 || k == 0 || k == h->nz - 1)) continue;
+            const long long r0 = ((long long)k * h->ny + j) * h->px;
+            for (long long t = r0 / T; t <= (r0 + h->px - 1) / T; ++t) f[(size_t)t] |= tlmk::kTileGeneral;
+        }
+    const long long sy = h->px, sz = (long long)h->px * h->ny;
+    for (long long c = 0; c < h->ncell; ++c)
+    {
+        const uint8_t m = h->mat[(size_t)c];
+        if (m == tlmk::kAir) continue;
+        const long long node = paddedNode(h, (uint64_t)c);
+        if (m >= tlmk::kDiel0)
+        {
+            mark(node, tlmk::kTileDiel);
+            continue;
+        }
+        // PEC: the node and every node that has it as a neighbour
+        const long long i = c % h->nx;
+        mark(node, tlmk::kTileGeneral);
+        if (i > 0) mark(node - 1, tlmk::kTileGeneral);
+        if (i < h->nx - 1) mark(node + 1, tlmk::kTileGeneral);
+        mark(node - sy, tlmk::kTileGeneral);
+        mark(node + sy, tlmk::kTileGeneral);
+        mark(node - sz, tlmk::kTileGeneral);
+        mark(node + sz, tlmk::kTileGeneral);
+    }
+    return f;
+}
+
 // Build the device tables of sources and monitors once, before the first
 // step: the node-sorted entry list, per-block ranges, sample slots, port
 // and probe descriptors, records and DFT accumulators.
@@ -155,6 +202,12 @@ tlm_status prepare(tlm_solver *h)
             while (e < ents.size() && ents[e].node < start) ++e;
             tile[b] = (int)e;
         }
+    }
+    {
+        const std::vector<uint8_t> flags = tileFlags(h, tile);
+        TLM_TRY(devAlloc(h, &h->dTileFlags, flags.size()));
+        TLM_CU(h, cudaMemcpyAsync(h->dTileFlags, flags.data(), flags.size(), cudaMemcpyHostToDevice,
+                                  h->stream));
     }
     if (!ents.empty())
     {
@@ -322,11 +375,15 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
     a.nz = h->nz;
     a.px = h->px;
     a.nq = h->nq;
+    a.div_nq = tlmk::makeFastDiv((unsigned)h->nq);
+    a.div_ny = tlmk::makeFastDiv((unsigned)h->ny);
     a.rho = (R)h->cfg.boundary_rho;
     a.scale = (R)h->scale;
     a.inv_scale = (R)(1.0f / h->scale);
     a.tile_begin = h->dTile;
     a.spec = h->dSpec;
+    a.tile_flags = h->dTileFlags;
+    a.neg_zero = -0.0f;
     a.sv = (R)sourceValue(h, n);
     a.samples = static_cast<R *>(h->dSamples) + (size_t)i * h->nsamp * 6;
     a.epart = (n % 16 == 0) ? h->dEpart + (size_t)((n - eFirst) / 16) * h->nblocks : nullptr;
@@ -558,10 +615,12 @@ tlm_status reshape(tlm_solver *h, int variant)
     if (variant < 0 || variant >= shapeCount(h->storage)) return h->fail(TLM_EINVAL, "no such variant");
     if (variant == h->variant && h->prepared) return TLM_OK;
     const long long cap = h->recCap;
+    const long long nquads = (long long)(h->px / shapeOf(h->storage, variant).V) * h->ny * h->nz;
+    if (nquads >= (1LL << 31)) return h->fail(TLM_EINVAL, "grid too large for this tile shape");
     h->variant = variant;
     h->V = shapeOf(h->storage, variant).V;
     h->nq = h->px / h->V;
-    h->nquads = (long long)h->nq * h->ny * h->nz;
+    h->nquads = nquads;
     h->nblocks = (int)((h->nquads + kBlock - 1) / kBlock);
     h->prepared = false;
     TLM_TRY(prepare(h));
@@ -705,6 +764,7 @@ void tlm_config_default(tlm_config *c)
     c->steps_per_launch = 0;
     c->kernel_variant = 0;
     c->rounding = 0;
+    c->general_tiles = 0;
 }
 
 int tlm_kernel_variants(int storage) { return shapeCount(storage); }
@@ -837,6 +897,8 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     if (cfg->kernel_variant < 0 || cfg->kernel_variant >= shapeCount(cfg->storage))
         return h->fail(TLM_EINVAL, "kernel_variant out of range for this storage mode");
     if (cfg->rounding < 0 || cfg->rounding > 1) return h->fail(TLM_EINVAL, "rounding must be 0 or 1");
+    if (cfg->general_tiles < 0 || cfg->general_tiles > 1)
+        return h->fail(TLM_EINVAL, "general_tiles must be 0 or 1");
     if (!std::isfinite(cfg->boundary_rho)) return h->fail(TLM_EINVAL, "boundary_rho not finite");
     bool anyDiel = false;
     for (long long c = 0; c < n; ++c)
@@ -869,7 +931,7 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     h->ncell = n;
     h->nquads = (long long)h->nq * h->ny * h->nz;
     const long long nb = (h->nquads + kBlock - 1) / kBlock;
-    if (nb > 0x7fffffffLL) return h->fail(TLM_EINVAL, "grid too large");
+    if (h->nquads >= (1LL << 31)) return h->fail(TLM_EINVAL, "grid too large");
     h->nblocks = (int)nb;
     h->anyDiel = anyDiel;
     h->mat.assign(mat, mat + n);

@@ -34,6 +34,7 @@ template <class S> struct StepArgs
     long long P;                   // plane stride (elements)
     long long nquads;              // number of V-node groups
     int nx, ny, nz, px, nq;        // nq = px / V
+    FastDiv div_nq, div_ny;        // division by nq and by ny (nquads < 2^31)
     R rho;
     R scale, inv_scale;            // pulse = stored * scale (BF16/F16)
     // sources and monitors
@@ -45,7 +46,16 @@ template <class S> struct StepArgs
     unsigned int *__restrict__ fault;  // bounds-check record (checked builds)
     unsigned int round_seed;       // per-step seed of stochastic rounding
     int stochastic;                // BF16/F16: round stochastically
+    const uint8_t *__restrict__ tile_flags;  // per tile: kTileGeneral / kTileDiel (nullptr: all general)
+    float neg_zero;                // -0.0f, supplied at run time (see mul2)
 };
+
+// Per-tile flags, computed on the host from the material map and the source
+// and monitor lists. A tile without kTileGeneral is an interior tile: every
+// thread of it is live, none of its nodes lies in a row on a y or z face of
+// the grid, neither its nodes nor their six neighbours are PEC, and it holds
+// no source or monitor. kTileDiel: the tile has stub-loaded nodes.
+enum : uint8_t { kTileGeneral = 1, kTileDiel = 2 };
 
 #ifdef TLM_CHECKED
 #define TLM_GUARD(idx, limit, code)                                                         \
@@ -65,7 +75,7 @@ __device__ __forceinline__ void loadVec(const S *__restrict__ base, long long no
     {
         static_assert(V == 4, "block floating point groups hold 4 nodes");
         float v[4];
-        bfpDecode(base[node >> 2].w, v);
+        bfpDecode(base[node >> 2], v);
 #pragma unroll
         for (int c = 0; c < 4; ++c) dst[c] = v[c];
     }
@@ -82,7 +92,7 @@ __device__ __forceinline__ typename Traits<S>::R loadOne(const S *__restrict__ b
                                                          typename Traits<S>::R scale)
 {
     if constexpr (std::is_same<S, Bfp4>::value)
-        return bfpDecodeOne(base[node >> 2].w, (int)(node & 3));
+        return bfpDecodeOne(base[node >> 2], (int)(node & 3));
     else
         return decode(base[node], scale);
 }
@@ -99,7 +109,7 @@ __device__ __forceinline__ void storeVec(S *__restrict__ base, long long node,
     {
         static_assert(V == 4, "block floating point groups hold 4 nodes");
         float v[4] = { src[0], src[1], src[2], src[3] };
-        base[node >> 2].w = bfpEncode(v, stochastic, mix32((unsigned)(node * 12 + salt) ^ seed));
+        base[node >> 2] = bfpEncode(v, stochastic, (unsigned)(node * 12 + salt) ^ seed);
     }
     else
     {
@@ -135,6 +145,223 @@ template <int V> __device__ __forceinline__ unsigned pecMask(const uint8_t (&m)[
     return r;
 }
 
+// Interior tile (see kTileGeneral): the gather needs no PEC and no y/z face
+// handling, so every pulse load is issued before any material is read; the
+// x faces (first and last node of a row) and the row padding are fixed up
+// per thread. Pairs of nodes scatter with packed FP32x2 arithmetic. The
+// results are bitwise those of the general tile body below.
+template <class S, int V>
+__device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel)
+{
+    using R = float;
+    static_assert(V % 2 == 0, "interior tiles scatter node pairs");
+    const int lane = threadIdx.x & 31;
+    const unsigned q = (unsigned)tile * kBlock + threadIdx.x;  // every thread of the tile is live
+    const unsigned rowu = fastDiv(q, a.div_nq);
+    const int x0 = (int)(q - rowu * (unsigned)a.nq) * V;
+    const long long node0 = (long long)q * V;
+    const long long P = a.P;
+    const long long sy = a.px, sz = (long long)a.px * a.ny;
+
+    // ---- loads: own x-slots, then the y and z neighbours' opposite faces ----
+    R ox[4][V];
+    R inc[12][V];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) loadVec<S, V>(a.in, s * P + node0, ox[s], a.scale);
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+    {
+        loadVec<S, V>(a.in, (6 + t) * P + node0 - sy, inc[4 + t], a.scale);   // -y face: (y,+) below
+        loadVec<S, V>(a.in, (4 + t) * P + node0 + sy, inc[6 + t], a.scale);   // +y face: (y,-) above
+        loadVec<S, V>(a.in, (10 + t) * P + node0 - sz, inc[8 + t], a.scale);  // -z face
+        loadVec<S, V>(a.in, (8 + t) * P + node0 + sz, inc[10 + t], a.scale);  // +z face
+    }
+    // ---- x neighbours: own vector, adjacent lane, or (warp edge) a scalar load ----
+    R prevX[2], nextX[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+    {
+        prevX[t] = __shfl_up_sync(0xffffffffu, ox[2 + t][V - 1], 1);
+        nextX[t] = __shfl_down_sync(0xffffffffu, ox[t][0], 1);
+    }
+    if (lane == 0 && x0 > 0)
+    {
+#pragma unroll
+        for (int t = 0; t < 2; ++t) prevX[t] = loadOne<S>(a.in, (2 + t) * P + node0 - 1, a.scale);
+    }
+    if (lane == 31 && x0 + V <= a.nx - 1)
+    {
+#pragma unroll
+        for (int t = 0; t < 2; ++t) nextX[t] = loadOne<S>(a.in, t * P + node0 + V, a.scale);
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+    {
+#pragma unroll
+        for (int c = 0; c < V; ++c)
+        {
+            inc[t][c] = (c > 0) ? ox[2 + t][c > 0 ? c - 1 : 0] : prevX[t];          // -x face
+            inc[2 + t][c] = (c < V - 1) ? ox[t][c < V - 1 ? c + 1 : 0] : nextX[t];  // +x face
+        }
+    }
+    // outer x faces: rho times the own reflected pulse
+    if (x0 == 0)
+    {
+#pragma unroll
+        for (int t = 0; t < 2; ++t) inc[t][0] = a.rho * ox[t][0];
+    }
+    const int cHi = a.nx - 1 - x0;  // the node at x = nx-1, if this thread holds it
+    if (cHi < V)
+    {
+#pragma unroll
+        for (int c = 0; c < V; ++c)
+            if (c == cHi)
+            {
+#pragma unroll
+                for (int t = 0; t < 2; ++t) inc[2 + t][c] = a.rho * ox[2 + t][c];
+            }
+    }
+    const unsigned liveMask = cHi >= V - 1 ? (1u << V) - 1 : (cHi < 0 ? 0u : (1u << (cHi + 1)) - 1);
+
+    // ---- energy: sum of squares of the incident link pulses, FP64 ----
+    if (a.epart != nullptr)
+    {
+        double e = 0.0;
+#pragma unroll
+        for (int c = 0; c < V; ++c)
+        {
+            if ((liveMask >> c) & 1u)
+            {
+#pragma unroll
+                for (int s = 0; s < 12; ++s) e += (double)inc[s][c] * (double)inc[s][c];
+            }
+        }
+        const double tot = blockSumDouble(e, red);
+        if (threadIdx.x == 0) a.epart[tile] = tot;
+    }
+
+    // ---- scatter (pairs of nodes) and store ----
+    uint8_t m[V];
+    unsigned dielMask = 0;
+    if (diel)
+    {
+        loadMat<V>(a.mat, node0, m);
+#pragma unroll
+        for (int c = 0; c < V; ++c) dielMask |= ((m[c] >= kDiel0) ? 1u : 0u) << c;
+        dielMask &= liveMask;
+    }
+    R vs[3][V];
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj)
+    {
+#pragma unroll
+        for (int c = 0; c < V; ++c) vs[jj][c] = R(0);
+    }
+    if (dielMask)
+    {
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj)
+        {
+            const Pack<R, V> p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
+#pragma unroll
+            for (int c = 0; c < V; ++c) vs[jj][c] = p.v[c];
+        }
+    }
+    R outv[12][V];
+    const float2 z = splat2(a.neg_zero);
+#pragma unroll
+    for (int pr = 0; pr < V / 2; ++pr)
+    {
+        const int c0 = 2 * pr, c1 = 2 * pr + 1;
+        const unsigned pm = (dielMask >> c0) & 3u;
+        if (pm == 0u)
+        {
+            float2 in2[12], o2[12];
+#pragma unroll
+            for (int s = 0; s < 12; ++s) in2[s] = make_float2(inc[s][c0], inc[s][c1]);
+            scatterAir2(in2, o2, z);
+#pragma unroll
+            for (int s = 0; s < 12; ++s)
+            {
+                outv[s][c0] = o2[s].x;
+                outv[s][c1] = o2[s].y;
+            }
+        }
+        else if (pm == 3u)
+        {
+            float2 in2[12], o2[12], v2[3];
+#pragma unroll
+            for (int s = 0; s < 12; ++s) in2[s] = make_float2(inc[s][c0], inc[s][c1]);
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) v2[jj] = make_float2(vs[jj][c0], vs[jj][c1]);
+            const int id0 = m[c0] - kDiel0, id1 = m[c1] - kDiel0;
+            scatterStub2(in2, v2, make_float2(a.yhat[id0], a.yhat[id1]), make_float2(a.ghat[id0], a.ghat[id1]),
+                         o2, z);
+#pragma unroll
+            for (int s = 0; s < 12; ++s)
+            {
+                outv[s][c0] = o2[s].x;
+                outv[s][c1] = o2[s].y;
+            }
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+            {
+                vs[jj][c0] = v2[jj].x;
+                vs[jj][c1] = v2[jj].y;
+            }
+        }
+        else
+        {
+            // one air and one stub-loaded node: scalar scatter of each
+#pragma unroll
+            for (int c = c0; c <= c1; ++c)
+            {
+                R in1[12], o1[12];
+#pragma unroll
+                for (int s = 0; s < 12; ++s) in1[s] = inc[s][c];
+                if ((dielMask >> c) & 1u)
+                {
+                    const int id = m[c] - kDiel0;
+                    R v3[3] = { vs[0][c], vs[1][c], vs[2][c] };
+                    scatterStub(in1, v3, a.yhat[id], a.ghat[id], o1);
+                    vs[0][c] = v3[0];
+                    vs[1][c] = v3[1];
+                    vs[2][c] = v3[2];
+                }
+                else
+                    scatterAir(in1, o1);
+#pragma unroll
+                for (int s = 0; s < 12; ++s) outv[s][c] = o1[s];
+            }
+        }
+    }
+    if (liveMask != (1u << V) - 1)
+    {
+        // row padding (and nothing else) is not live: its pulses stay zero
+#pragma unroll
+        for (int c = 0; c < V; ++c)
+            if (!((liveMask >> c) & 1u))
+            {
+#pragma unroll
+                for (int s = 0; s < 12; ++s) outv[s][c] = R(0);
+            }
+    }
+#pragma unroll
+    for (int s = 0; s < 12; ++s)
+        storeVec<S, V>(a.out, s * P + node0, outv[s], a.inv_scale, a.stochastic != 0, a.round_seed, s);
+    if (dielMask)
+    {
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj)
+        {
+            Pack<R, V> p;
+#pragma unroll
+            for (int c = 0; c < V; ++c) p.v[c] = vs[jj][c];
+            *reinterpret_cast<Pack<R, V> *>(a.stub + jj * P + node0) = p;
+        }
+    }
+}
+
 // One tile of kBlock threads x V nodes: tile `tile` covers the V-node
 // groups [tile*kBlock, (tile+1)*kBlock). `red` is kBlock/32 doubles of
 // shared memory. kIncident: the input planes hold INCIDENT pulses (state
@@ -144,15 +371,28 @@ template <class S, int V, bool kIncident, bool kSelect = true>
 __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double *red)
 {
     using R = typename Traits<S>::R;
+    if constexpr (!kIncident && std::is_same<R, float>::value && V % 2 == 0)
+    {
+        if (a.tile_flags != nullptr)
+        {
+            const uint8_t f = a.tile_flags[tile];
+            if (!(f & kTileGeneral))
+            {
+                stepTileInterior<S, V>(a, tile, red, (f & kTileDiel) != 0);
+                return;
+            }
+        }
+    }
 
     const int lane = threadIdx.x & 31;
     const long long q = (long long)tile * kBlock + threadIdx.x;
     const bool live = q < a.nquads;
     const long long qq = live ? q : 0;
-    const int xq = (int)(qq % a.nq);
-    const long long row = qq / a.nq;
-    const int j = (int)(row % a.ny);
-    const int k = (int)(row / a.ny);
+    const unsigned rowu = fastDiv((unsigned)qq, a.div_nq);
+    const int xq = (int)((unsigned)qq - rowu * (unsigned)a.nq);
+    const unsigned ku = fastDiv(rowu, a.div_ny);
+    const int j = (int)(rowu - ku * (unsigned)a.ny);
+    const int k = (int)ku;
     const int x0 = xq * V;
     const long long node0 = qq * V;
     const long long P = a.P;

@@ -89,7 +89,8 @@ class TlmConfig:
     pulseScale: float = 0.0
     stepsPerLaunch: int = 0
     kernelVariant: int = 0
-    rounding: int = 0          # BF16/F16 storage: 0 nearest, 1 stochastic
+    rounding: int = 0          # 16-bit storage: 0 nearest, 1 stochastic
+    generalTiles: bool = False  # True: no interior-tile fast path (cross-checks)
 
     def to_c(self):
         c = _lib.ConfigC()
@@ -106,6 +107,7 @@ class TlmConfig:
         c.steps_per_launch = int(self.stepsPerLaunch)
         c.kernel_variant = int(self.kernelVariant)
         c.rounding = int(self.rounding)
+        c.general_tiles = 1 if self.generalTiles else 0
         return c
 
 

@@ -109,7 +109,10 @@ typedef struct tlm_config {
     int steps_per_launch;/* steps per monitor window; 0 = default (64) */
     int kernel_variant;  /* thread-tile shape of the step kernel; 0 = default
                             (tlm_kernel_variants lists the others) */
-    int rounding;        /* BF16/F16 storage: 0 round to nearest, 1 stochastic */
+    int rounding;        /* 16-bit storage: 0 round to nearest, 1 stochastic */
+    int general_tiles;   /* 1: every tile runs the general step body (no
+                            interior-tile fast path); results are identical,
+                            the switch exists to cross-check the two bodies */
 } tlm_config;
 
 typedef struct tlm_solver *tlm_handle;

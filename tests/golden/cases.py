@@ -55,3 +55,88 @@ def small_cases():
             w.meta["plane_wave"] = (2, nz // 2, 0, 0.7)
         cases.append(w)
     return cases
+
+
+def mid_cases():
+    """Grids large enough to hold interior tiles of the step kernel (tiles of
+    1024 nodes away from the y/z faces, PEC and sources), with x extents that
+    leave row padding, a PEC block and isolated PEC voxels, overlapping lossy
+    dielectric boxes,
+    three-cell ports and probes."""
+    cases = []
+    specs = [
+        # name, dims, rho, nbox, pec, waveform, steps, seed
+        ("mid_pec_diel", (45, 150, 20), 0.3, 4, 12, 2, 40, 11),
+        ("mid_diel_rho_m1", (61, 120, 18), -1.0, 5, 0, 1, 36, 12),
+        ("mid_air", (30, 200, 14), 0.0, 0, 0, 2, 30, 13),
+    ]
+    for name, (nx, ny, nz), rho, nbox, pec, wf, steps, seed in specs:
+        rng = np.random.default_rng(seed)
+        mat = np.zeros((nz, ny, nx), np.uint8)
+        table = []
+        for b in range(nbox):
+            lo = [int(rng.integers(0, d)) for d in (nz, ny, nx)]
+            hi = [min(d, l + int(rng.integers(4, d // 2 + 5))) for l, d in zip(lo, (nz, ny, nx))]
+            mat[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = 2 + b
+            table.append((float(np.float32(rng.uniform(1, 10))), float(np.float32(rng.uniform(0, 0.05)))))
+        if pec > 0:
+            # a small PEC block and `pec` isolated PEC voxels
+            k0, j0, i0 = (int(rng.integers(1, d - 4)) for d in (nz, ny, nx))
+            mat[k0:k0 + 3, j0:j0 + 3, i0:i0 + 3] = 1
+            for _ in range(pec):
+                mat[tuple(int(rng.integers(0, d)) for d in (nz, ny, nx))] = 1
+        mat = mat.reshape(-1)
+        w = workloads.Workload(name, nx, ny, nz, mat, table, dl=1e-3, f0=3e10, waveform=wf,
+                               steps=steps, rho=rho)
+        kk, jj, ii = np.unravel_index(np.arange(mat.size), (nz, ny, nx))
+        inner = (ii > 0) & (ii < nx - 1) & (jj > 0) & (jj < ny - 1) & (kk > 0) & (kk < nz - 1)
+        air = np.flatnonzero((mat == 0) & inner)
+        for p in range(2):
+            cells = [int(c) for c in rng.choice(air, 3)]
+            w.ports.append((cells, int(rng.integers(0, 3)), float(np.float32(rng.uniform(-2, 2)))))
+        for q in range(3):
+            w.probes_cell.append(tuple(int(rng.integers(0, d)) for d in (nx, ny, nz)))
+        cases.append(w)
+    return cases
+
+
+def interior_tiles(w, V=4, block=256):
+    """Number of interior tiles the step kernel finds in `w` with V nodes per
+    thread (mirrors the host rule: no y/z face row, no PEC node or PEC
+    neighbour, no source or monitor node, not the partial last tile)."""
+    nx, ny, nz = w.nx, w.ny, w.nz
+    px = (nx + 7) // 8 * 8
+    P = px * ny * nz
+    T = block * V
+    nb = (P // V + block - 1) // block
+    gen = np.zeros(nb, bool)
+    if (P // V) % block:
+        gen[-1] = True
+    mat = np.asarray(w.mat).reshape(nz, ny, nx)
+    kk, jj = np.meshgrid(np.arange(nz), np.arange(ny), indexing="ij")
+    face = (jj == 0) | (jj == ny - 1) | (kk == 0) | (kk == nz - 1)
+    for k, j in zip(kk[face], jj[face]):
+        r0 = (k * ny + j) * px
+        gen[r0 // T:(r0 + px - 1) // T + 1] = True
+
+    def node(i, j, k):
+        return (k * ny + j) * px + i
+
+    for k, j, i in zip(*np.nonzero(mat == 1)):
+        for n in (node(i, j, k), node(i - 1, j, k) if i > 0 else -1, node(i + 1, j, k) if i < nx - 1 else -1,
+                  node(i, j, k) - px, node(i, j, k) + px, node(i, j, k) - px * ny, node(i, j, k) + px * ny):
+            if 0 <= n < P:
+                gen[n // T] = True
+    spec = []
+    for cells, _, _ in w.ports:
+        for c in cells:
+            spec.append(c)
+            i, j, k = c % nx, (c // nx) % ny, c // (nx * ny)
+            spec += [(k * ny + j2) * nx + i2 for i2, j2 in ((i, j - 1), (i, j + 1), (i - 1, j), (i + 1, j))
+                     if 0 <= i2 < nx and 0 <= j2 < ny]
+    for (i, j, k) in w.probes_cell:
+        spec.append((k * ny + j) * nx + i)
+    for c in spec:
+        i, r = c % nx, c // nx
+        gen[(r * px + i) // T] = True
+    return int((~gen).sum())

@@ -1,0 +1,62 @@
+"""The interior-tile body of the step kernel on a B200.
+
+Tiles away from the y/z faces, PEC and sources take a second step body (all
+pulse loads first, packed FP32x2 scatter of node pairs). On grids that hold
+such tiles: FP32 storage is bitwise the reference's CPU step (oracle), and
+for every storage mode and tile shape the interior body gives bitwise the
+state and records of the general body (tlm_config.general_tiles = 1)."""
+import numpy as np
+import pytest
+
+from emsolver_b200 import _lib
+from emsolver_b200.runner import build_solver, records
+from emsolver_b200.solver import Storage
+from oracle import Oracle, drive
+from tests.golden.cases import interior_tiles, mid_cases
+
+pytestmark = pytest.mark.gpu
+
+MID = mid_cases()
+
+
+def test_mid_cases_hold_interior_tiles():
+    for w in MID:
+        assert interior_tiles(w) > 0 and interior_tiles(w, V=2) > 0 and interior_tiles(w, V=8) > 0
+
+
+@pytest.mark.parametrize("w", MID, ids=[w.name for w in MID])
+def test_interior_tiles_bitwise_vs_oracle(built, w):
+    s = build_solver(w)
+    s.step(w.steps)
+    O = Oracle(False)
+    drive.setup(O, w)
+    drive.advance(O, w, w.steps)
+    assert np.array_equal(s.pulses(), O.pulses())
+    if w.table:
+        assert np.array_equal(s.stubs(), O.stubs())
+    ra, ro = records(s, w), drive.records(O, w)
+    for k in ra:
+        if k.startswith("energy"):
+            continue
+        assert np.array_equal(ra[k], ro[k]), k
+
+
+@pytest.mark.parametrize("storage", [Storage.F32, Storage.BF16, Storage.F16, Storage.BFP16, Storage.F64])
+@pytest.mark.parametrize("rounding", [0, 1])
+def test_interior_body_equals_general_body(built, storage, rounding):
+    if storage in (Storage.F32, Storage.F64) and rounding:
+        pytest.skip("rounding applies to 16-bit storage")
+    L = _lib.load()
+    w = MID[0]
+    for v in range(L.tlm_kernel_variants(int(storage))):
+        out = []
+        for general in (True, False):
+            s = build_solver(w, storage=storage, kernel_variant=v, rounding=rounding, general_tiles=general)
+            s.step(w.steps)
+            out.append((s.pulses(f64=True), s.stubs(), records(s, w, f64=True)))
+            s.close()
+        (pa, sa, ra), (pb, sb, rb) = out
+        assert np.array_equal(pa, pb), (storage, v)
+        assert np.array_equal(sa, sb), (storage, v)
+        for k in ra:
+            assert np.array_equal(ra[k], rb[k]), (storage, v, k)

@@ -242,7 +242,7 @@ def test_bfp16_storage_quantisation_bound(built):
     pad = np.zeros((nz, ny, px, 12))
     pad[:, :, :nx] = want
     gmax = np.abs(pad).reshape(nz, ny, px // 4, 4, 12).max(axis=3)
-    bound = np.repeat(gmax, 4, axis=2)[:, :, :nx] * 2.0 ** -13 * (1 + 1e-6)
+    bound = np.repeat(gmax, 4, axis=2)[:, :, :nx] * 2.0 ** -13 * (1 + 2.0 ** -11)
     assert np.all(np.abs(got - want) <= bound)
     assert np.all(got[:, :, :4, 3] == 0.0)
     assert np.all(got[~np.broadcast_to(live, got.shape)] == 0.0)
