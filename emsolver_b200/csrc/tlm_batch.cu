@@ -259,35 +259,14 @@ tlm_status launchGroupStep(tlm_batch_s *b, Group &g, int i, bool doLaunch)
 }
 
 // The step launch of a group in its tile shape (the shape tables of
-// tlm_internal.h: variant 0 = Traits<S> default).
+// tlm_internal.h).
 template <class S> tlm_status launchShape(tlm_batch_s *b, Group &g, int i, bool go)
 {
-    constexpr int V0 = tlmk::Traits<S>::V;
-    constexpr int M0 = tlmk::Traits<S>::kMinBlocks;
-    constexpr bool S0 = tlmk::Traits<S>::kSelect;
-    if (g.variant == 0) return launchGroupStep<S, V0, M0, S0>(b, g, i, go);
-    if constexpr (std::is_same<S, double>::value)
-    {
-        if (g.variant == 1) return launchGroupStep<S, 1, 4, false>(b, g, i, go);
-        return launchGroupStep<S, 2, 3, false>(b, g, i, go);
-    }
-    else if constexpr (std::is_same<S, float>::value)
-    {
-        if (g.variant == 1) return launchGroupStep<S, 4, 3, true>(b, g, i, go);
-        if (g.variant == 2) return launchGroupStep<S, 2, 4, true>(b, g, i, go);
-        return launchGroupStep<S, 4, 2, false>(b, g, i, go);
-    }
-    else if constexpr (std::is_same<S, tlmk::Bfp4>::value)
-    {
-        if (g.variant == 1) return launchGroupStep<S, 4, 3, true>(b, g, i, go);
-        return launchGroupStep<S, 4, 2, false>(b, g, i, go);
-    }
-    else
-    {
-        if (g.variant == 1) return launchGroupStep<S, 4, 3, true>(b, g, i, go);
-        if (g.variant == 2) return launchGroupStep<S, 2, 4, true>(b, g, i, go);
-        return launchGroupStep<S, 8, 2, false>(b, g, i, go);
-    }
+    tlm_status st = TLM_EINVAL;
+    withShape<S>(g.variant, [&](auto V, auto MINB, auto SEL) {
+        st = launchGroupStep<S, V(), MINB(), SEL()>(b, g, i, go);
+    });
+    return st;
 }
 
 tlm_status launchStep(tlm_batch_s *b, Group &g, int i, bool go = true)

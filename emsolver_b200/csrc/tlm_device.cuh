@@ -38,9 +38,9 @@ template <class S> struct Traits;
 template <> struct Traits<float>
 {
     using R = float;
-    static constexpr int V = 4;
-    static constexpr int kMinBlocks = 3;
-    static constexpr bool kSelect = false;
+    static constexpr int V = 2;
+    static constexpr int kMinBlocks = 4;
+    static constexpr bool kSelect = true;
     static constexpr bool kScaled = false;
 };
 template <> struct Traits<double>
@@ -56,7 +56,7 @@ template <> struct Traits<__half>
     using R = float;
     static constexpr int V = 4;
     static constexpr int kMinBlocks = 3;
-    static constexpr bool kSelect = false;
+    static constexpr bool kSelect = true;
     static constexpr bool kScaled = true;
 };
 template <> struct Traits<__nv_bfloat16>
@@ -64,7 +64,7 @@ template <> struct Traits<__nv_bfloat16>
     using R = float;
     static constexpr int V = 4;
     static constexpr int kMinBlocks = 3;
-    static constexpr bool kSelect = false;
+    static constexpr bool kSelect = true;
     static constexpr bool kScaled = true;
 };
 
@@ -123,7 +123,7 @@ template <> struct Traits<Bfp4>
     using R = float;
     static constexpr int V = 4;
     static constexpr int kMinBlocks = 3;
-    static constexpr bool kSelect = false;
+    static constexpr bool kSelect = true;
     static constexpr bool kScaled = false;
 };
 

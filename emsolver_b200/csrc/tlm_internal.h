@@ -6,6 +6,7 @@
 #include "tlm_device.cuh"
 
 #include <atomic>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -53,29 +54,85 @@ inline size_t storageBytes(int storage)
 }
 inline size_t realBytes(int storage) { return storage == TLM_STORE_F64 ? 8 : 4; }
 
-// Step-kernel tile shapes per storage mode: {nodes per thread, min blocks
-// per SM}. Entry 0 is the default; the autotuner and kernel_variant pick
-// among them.
+// Step-kernel tile shapes per storage mode: {nodes per thread V, min blocks
+// per SM, scatter style}. Entry 0 is the default (tlmk::Traits<S>, the
+// fastest shape measured on B200 for the 192^3 heterogeneous grid); the
+// autotuner and tlm_config.kernel_variant pick among the others.
 struct Shape
 {
     int V, minb;
     int select;  // 1: warp-uniform select between air and stub scatter; 0: per-node branch
 };
-constexpr Shape kShapesF32[] = { { 4, 3, 0 }, { 4, 3, 1 }, { 2, 4, 1 }, { 4, 2, 0 } };
+constexpr Shape kShapesF32[] = { { 2, 4, 1 }, { 4, 3, 1 }, { 4, 3, 0 }, { 4, 2, 0 } };
 constexpr Shape kShapesF64[] = { { 1, 4, 1 }, { 1, 4, 0 }, { 2, 3, 0 } };
-constexpr Shape kShapesHalf[] = { { 4, 3, 0 }, { 4, 3, 1 }, { 2, 4, 1 }, { 8, 2, 0 } };
-// block floating point: a thread owns one 4-node group
-constexpr Shape kShapesBfp[] = { { 4, 3, 0 }, { 4, 3, 1 }, { 4, 2, 0 } };
+constexpr Shape kShapesHalf[] = { { 4, 3, 1 }, { 4, 3, 0 }, { 2, 4, 1 }, { 8, 2, 0 } };
+// block floating point: a thread owns whole 4-node groups
+constexpr Shape kShapesBfp[] = { { 4, 3, 1 }, { 4, 3, 0 }, { 4, 2, 0 } };
+
+template <class S> struct ShapeTable;
+template <> struct ShapeTable<float>
+{
+    static constexpr const Shape *v = kShapesF32;
+    static constexpr int n = sizeof(kShapesF32) / sizeof(Shape);
+};
+template <> struct ShapeTable<double>
+{
+    static constexpr const Shape *v = kShapesF64;
+    static constexpr int n = sizeof(kShapesF64) / sizeof(Shape);
+};
+template <> struct ShapeTable<__half>
+{
+    static constexpr const Shape *v = kShapesHalf;
+    static constexpr int n = sizeof(kShapesHalf) / sizeof(Shape);
+};
+template <> struct ShapeTable<__nv_bfloat16>
+{
+    static constexpr const Shape *v = kShapesHalf;
+    static constexpr int n = sizeof(kShapesHalf) / sizeof(Shape);
+};
+template <> struct ShapeTable<tlmk::Bfp4>
+{
+    static constexpr const Shape *v = kShapesBfp;
+    static constexpr int n = sizeof(kShapesBfp) / sizeof(Shape);
+};
+
+// Entry 0 of every table is the storage type's default kernel shape.
+template <class S> constexpr bool defaultShapeMatches()
+{
+    return ShapeTable<S>::v[0].V == tlmk::Traits<S>::V && ShapeTable<S>::v[0].minb == tlmk::Traits<S>::kMinBlocks &&
+           (ShapeTable<S>::v[0].select != 0) == tlmk::Traits<S>::kSelect;
+}
+static_assert(defaultShapeMatches<float>() && defaultShapeMatches<double>() && defaultShapeMatches<__half>() &&
+                  defaultShapeMatches<__nv_bfloat16>() && defaultShapeMatches<tlmk::Bfp4>(),
+              "entry 0 of a shape table must be the Traits default");
+
+// Calls f(V, MINB, SEL) (std::integral_constant arguments) for shape
+// `variant` of storage type S; the one place where table entries become
+// kernel template arguments.
+template <class S, int I = 0, class F> void withShape(int variant, F &&f)
+{
+    if constexpr (I < ShapeTable<S>::n)
+    {
+        if (variant == I)
+        {
+            constexpr Shape sh = ShapeTable<S>::v[I];
+            f(std::integral_constant<int, sh.V>{}, std::integral_constant<int, sh.minb>{},
+              std::integral_constant<bool, sh.select != 0>{});
+        }
+        else
+            withShape<S, I + 1>(variant, f);
+    }
+}
 
 inline int shapeCount(int storage)
 {
     switch (storage)
     {
-    case TLM_STORE_F64: return (int)(sizeof(kShapesF64) / sizeof(Shape));
+    case TLM_STORE_F64: return ShapeTable<double>::n;
     case TLM_STORE_BF16:
-    case TLM_STORE_F16: return (int)(sizeof(kShapesHalf) / sizeof(Shape));
-    case TLM_STORE_BFP16: return (int)(sizeof(kShapesBfp) / sizeof(Shape));
-    case TLM_STORE_F32: return (int)(sizeof(kShapesF32) / sizeof(Shape));
+    case TLM_STORE_F16: return ShapeTable<__half>::n;
+    case TLM_STORE_BFP16: return ShapeTable<tlmk::Bfp4>::n;
+    case TLM_STORE_F32: return ShapeTable<float>::n;
     default: return 0;
     }
 }

@@ -28,6 +28,7 @@ void tlmSetThreadError(const std::string &m);
 // Scratch: one energy partial per step-kernel block. 65,536 blocks of 256
 // threads x 4 nodes bound the grid at 67,108,864 padded nodes.
 constexpr int kNoAllocMaxBlocks = 65536;
+constexpr int kNoAllocV = 4;  // nodes per thread: 65536 blocks x 256 x 4 = 67,108,864 nodes
 static __device__ __align__(256) double g_noallocPartials[kNoAllocMaxBlocks];
 // Sink for the bounds-check record of the checked library build (unused by
 // the regular build), so that no kernel is ever handed a null fault word.
@@ -116,7 +117,7 @@ tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_planes, fl
     if (!aligned16(in_planes) || !aligned16(out_planes) || (stubs && !aligned16(stubs)) ||
         ((uintptr_t)mat & 3u))
         return noallocFail(TLM_EINVAL, "planes must be 16-byte aligned, the material map 4-byte aligned");
-    constexpr int V = tlmk::Traits<float>::V;
+    constexpr int V = kNoAllocV;
     const long long px = (long long)(nx + tlmk::kPadX - 1) / tlmk::kPadX * tlmk::kPadX;
     const long long P = px * ny * nz;
     const long long nq = px / V;
@@ -161,9 +162,9 @@ tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_planes, fl
     a.fault = fault;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (input_is_incident)
-        tlmk::stepKernel<float, true><<<(unsigned)nblocks, tlmk::kBlock, 0, s>>>(a);
+        tlmk::stepKernelShaped<float, kNoAllocV, 3, true, false><<<(unsigned)nblocks, tlmk::kBlock, 0, s>>>(a);
     else
-        tlmk::stepKernel<float, false><<<(unsigned)nblocks, tlmk::kBlock, 0, s>>>(a);
+        tlmk::stepKernelShaped<float, kNoAllocV, 3, false, false><<<(unsigned)nblocks, tlmk::kBlock, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && energy_out)
     {

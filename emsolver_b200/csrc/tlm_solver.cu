@@ -113,8 +113,8 @@ long long paddedNode(const tlm_solver *h, uint64_t cell)
 
 // Per-tile flags of the step kernel (tlmk::kTileGeneral, tlmk::kTileDiel):
 // a tile is general when it is the partial last tile, holds a source or
-// monitor entry (tileBegin ranges), covers a row on a y or z face of the
-// grid, or holds a node that is PEC or next to a PEC node.
+// monitor entry (tileBegin ranges), or holds a node that is PEC or next to a
+// PEC node.
 std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tileBegin)
 {
     const long long T = (long long)kBlock * h->V;
@@ -126,34 +126,33 @@ std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tile
     if (h->nquads % kBlock) f[(size_t)nb - 1] |= tlmk::kTileGeneral;
     for (int b = 0; b < nb; ++b)
         if (tileBegin[b + 1] > tileBegin[b]) f[(size_t)b] |= tlmk::kTileGeneral;
+    const long long sy = h->px, sz = (long long)h->px * h->ny;
+    const uint8_t *mat = h->mat.data();
     for (int k = 0; k < h->nz; ++k)
         for (int j = 0; j < h->ny; ++j)
         {
-            if (!(j == 0 || j == h->ny - 1 || k == 0 || k == h->nz - 1)) continue;
             const long long r0 = ((long long)k * h->ny + j) * h->px;
-            for (long long t = r0 / T; t <= (r0 + h->px - 1) / T; ++t) f[(size_t)t] |= tlmk::kTileGeneral;
+            const uint8_t *row = mat + ((size_t)k * h->ny + j) * h->nx;
+            for (int i = 0; i < h->nx; ++i)
+            {
+                const uint8_t m = row[i];
+                if (m == tlmk::kAir) continue;
+                const long long node = r0 + i;
+                if (m >= tlmk::kDiel0)
+                {
+                    f[(size_t)(node / T)] |= tlmk::kTileDiel;
+                    continue;
+                }
+                // PEC: the node and every node that has it as a neighbour
+                mark(node, tlmk::kTileGeneral);
+                if (i > 0) mark(node - 1, tlmk::kTileGeneral);
+                if (i < h->nx - 1) mark(node + 1, tlmk::kTileGeneral);
+                mark(node - sy, tlmk::kTileGeneral);
+                mark(node + sy, tlmk::kTileGeneral);
+                mark(node - sz, tlmk::kTileGeneral);
+                mark(node + sz, tlmk::kTileGeneral);
+            }
         }
-    const long long sy = h->px, sz = (long long)h->px * h->ny;
-    for (long long c = 0; c < h->ncell; ++c)
-    {
-        const uint8_t m = h->mat[(size_t)c];
-        if (m == tlmk::kAir) continue;
-        const long long node = paddedNode(h, (uint64_t)c);
-        if (m >= tlmk::kDiel0)
-        {
-            mark(node, tlmk::kTileDiel);
-            continue;
-        }
-        // PEC: the node and every node that has it as a neighbour
-        const long long i = c % h->nx;
-        mark(node, tlmk::kTileGeneral);
-        if (i > 0) mark(node - 1, tlmk::kTileGeneral);
-        if (i < h->nx - 1) mark(node + 1, tlmk::kTileGeneral);
-        mark(node - sy, tlmk::kTileGeneral);
-        mark(node + sy, tlmk::kTileGeneral);
-        mark(node - sz, tlmk::kTileGeneral);
-        mark(node + sz, tlmk::kTileGeneral);
-    }
     return f;
 }
 
@@ -312,50 +311,17 @@ tlm_status ensureRecords(tlm_solver *h, long long need)
     return TLM_OK;
 }
 
-template <class S, int V, int MINB, bool SEL>
-void launchWithShape(const tlmk::StepArgs<S> &a, bool incident, int nblocks, cudaStream_t st)
-{
-    if (incident)
-        tlmk::stepKernelShaped<S, V, MINB, true, SEL><<<nblocks, kBlock, 0, st>>>(a);
-    else
-        tlmk::stepKernelShaped<S, V, MINB, false, SEL><<<nblocks, kBlock, 0, st>>>(a);
-}
-
 // Launch the step kernel in the tile shape `variant` of the storage type
-// (variant 0 is stepKernel's default shape; the table is tlmi::kShapes*).
+// (the shape tables of tlm_internal.h).
 template <class S>
 void launchShaped(const tlmk::StepArgs<S> &a, int variant, bool incident, int nblocks, cudaStream_t st)
 {
-    if (variant == 0)
-    {
+    withShape<S>(variant, [&](auto V, auto MINB, auto SEL) {
         if (incident)
-            tlmk::stepKernel<S, true><<<nblocks, kBlock, 0, st>>>(a);
+            tlmk::stepKernelShaped<S, V(), MINB(), true, SEL()><<<nblocks, kBlock, 0, st>>>(a);
         else
-            tlmk::stepKernel<S, false><<<nblocks, kBlock, 0, st>>>(a);
-        return;
-    }
-    if constexpr (std::is_same<S, double>::value)
-    {
-        if (variant == 1) launchWithShape<S, 1, 4, false>(a, incident, nblocks, st);
-        else launchWithShape<S, 2, 3, false>(a, incident, nblocks, st);
-    }
-    else if constexpr (std::is_same<S, float>::value)
-    {
-        if (variant == 1) launchWithShape<S, 4, 3, true>(a, incident, nblocks, st);
-        else if (variant == 2) launchWithShape<S, 2, 4, true>(a, incident, nblocks, st);
-        else launchWithShape<S, 4, 2, false>(a, incident, nblocks, st);
-    }
-    else if constexpr (std::is_same<S, tlmk::Bfp4>::value)
-    {
-        if (variant == 1) launchWithShape<S, 4, 3, true>(a, incident, nblocks, st);
-        else launchWithShape<S, 4, 2, false>(a, incident, nblocks, st);
-    }
-    else
-    {
-        if (variant == 1) launchWithShape<S, 4, 3, true>(a, incident, nblocks, st);
-        else if (variant == 2) launchWithShape<S, 2, 4, true>(a, incident, nblocks, st);
-        else launchWithShape<S, 8, 2, false>(a, incident, nblocks, st);
-    }
+            tlmk::stepKernelShaped<S, V(), MINB(), false, SEL()><<<nblocks, kBlock, 0, st>>>(a);
+    });
 }
 
 template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long eFirst)

@@ -52,9 +52,9 @@ template <class S> struct StepArgs
 
 // Per-tile flags, computed on the host from the material map and the source
 // and monitor lists. A tile without kTileGeneral is an interior tile: every
-// thread of it is live, none of its nodes lies in a row on a y or z face of
-// the grid, neither its nodes nor their six neighbours are PEC, and it holds
-// no source or monitor. kTileDiel: the tile has stub-loaded nodes.
+// thread of it is live, neither its nodes nor their six neighbours are PEC,
+// and it holds no source or monitor. kTileDiel: the tile has stub-loaded
+// nodes.
 enum : uint8_t { kTileGeneral = 1, kTileDiel = 2 };
 
 #ifdef TLM_CHECKED
@@ -145,11 +145,13 @@ template <int V> __device__ __forceinline__ unsigned pecMask(const uint8_t (&m)[
     return r;
 }
 
-// Interior tile (see kTileGeneral): the gather needs no PEC and no y/z face
-// handling, so every pulse load is issued before any material is read; the
-// x faces (first and last node of a row) and the row padding are fixed up
-// per thread. Pairs of nodes scatter with packed FP32x2 arithmetic. The
-// results are bitwise those of the general tile body below.
+// Interior tile (see kTileGeneral): the gather needs no PEC handling, so
+// every pulse load is issued before any material is read. On the outer faces
+// the load of the neighbour's pulse becomes a load of the own pulse, scaled
+// by rho afterwards (y/z faces: per thread; x faces, the first and last node
+// of a row, and the row padding: fixed up per node). Pairs of nodes scatter
+// with packed FP32x2 arithmetic. The results are bitwise those of the
+// general tile body below.
 template <class S, int V>
 __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel)
 {
@@ -159,9 +161,13 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     const unsigned q = (unsigned)tile * kBlock + threadIdx.x;  // every thread of the tile is live
     const unsigned rowu = fastDiv(q, a.div_nq);
     const int x0 = (int)(q - rowu * (unsigned)a.nq) * V;
+    const unsigned ku = fastDiv(rowu, a.div_ny);
+    const int j = (int)(rowu - ku * (unsigned)a.ny);
+    const int k = (int)ku;
     const long long node0 = (long long)q * V;
     const long long P = a.P;
     const long long sy = a.px, sz = (long long)a.px * a.ny;
+    const bool atYlo = j == 0, atYhi = j == a.ny - 1, atZlo = k == 0, atZhi = k == a.nz - 1;
 
     // ---- loads: own x-slots, then the y and z neighbours' opposite faces ----
     R ox[4][V];
@@ -171,10 +177,12 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
 #pragma unroll
     for (int t = 0; t < 2; ++t)
     {
-        loadVec<S, V>(a.in, (6 + t) * P + node0 - sy, inc[4 + t], a.scale);   // -y face: (y,+) below
-        loadVec<S, V>(a.in, (4 + t) * P + node0 + sy, inc[6 + t], a.scale);   // +y face: (y,-) above
-        loadVec<S, V>(a.in, (10 + t) * P + node0 - sz, inc[8 + t], a.scale);  // -z face
-        loadVec<S, V>(a.in, (8 + t) * P + node0 + sz, inc[10 + t], a.scale);  // +z face
+        // -y face: (y,+) of the row below; +y face: (y,-) of the row above;
+        // on an outer face the own pulse of the face instead
+        loadVec<S, V>(a.in, atYlo ? (4 + t) * P + node0 : (6 + t) * P + node0 - sy, inc[4 + t], a.scale);
+        loadVec<S, V>(a.in, atYhi ? (6 + t) * P + node0 : (4 + t) * P + node0 + sy, inc[6 + t], a.scale);
+        loadVec<S, V>(a.in, atZlo ? (8 + t) * P + node0 : (10 + t) * P + node0 - sz, inc[8 + t], a.scale);
+        loadVec<S, V>(a.in, atZhi ? (10 + t) * P + node0 : (8 + t) * P + node0 + sz, inc[10 + t], a.scale);
     }
     // ---- x neighbours: own vector, adjacent lane, or (warp edge) a scalar load ----
     R prevX[2], nextX[2];
@@ -204,7 +212,22 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
             inc[2 + t][c] = (c < V - 1) ? ox[t][c < V - 1 ? c + 1 : 0] : nextX[t];  // +x face
         }
     }
-    // outer x faces: rho times the own reflected pulse
+    // outer faces: rho times the own reflected pulse
+    if (atYlo | atYhi | atZlo | atZhi)
+    {
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+        {
+#pragma unroll
+            for (int c = 0; c < V; ++c)
+            {
+                if (atYlo) inc[4 + t][c] = a.rho * inc[4 + t][c];
+                if (atYhi) inc[6 + t][c] = a.rho * inc[6 + t][c];
+                if (atZlo) inc[8 + t][c] = a.rho * inc[8 + t][c];
+                if (atZhi) inc[10 + t][c] = a.rho * inc[10 + t][c];
+            }
+        }
+    }
     if (x0 == 0)
     {
 #pragma unroll

@@ -58,11 +58,10 @@ def small_cases():
 
 
 def mid_cases():
-    """Grids large enough to hold interior tiles of the step kernel (tiles of
-    1024 nodes away from the y/z faces, PEC and sources), with x extents that
-    leave row padding, a PEC block and isolated PEC voxels, overlapping lossy
-    dielectric boxes,
-    three-cell ports and probes."""
+    """Grids that hold both interior tiles of the step kernel (no PEC, source
+    or monitor nearby) and general ones: x extents that leave row padding, a
+    PEC block and isolated PEC voxels, overlapping lossy dielectric boxes,
+    three-cell ports and probes, outer faces with rho in {0, 0.3, -1}."""
     cases = []
     specs = [
         # name, dims, rho, nbox, pec, waveform, steps, seed
@@ -102,8 +101,8 @@ def mid_cases():
 
 def interior_tiles(w, V=4, block=256):
     """Number of interior tiles the step kernel finds in `w` with V nodes per
-    thread (mirrors the host rule: no y/z face row, no PEC node or PEC
-    neighbour, no source or monitor node, not the partial last tile)."""
+    thread (mirrors the host rule: no PEC node or PEC neighbour, no source or
+    monitor node, not the partial last tile)."""
     nx, ny, nz = w.nx, w.ny, w.nz
     px = (nx + 7) // 8 * 8
     P = px * ny * nz
@@ -113,11 +112,6 @@ def interior_tiles(w, V=4, block=256):
     if (P // V) % block:
         gen[-1] = True
     mat = np.asarray(w.mat).reshape(nz, ny, nx)
-    kk, jj = np.meshgrid(np.arange(nz), np.arange(ny), indexing="ij")
-    face = (jj == 0) | (jj == ny - 1) | (kk == 0) | (kk == nz - 1)
-    for k, j in zip(kk[face], jj[face]):
-        r0 = (k * ny + j) * px
-        gen[r0 // T:(r0 + px - 1) // T + 1] = True
 
     def node(i, j, k):
         return (k * ny + j) * px + i
