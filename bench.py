@@ -344,9 +344,11 @@ def run_batched(args):
     seq = sequential_solves(ws)
     t0 = time.perf_counter()
     solvers = [build_solver(w) for w in ws]
+    tb = time.perf_counter()
     b = Batch()
     for s in solvers:
         b.attach(s)
+    ta = time.perf_counter()
     tuning = b.autotune(trial_windows=2) if args.autotune else b.get_tuning()
     t1 = time.perf_counter()
     ext = torch.cuda.ExternalStream(b.stream())
@@ -378,7 +380,8 @@ def run_batched(args):
                                  "p99_s": float(np.percentile(seq, 99))},
         "speedup_vs_sequential": sum(seq) / batched_s,
         "batched_gpu": {"node_updates_per_s": work / (gpu_ms / 1e3), "seconds": gpu_ms / 1e3,
-                        "setup_s": t1 - t0, "readback_s": t2 - t1 - gpu_ms / 1e3,
+                        "setup_s": t1 - t0, "setup_build_s": tb - t0, "setup_attach_s": ta - tb,
+                        "readback_s": t2 - t1 - gpu_ms / 1e3,
                         "hbm_frac": bytes_all / (gpu_ms / 1e3) / 1e9 / peak, "peak_kind": kind},
     }
     print(json.dumps(line), flush=True)
