@@ -41,7 +41,8 @@ class ConfigC(C.Structure):
                 ("settle_steps", C.c_int), ("boundary_rho", C.c_float), ("huy_offset", C.c_int),
                 ("use_gpu", C.c_int), ("record_every", C.c_int), ("storage", C.c_int),
                 ("pulse_scale", C.c_float), ("steps_per_launch", C.c_int),
-                ("kernel_variant", C.c_int), ("rounding", C.c_int), ("general_tiles", C.c_int)]
+                ("kernel_variant", C.c_int), ("rounding", C.c_int), ("general_tiles", C.c_int),
+                ("surface_monitors", C.c_int)]
 
 
 class BatchTuningC(C.Structure):
@@ -124,6 +125,22 @@ SIGNATURES = {
     "tlm_waveform_value": (_st, [C.c_int, C.c_float, C.c_float, C.c_int, _P(C.c_float)]),
     "tlm_scatter_unitarity_error": (_st, [C.c_int, _P(C.c_float)]),
     "tlm_stub_unitarity_error": (_st, [C.c_int, C.c_float, _P(C.c_float)]),
+    "tlm_get_surface_faces": (_st, [_h, _P(C.c_uint64), _P(C.c_int), _P(C.c_int), _P(C.c_float), C.c_int,
+                                    _P(C.c_int)]),
+    "tlm_get_js_instant": (_st, [_h, _P(C.c_float), C.c_int, _P(C.c_int)]),
+    "tlm_get_js_dft": (_st, [_h, _P(C.c_float), _P(C.c_float), _P(C.c_float), C.c_int, _P(C.c_int),
+                             _P(C.c_int)]),
+    "tlm_get_huygens_faces": (_st, [_h, _P(C.c_uint64), _P(C.c_int), _P(C.c_int), _P(C.c_float), C.c_int,
+                                    _P(C.c_int)]),
+    "tlm_get_huygens_dft": (_st, [_h, _P(C.c_float), C.c_int, _P(C.c_int), _P(C.c_int)]),
+    "tlm_set_field_plane": (_st, [_h, C.c_int, C.c_int]),
+    "tlm_get_field_plane": (_st, [_h, _P(C.c_float), C.c_size_t, _P(C.c_int), _P(C.c_int), _P(C.c_int),
+                                  _P(C.c_int)]),
+    "tlm_frame_count": (_st, [_h, _P(C.c_int)]),
+    "tlm_get_frame": (_st, [_h, C.c_int, _P(C.c_int), _P(C.c_float), C.c_int, _P(C.c_float), C.c_size_t,
+                            _P(C.c_int), _P(C.c_int), _P(C.c_int), _P(C.c_int)]),
+    "tlm_compute_far_field": (_st, [_h, C.c_int, C.c_int, _P(C.c_float), _P(C.c_float), _P(C.c_float),
+                                    _P(C.c_float), _P(C.c_float)]),
     "tlm_step_planes_noalloc": (_st, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
                                       C.c_void_p, C.c_void_p]),

@@ -77,6 +77,21 @@ void tables_f64(const float *epsr, const float *sigma, int n, float dl, double *
 }
 
 // Probe scale -1/dl (TlmSolver.cpp:709).
+// Phase of the surface-monitor DFT at step n (TlmSolver.cpp:619-620):
+// 2 pi f0 (n dt), then its cosine and sine.
+void dft_phase_f32(float f0, float dt, int n, float *c, float *s)
+{
+    const float phase = 2.0f * (float)kPiD * f0 * ((float)n * dt);
+    *c = std::cos(phase);
+    *s = std::sin(phase);
+}
+void dft_phase_f64(float f0, double dt, int n, double *c, double *s)
+{
+    const double phase = 2.0 * kPiD * (double)f0 * ((double)n * dt);
+    *c = std::cos(phase);
+    *s = std::sin(phase);
+}
+
 float probe_scale_f32(float dl) { return -1.0f / dl; }
 double probe_scale_f64(float dl) { return -1.0 / (double)dl; }
 

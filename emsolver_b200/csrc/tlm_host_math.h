@@ -12,6 +12,8 @@ void tables_f32(const float *epsr, const float *sigma, int n, float dl, float *y
 void tables_f64(const float *epsr, const float *sigma, int n, float dl, double *yhat,
                 double *ghat);
 float probe_scale_f32(float dl);
+void dft_phase_f32(float f0, float dt, int n, float *c, float *s);
+void dft_phase_f64(float f0, double dt, int n, double *c, double *s);
 double probe_scale_f64(float dl);
 void cell_of(const float origin[3], float dl, float x, float y, float z, int *i, int *j, int *k);
 } // namespace tlmh

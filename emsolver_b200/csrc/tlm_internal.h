@@ -150,6 +150,39 @@ inline Shape shapeOf(int storage, int variant)
 
 } // namespace tlmi
 
+namespace tlmi {
+// Surface monitors of one handle (TlmSolver.cpp:303-348, 616-675, 715-763):
+// PEC-face surface currents, Huygens-box phasors, |E| cut plane, frames.
+struct SurfaceState
+{
+    // face lists in the reference's order (reference linear cell indices)
+    std::vector<uint64_t> jsCell;
+    std::vector<int> jsAxis, jsSign;
+    std::vector<float> jsCenter;  // 3 per face
+    std::vector<uint64_t> huyCell;
+    std::vector<int> huyAxis, huySign;
+    std::vector<float> huyPos;  // 3 per face, relative to the domain centre
+    // device copies and accumulators (element type: the storage's real type)
+    long long *dJsNode = nullptr, *dHuyNode = nullptr;  // node * 8 + axis * 2 + (sign < 0)
+    void *dJsInst = nullptr, *dJsAcc = nullptr, *dHuyAcc = nullptr;
+    // cut plane (set by tlm_set_field_plane)
+    int planeAxis = -1, planeIndex = 0;
+    int planeN1 = 0, planeN2 = 0, planeAxisDone = -1, planeIndexDone = 0;
+    bool planeValid = false;
+    void *dPlane = nullptr;
+    size_t planeCap = 0;  // elements
+    // playback frames
+    struct Frame
+    {
+        int step, hasPlane, axis, index, n1, n2;
+        size_t off;  // element offset in dFrames
+    };
+    std::vector<Frame> frames;
+    void *dFrames = nullptr;
+    size_t framesCap = 0, framesUsed = 0;  // elements
+};
+} // namespace tlmi
+
 struct tlm_solver
 {
     int device = 0;
@@ -190,6 +223,7 @@ struct tlm_solver
     std::vector<double> dftFreqs;
     bool prepared = false;
     int nsamp = 0;
+    int specCount = 0;     // entries of dSpec
 
     // time-loop state
     int curStep = 0;       // steps enqueued
@@ -221,6 +255,9 @@ struct tlm_solver
     struct tlm_batch_s *batch = nullptr;
     void *dSv = nullptr;
     long long svCount = 0;
+
+    // surface monitors
+    tlmi::SurfaceState surf;
 
     // kernel timing
     bool timing = false;
@@ -309,6 +346,13 @@ tlm_status uploadSourceTable(tlm_solver *h, long long steps);
 tlm_status setWindow(tlm_solver *h, int window);
 tlm_status rewind(tlm_solver *h);
 tlm_status reshape(tlm_solver *h, int variant);
+// Surface monitors (defined in tlm_surface.cu).
+void buildSurfaceLists(tlm_solver *h);
+tlm_status prepareSurface(tlm_solver *h);
+void freeSurface(tlm_solver *h);
+tlm_status rewindSurface(tlm_solver *h);
+bool surfaceActive(const tlm_solver *h);
+tlm_status launchSurface(tlm_solver *h, int n);
 // The library's memory pool on a device (created on first use) and the
 // bytes it could hand out: free device memory plus blocks it keeps for reuse.
 cudaMemPool_t devicePool(int device);

@@ -429,6 +429,9 @@ tlm_status tlm_server_submit(tlm_server s, const tlm_request *q, uint64_t *id)
         return serverFail(TLM_EINVAL, "material map does not match the grid");
     if (q->n_ports < 0 || q->n_probes < 0 || q->n_freq < 0 || q->n_table < 0 || q->n_source < 0)
         return serverFail(TLM_EINVAL, "negative count");
+    if (q->cfg.surface_monitors || q->cfg.record_every)
+        return serverFail(TLM_EINVAL, "served requests record ports and probes only "
+                                      "(surface_monitors = 0, record_every = 0)");
     auto r = std::make_shared<Request>();
     r->grid = q->grid;
     r->mat.assign(q->mat, q->mat + q->n_cells);

@@ -57,6 +57,7 @@ namespace tlmi {
 
 void freeMonitors(tlm_solver *h)
 {
+    freeSurface(h);
     devFree(h, h->dSpec);
     devFree(h, h->dTile);
     devFree(h, h->dTileFlags);
@@ -208,6 +209,7 @@ tlm_status prepare(tlm_solver *h)
         TLM_CU(h, cudaMemcpyAsync(h->dTileFlags, flags.data(), flags.size(), cudaMemcpyHostToDevice,
                                   h->stream));
     }
+    h->specCount = (int)ents.size();
     if (!ents.empty())
     {
         TLM_TRY(devAlloc(h, &h->dSpec, ents.size() * sizeof(SpecEntry)));
@@ -270,6 +272,7 @@ tlm_status prepare(tlm_solver *h)
         TLM_TRY(devAlloc(h, &h->dDft, (size_t)np * nf * 4 * sizeof(double)));
         TLM_CU(h, cudaMemsetAsync(h->dDft, 0, (size_t)np * nf * 4 * sizeof(double), h->stream));
     }
+    TLM_TRY(prepareSurface(h));
     h->prepared = true;
     return TLM_OK;
 }
@@ -370,6 +373,7 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
     }
     a.round_seed = tlmk::mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
     a.stochastic = h->cfg.rounding == 1 ? 1 : 0;
+    if (surfaceActive(h)) TLM_TRY(launchSurface(h, n));  // reads the same input buffer, first
     launchShaped<S>(a, h->variant, h->stateIncident, h->nblocks, h->stream);
     TLM_CU(h, cudaGetLastError());
     if (h->timing) TLM_CU(h, cudaEventRecord(e1, h->stream));
@@ -564,6 +568,7 @@ tlm_status rewind(tlm_solver *h)
         TLM_CU(h, cudaMemsetAsync(h->dDft, 0,
                                   h->ports.size() * h->dftFreqs.size() * 4 * sizeof(double), h->stream));
     TLM_CU(h, cudaMemsetAsync(h->dElatest, 0, sizeof(double), h->stream));
+    TLM_TRY(rewindSurface(h));
     TLM_CU(h, cudaStreamSynchronize(h->stream));
     h->curStep = 0;
     h->curBuf = 0;
@@ -731,6 +736,7 @@ void tlm_config_default(tlm_config *c)
     c->kernel_variant = 0;
     c->rounding = 0;
     c->general_tiles = 0;
+    c->surface_monitors = 0;
 }
 
 int tlm_kernel_variants(int storage) { return shapeCount(storage); }
@@ -865,6 +871,10 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     if (cfg->rounding < 0 || cfg->rounding > 1) return h->fail(TLM_EINVAL, "rounding must be 0 or 1");
     if (cfg->general_tiles < 0 || cfg->general_tiles > 1)
         return h->fail(TLM_EINVAL, "general_tiles must be 0 or 1");
+    if (cfg->surface_monitors < 0 || cfg->surface_monitors > 1)
+        return h->fail(TLM_EINVAL, "surface_monitors must be 0 or 1");
+    if (cfg->record_every < 0 || cfg->huy_offset < 0)
+        return h->fail(TLM_EINVAL, "record_every and huy_offset must be >= 0");
     if (!std::isfinite(cfg->boundary_rho)) return h->fail(TLM_EINVAL, "boundary_rho not finite");
     bool anyDiel = false;
     for (long long c = 0; c < n; ++c)
@@ -932,6 +942,9 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     h->stopFlag.store(false);
     h->evUsed = 0;
     h->scale = 1.0f;
+    h->surf.planeAxis = -1;
+    h->surf.planeIndex = 0;
+    buildSurfaceLists(h);
 
     // HBM admission: refuse up front if the state would not fit.
     const size_t sb = storageBytes(h->storage), rb = realBytes(h->storage);

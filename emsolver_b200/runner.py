@@ -11,7 +11,9 @@ def build_solver(w, device: int = 0, storage: int | None = None, steps_per_launc
     setup, ports (in order), plane wave, probes at cell centres, port DFT."""
     s = TlmSolver(device, variant)
     grid = VoxelGridSpec(w.nx, w.ny, w.nz, tuple(w.origin), w.dl)
-    cfg = TlmConfig(f0=w.f0, waveform=w.waveform, totalSteps=w.steps, settleSteps=0,
+    cfg = TlmConfig(f0=w.f0, waveform=w.waveform, totalSteps=w.steps, settleSteps=w.meta.get("settle_steps", 0),
+                    huyOffset=w.meta.get("huy_offset", 0), recordEvery=w.meta.get("record_every", 0),
+                    surfaceMonitors=bool(w.meta.get("surface_monitors", False)),
                     boundaryRho=w.rho, storage=w.storage if storage is None else storage,
                     stepsPerLaunch=steps_per_launch, pulseScale=pulse_scale,
                     kernelVariant=kernel_variant, rounding=rounding, generalTiles=general_tiles)
@@ -26,6 +28,8 @@ def build_solver(w, device: int = 0, storage: int | None = None, steps_per_launc
         s.addProbe(w.cell_center(i, j, k))
     if w.dft_freqs is not None:
         s.setPortDft(w.dft_freqs)
+    if "field_plane" in w.meta:
+        s.setFieldPlane(*w.meta["field_plane"])
     return s
 
 

@@ -91,6 +91,7 @@ class TlmConfig:
     kernelVariant: int = 0
     rounding: int = 0          # 16-bit storage: 0 nearest, 1 stochastic
     generalTiles: bool = False  # True: no interior-tile fast path (cross-checks)
+    surfaceMonitors: bool = False  # PEC-surface Js and Huygens-box DFT monitors
 
     def to_c(self):
         c = _lib.ConfigC()
@@ -108,6 +109,7 @@ class TlmConfig:
         c.kernel_variant = int(self.kernelVariant)
         c.rounding = int(self.rounding)
         c.general_tiles = 1 if self.generalTiles else 0
+        c.surface_monitors = 1 if self.surfaceMonitors else 0
         return c
 
 
@@ -361,6 +363,103 @@ class TlmSolver:
     def setPulses(self, v):
         a = np.ascontiguousarray(v, dtype=np.float32).reshape(-1)
         self._c(self._L.tlm_set_pulses(self._h, _fp(a, C.c_float), a.size))
+
+    # ---- surface monitors (TlmSolver.h:237-245), cut plane, frames, far field
+    def faces(self):
+        """PEC-surface faces (TlmSolver::faces): cells, axis, sign, centre [n, 3]."""
+        n = C.c_int(0)
+        self._c(self._L.tlm_get_surface_faces(self._h, None, None, None, None, 0, C.byref(n)))
+        m = max(n.value, 1)
+        cells, axis, sign = np.zeros(m, np.uint64), np.zeros(m, np.int32), np.zeros(m, np.int32)
+        center = np.zeros((m, 3), np.float32)
+        self._c(self._L.tlm_get_surface_faces(self._h, _fp(cells, C.c_uint64), _fp(axis, C.c_int),
+                                              _fp(sign, C.c_int), _fp(center, C.c_float), n.value,
+                                              C.byref(n)))
+        k = n.value
+        return {"cells": cells[:k], "axis": axis[:k], "sign": sign[:k], "center": center[:k]}
+
+    def getJsInstant(self):
+        n = C.c_int(0)
+        self._c(self._L.tlm_get_js_instant(self._h, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float32)
+        self._c(self._L.tlm_get_js_instant(self._h, _fp(out, C.c_float), n.value, C.byref(n)))
+        return out[:n.value]
+
+    def getJsDft(self, raw: bool = False):
+        """|Js| DFT magnitude per face (getJsDft after finalizeDft); with
+        raw=True also (re [n, 2], im [n, 2], samples)."""
+        n, ns = C.c_int(0), C.c_int(0)
+        self._c(self._L.tlm_get_js_dft(self._h, None, None, None, 0, C.byref(n), C.byref(ns)))
+        m = max(n.value, 1)
+        mag, re, im = np.zeros(m, np.float32), np.zeros(2 * m, np.float32), np.zeros(2 * m, np.float32)
+        self._c(self._L.tlm_get_js_dft(self._h, _fp(mag, C.c_float), _fp(re, C.c_float), _fp(im, C.c_float),
+                                       n.value, C.byref(n), C.byref(ns)))
+        k = n.value
+        if raw:
+            return mag[:k], re[:2 * k].reshape(k, 2), im[:2 * k].reshape(k, 2), ns.value
+        return mag[:k]
+
+    def huygensFaces(self):
+        n = C.c_int(0)
+        self._c(self._L.tlm_get_huygens_faces(self._h, None, None, None, None, 0, C.byref(n)))
+        m = max(n.value, 1)
+        cells, axis, sign = np.zeros(m, np.uint64), np.zeros(m, np.int32), np.zeros(m, np.int32)
+        pos = np.zeros((m, 3), np.float32)
+        self._c(self._L.tlm_get_huygens_faces(self._h, _fp(cells, C.c_uint64), _fp(axis, C.c_int),
+                                              _fp(sign, C.c_int), _fp(pos, C.c_float), n.value, C.byref(n)))
+        k = n.value
+        return {"cells": cells[:k], "axis": axis[:k], "out_sign": sign[:k], "pos": pos[:k]}
+
+    def huygensDft(self):
+        """(accumulators [n, 8], samples)."""
+        n, ns = C.c_int(0), C.c_int(0)
+        self._c(self._L.tlm_get_huygens_dft(self._h, None, 0, C.byref(n), C.byref(ns)))
+        acc = np.zeros(max(n.value, 1) * 8, np.float32)
+        self._c(self._L.tlm_get_huygens_dft(self._h, _fp(acc, C.c_float), n.value, C.byref(n), C.byref(ns)))
+        return acc[:8 * n.value].reshape(n.value, 8), ns.value
+
+    def setFieldPlane(self, axis: int, index: int):
+        self._c(self._L.tlm_set_field_plane(self._h, int(axis), int(index)))
+
+    def getFieldPlane(self):
+        """(plane [n2, n1], axis, index), or None before a plane exists."""
+        ax, idx, n1, n2 = (C.c_int(0) for _ in range(4))
+        st = self._L.tlm_get_field_plane(self._h, None, 0, C.byref(ax), C.byref(idx), C.byref(n1), C.byref(n2))
+        if st != 0:
+            return None
+        out = np.zeros(n1.value * n2.value, np.float32)
+        self._c(self._L.tlm_get_field_plane(self._h, _fp(out, C.c_float), out.size, C.byref(ax), C.byref(idx),
+                                            C.byref(n1), C.byref(n2)))
+        return out.reshape(n2.value, n1.value), ax.value, idx.value
+
+    def frameCount(self):
+        n = C.c_int(0)
+        self._c(self._L.tlm_frame_count(self._h, C.byref(n)))
+        return n.value
+
+    def getFrame(self, idx: int):
+        nj = C.c_int(0)
+        self._c(self._L.tlm_get_js_instant(self._h, None, 0, C.byref(nj)))
+        dims = sorted((self._grid.nx * self._grid.ny, self._grid.nx * self._grid.nz, self._grid.ny * self._grid.nz))
+        js = np.zeros(max(nj.value, 1), np.float32)
+        plane = np.zeros(dims[-1], np.float32)
+        st, ax, pi, n1, n2 = (C.c_int(0) for _ in range(5))
+        self._c(self._L.tlm_get_frame(self._h, int(idx), C.byref(st), _fp(js, C.c_float), nj.value,
+                                      _fp(plane, C.c_float), plane.size, C.byref(ax), C.byref(pi), C.byref(n1),
+                                      C.byref(n2)))
+        npl = n1.value * n2.value
+        return {"step": st.value, "js": js[:nj.value],
+                "plane": plane[:npl].reshape(n2.value, n1.value) if npl else None,
+                "axis": ax.value, "index": pi.value}
+
+    def computeFarField(self, nTheta: int = 37, nPhi: int = 73):
+        """FarFieldData (TlmSolver.h:103-110) as a dict."""
+        U = np.zeros(nTheta * nPhi, np.float32)
+        um, d, pt, pp = (C.c_float(0) for _ in range(4))
+        self._c(self._L.tlm_compute_far_field(self._h, int(nTheta), int(nPhi), _fp(U, C.c_float), C.byref(um),
+                                              C.byref(d), C.byref(pt), C.byref(pp)))
+        return {"U": U.reshape(nTheta, nPhi), "uMax": um.value, "directivity": d.value,
+                "peakThetaDeg": pt.value, "peakPhiDeg": pp.value}
 
     def stubs(self):
         n = self._grid.ncells * 3

@@ -98,11 +98,12 @@ typedef struct tlm_config {
     float f0;            /* excitation / analysis frequency (Hz) */
     int waveform;        /* tlm_waveform */
     int total_steps;     /* tlm_run stops here */
-    int settle_steps;    /* kept for interface parity (Js DFT start) */
+    int settle_steps;    /* the Js and Huygens DFTs start at this step */
     float boundary_rho;  /* outer-face reflection coefficient */
-    int huy_offset;      /* Huygens box inset; accepted, not yet used */
+    int huy_offset;      /* Huygens box inset in cells (>= 2 enables the box;
+                            needs surface_monitors) */
     int use_gpu;         /* ignored: this library always runs on the GPU */
-    int record_every;    /* accepted, playback frames not yet produced */
+    int record_every;    /* record a playback frame every N steps (0 = off) */
     /* --- extensions --- */
     int storage;         /* tlm_storage */
     float pulse_scale;   /* BF16/F16 per-grid scale (0 = choose from sources) */
@@ -113,6 +114,11 @@ typedef struct tlm_config {
     int general_tiles;   /* 1: every tile runs the general step body (no
                             interior-tile fast path); results are identical,
                             the switch exists to cross-check the two bodies */
+    int surface_monitors;/* 1: record the reference's PEC-surface currents
+                            (|Js| per face and its DFT at f0) and, with
+                            huy_offset >= 2, the Huygens-box phasors that the
+                            far field needs. One extra small launch per step;
+                            not available for handles driven by a batch */
 } tlm_config;
 
 typedef struct tlm_solver *tlm_handle;
@@ -381,6 +387,53 @@ TLM_API tlm_status tlm_server_release(tlm_server s, uint64_t id);
 TLM_API tlm_status tlm_server_stats(tlm_server s, tlm_server_stats_t *out);
 /* Device bytes a request holds while it runs (what admission counts). */
 TLM_API tlm_status tlm_request_footprint(const tlm_request *req, size_t *bytes);
+
+/* ---- surface monitors, cut plane, frames, far field ----------------- */
+
+/* TlmSolver::faces() (TlmSolver.h:237; built by BuildPecSurfaceFaces,
+ * Geometry.cpp:402-436): faces between a PEC cell and a non-PEC neighbour, in
+ * the reference's order. Per face: the neighbour's linear cell index, the
+ * normal axis, the side (+1: the neighbour is on the + side) and the face
+ * centre (3 floats). Any output may be NULL; *n = face count. Empty unless
+ * tlm_config.surface_monitors = 1. */
+TLM_API tlm_status tlm_get_surface_faces(tlm_handle h, uint64_t *air_cells, int *axis, int *sign,
+                                         float *centers, int cap, int *n);
+/* getJsInstant (TlmSolver.cpp:926-930): |Js| per face at the last step. */
+TLM_API tlm_status tlm_get_js_instant(tlm_handle h, float *out, int cap, int *n);
+/* getJsDft after finalizeDft (TlmSolver.cpp:467-481, 950-957): per face
+ * 2/samples * |(Re1, Im1, Re2, Im2)| of the DFT at f0 over the steps from
+ * settle_steps on; re/im (2 per face) are the raw accumulators (jsDftRe/Im).
+ * Any output may be NULL. */
+TLM_API tlm_status tlm_get_js_dft(tlm_handle h, float *magnitude, float *re, float *im, int cap, int *n,
+                                  int *samples);
+/* The Huygens box (TlmSolver::buildHuygens, TlmSolver.cpp:310-348): air cells
+ * inset huy_offset cells, per face the cell, normal axis, outward sign and
+ * position relative to the domain centre (3 floats). */
+TLM_API tlm_status tlm_get_huygens_faces(tlm_handle h, uint64_t *cells, int *axis, int *out_sign, float *pos,
+                                         int cap, int *n);
+/* The Huygens phasors (huyDft, TlmSolver.cpp:652-675): 8 floats per face,
+ * E1 re/im, E2 re/im, eta0*H1 re/im, eta0*H2 re/im. */
+TLM_API tlm_status tlm_get_huygens_dft(tlm_handle h, float *acc8, int cap, int *n, int *samples);
+/* setFieldPlane (TlmSolver.cpp:961-966): |E| over the plane normal to axis
+ * (-1 = off) at index, computed every second step. Between steps only. */
+TLM_API tlm_status tlm_set_field_plane(tlm_handle h, int axis, int index);
+/* getFieldPlane (TlmSolver.cpp:969-982): n1 x n2 floats (n1 along the first
+ * remaining axis); TLM_ESTATE if no plane has been computed. */
+TLM_API tlm_status tlm_get_field_plane(tlm_handle h, float *out, size_t cap, int *axis, int *index, int *n1,
+                                       int *n2);
+/* frameCount / getFrame (TlmSolver.cpp:933-947): one frame every
+ * record_every steps with |Js| per face and the latest cut plane (if any). */
+TLM_API tlm_status tlm_frame_count(tlm_handle h, int *n);
+TLM_API tlm_status tlm_get_frame(tlm_handle h, int idx, int *step, float *js, int js_cap, float *plane,
+                                 size_t plane_cap, int *axis, int *index, int *n1, int *n2);
+/* computeFarField (ComputeFarFieldFromHuygens, TlmSolver.cpp:805-916): the
+ * radiation intensity U over n_theta x n_phi directions (theta 0..pi, phi
+ * 0..2pi inclusive, U may be NULL), its maximum, the directivity and the
+ * peak direction, from the Huygens phasors at f0. Sums run in FP64 on the
+ * device, so U agrees with the reference's FP32 sums to their rounding, not
+ * bitwise. TLM_ESTATE without Huygens data. */
+TLM_API tlm_status tlm_compute_far_field(tlm_handle h, int n_theta, int n_phi, float *U, float *u_max,
+                                         float *directivity, float *peak_theta_deg, float *peak_phi_deg);
 
 /* ---- one step over caller-owned device memory, no allocation -------- */
 

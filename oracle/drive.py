@@ -9,10 +9,18 @@ from __future__ import annotations
 import numpy as np
 
 
-def setup(S, w, settle_steps=0):
+def setup(S, w, settle_steps=None):
+    """Settle steps, Huygens inset, frame period and cut plane come from
+    ``w.meta`` ("settle_steps", "huy_offset", "record_every", "field_plane")
+    when present."""
     wf = w.waveform if w.waveform != 3 else 2
+    if settle_steps is None:
+        settle_steps = w.meta.get("settle_steps", 0)
     S.setup(w.nx, w.ny, w.nz, w.mat, w.table, origin=w.origin, dl=w.dl, f0=w.f0, waveform=wf,
-            total_steps=w.steps, settle_steps=settle_steps, rho=w.rho)
+            total_steps=w.steps, settle_steps=settle_steps, rho=w.rho,
+            huy_offset=w.meta.get("huy_offset", 0), record_every=w.meta.get("record_every", 0))
+    if "field_plane" in w.meta:
+        S.set_field_plane(*w.meta["field_plane"])
     port_idx = [S.add_port(np.asarray(cells, np.uint64), pol, amp) for cells, pol, amp in w.ports]
     probe_idx = [S.add_probe(*w.cell_center(i, j, k)) for (i, j, k) in w.probes_cell]
     return port_idx, probe_idx

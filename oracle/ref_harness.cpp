@@ -55,6 +55,13 @@ public:
     static const std::vector<float> &ghat(const TlmSolver &s) { return s.ghat; }
     static int threads(const TlmSolver &s) { return s.pool->threadCount(); }
     static const std::vector<TlmPort> &ports(const TlmSolver &s) { return s.portList; }
+    static const std::vector<float> &jsDftRe(const TlmSolver &s) { return s.jsDftRe; }
+    static const std::vector<float> &jsDftIm(const TlmSolver &s) { return s.jsDftIm; }
+    static int dftSamples(const TlmSolver &s) { return s.dftSamples; }
+    static const std::vector<HuyFace> &huyFaces(const TlmSolver &s) { return s.huyFaces; }
+    static const std::vector<float> &huyDft(const TlmSolver &s) { return s.huyDft; }
+    static int huySamples(const TlmSolver &s) { return s.huySamples; }
+    static void finalizeDft(TlmSolver &s) { s.finalizeDft(); }
 
 private:
     // Soft source: q = 0.5*amp*sv onto the two link pulses of polarisation
@@ -82,10 +89,26 @@ extern "C" {
 void *ref_create(void) { return new TlmSolver(); }
 void ref_destroy(void *h) { delete static_cast<TlmSolver *>(h); }
 
+int ref_setup_ex(void *h, int nx, int ny, int nz, float ox, float oy, float oz,
+                 float dl, const uint8_t *mat, const float *epsr,
+                 const float *sigma, int ntab, float f0, int waveform,
+                 int totalSteps, int settleSteps, float rho, int huyOffset,
+                 int recordEvery);
+
 int ref_setup(void *h, int nx, int ny, int nz, float ox, float oy, float oz,
               float dl, const uint8_t *mat, const float *epsr,
               const float *sigma, int ntab, float f0, int waveform,
               int totalSteps, int settleSteps, float rho)
+{
+    return ref_setup_ex(h, nx, ny, nz, ox, oy, oz, dl, mat, epsr, sigma, ntab, f0,
+                        waveform, totalSteps, settleSteps, rho, 0, 0);
+}
+
+int ref_setup_ex(void *h, int nx, int ny, int nz, float ox, float oy, float oz,
+                 float dl, const uint8_t *mat, const float *epsr,
+                 const float *sigma, int ntab, float f0, int waveform,
+                 int totalSteps, int settleSteps, float rho, int huyOffset,
+                 int recordEvery)
 {
     TlmSolver *s = static_cast<TlmSolver *>(h);
     VoxelGridSpec g;
@@ -106,9 +129,9 @@ int ref_setup(void *h, int nx, int ny, int nz, float ox, float oy, float oz,
     cfg.totalSteps = totalSteps;
     cfg.settleSteps = settleSteps;
     cfg.boundaryRho = rho;
-    cfg.huyOffset = 0;
+    cfg.huyOffset = huyOffset;
     cfg.useGpu = false;
-    cfg.recordEvery = 0;
+    cfg.recordEvery = recordEvery;
     s->setup(g, std::move(m), std::move(tab), cfg);
     return 0;
 }
@@ -217,6 +240,103 @@ int ref_energy_history(void *h, int *steps, float *vals, int cap)
     int n = (int)st.size();
     for (int t = 0; t < n && t < cap; ++t) { steps[t] = st[t]; vals[t] = va[t]; }
     return n;
+}
+
+// ---- surface monitors: Js faces, Huygens box, cut plane, frames, far field
+int ref_surface_faces(void *h, uint64_t *cells, int *axis, int *sign, float *center, int cap)
+{
+    const auto &f = static_cast<TlmSolver *>(h)->faces();
+    for (int t = 0; t < (int)f.size() && t < cap; ++t)
+    {
+        if (cells) cells[t] = (uint64_t)f[t].airCell;
+        if (axis) axis[t] = f[t].axis;
+        if (sign) sign[t] = f[t].sign;
+        if (center) { center[3 * t] = f[t].center.x; center[3 * t + 1] = f[t].center.y; center[3 * t + 2] = f[t].center.z; }
+    }
+    return (int)f.size();
+}
+int ref_js_instant(void *h, float *out, int cap)
+{
+    std::vector<float> v;
+    static_cast<TlmSolver *>(h)->getJsInstant(v);
+    for (int t = 0; t < (int)v.size() && t < cap; ++t) out[t] = v[t];
+    return (int)v.size();
+}
+// Raw Js DFT accumulators, and the magnitudes of the reference's own
+// finalizeDft (which run() calls after the last step).
+int ref_js_dft(void *h, float *re, float *im, float *mag, int cap, int *samples)
+{
+    TlmSolver &s = *static_cast<TlmSolver *>(h);
+    const auto &r = GpuTlm::jsDftRe(s);
+    const auto &i = GpuTlm::jsDftIm(s);
+    for (int t = 0; t < (int)r.size() && t / 2 < cap; ++t) { if (re) re[t] = r[t]; if (im) im[t] = i[t]; }
+    if (mag)
+    {
+        GpuTlm::finalizeDft(s);
+        std::vector<float> m;
+        s.getJsDft(m);
+        for (int t = 0; t < (int)m.size() && t < cap; ++t) mag[t] = m[t];
+    }
+    if (samples) *samples = GpuTlm::dftSamples(s);
+    return (int)(r.size() / 2);
+}
+int ref_huygens_faces(void *h, uint64_t *cells, int *axis, int *outSign, float *pos, int cap)
+{
+    const auto &f = GpuTlm::huyFaces(*static_cast<TlmSolver *>(h));
+    for (int t = 0; t < (int)f.size() && t < cap; ++t)
+    {
+        if (cells) cells[t] = (uint64_t)f[t].cell;
+        if (axis) axis[t] = f[t].axis;
+        if (outSign) outSign[t] = f[t].outSign;
+        if (pos) { pos[3 * t] = f[t].pos.x; pos[3 * t + 1] = f[t].pos.y; pos[3 * t + 2] = f[t].pos.z; }
+    }
+    return (int)f.size();
+}
+int ref_huygens_dft(void *h, float *acc, int cap, int *samples)
+{
+    const TlmSolver &s = *static_cast<TlmSolver *>(h);
+    const auto &a = GpuTlm::huyDft(s);
+    for (int t = 0; t < (int)a.size() && t / 8 < cap; ++t) acc[t] = a[t];
+    if (samples) *samples = GpuTlm::huySamples(s);
+    return (int)(a.size() / 8);
+}
+void ref_set_field_plane(void *h, int axis, int index)
+{
+    static_cast<TlmSolver *>(h)->setFieldPlane(axis, index);
+}
+int ref_field_plane(void *h, float *out, size_t cap, int *axis, int *index, int *n1, int *n2)
+{
+    std::vector<float> v;
+    if (!static_cast<TlmSolver *>(h)->getFieldPlane(v, *axis, *index, *n1, *n2)) return -1;
+    for (size_t t = 0; t < v.size() && t < cap; ++t) out[t] = v[t];
+    return 0;
+}
+int ref_frame_count(void *h) { return static_cast<TlmSolver *>(h)->frameCount(); }
+int ref_get_frame(void *h, int idx, int *step, float *js, int jsCap, float *plane, size_t planeCap,
+                  int *axis, int *pidx, int *n1, int *n2)
+{
+    VizFrame fr;
+    if (!static_cast<TlmSolver *>(h)->getFrame(idx, fr)) return -1;
+    *step = fr.step;
+    for (int t = 0; t < (int)fr.js.size() && t < jsCap; ++t) js[t] = fr.js[t];
+    for (size_t t = 0; t < fr.plane.size() && t < planeCap; ++t) plane[t] = fr.plane[t];
+    *axis = fr.planeAxis;
+    *pidx = fr.planeIdx;
+    *n1 = fr.planeN1;
+    *n2 = fr.planeN2;
+    return (int)fr.plane.size();
+}
+int ref_far_field(void *h, int nTheta, int nPhi, float *U, float *uMax, float *directivity,
+                  float *peakTheta, float *peakPhi)
+{
+    FarFieldData d;
+    if (!static_cast<TlmSolver *>(h)->computeFarField(d, nTheta, nPhi)) return -1;
+    for (size_t t = 0; t < d.U.size(); ++t) U[t] = d.U[t];
+    *uMax = d.uMax;
+    *directivity = d.directivity;
+    *peakTheta = d.peakThetaDeg;
+    *peakPhi = d.peakPhiDeg;
+    return 0;
 }
 
 float ref_scatter_unitarity(void) { return TlmSolver::ScatterUnitarityError(); }

@@ -159,6 +159,20 @@ public:
     virtual int getPort(int idx, double *v, double *i, int cap) const = 0;
     virtual int energyHistory(int *steps, double *vals, int cap) const = 0;
     virtual double dt() const = 0;
+    // surface monitors (TlmSolver.cpp:303-348, 616-675, 715-763, 805-916)
+    virtual int configureSurface(int huyOffset, int recordEvery) = 0;
+    virtual void setFieldPlane(int axis, int index) = 0;
+    virtual int surfaceFaces(uint64_t *cells, int *axis, int *sign, float *center, int cap) const = 0;
+    virtual int jsInstant(double *out, int cap) const = 0;
+    virtual int jsDft(double *re, double *im, double *mag, int cap, int *samples) const = 0;
+    virtual int huygensFaces(uint64_t *cells, int *axis, int *outSign, float *pos, int cap) const = 0;
+    virtual int huygensDft(double *acc, int cap, int *samples) const = 0;
+    virtual int fieldPlane(double *out, size_t cap, int *axis, int *index, int *n1, int *n2) const = 0;
+    virtual int frameCount() const = 0;
+    virtual int getFrame(int idx, int *step, double *js, int jsCap, double *plane, size_t planeCap,
+                         int *axis, int *pidx, int *n1, int *n2) const = 0;
+    virtual int farField(int nTheta, int nPhi, double *U, double *uMax, double *directivity,
+                         double *peakTheta, double *peakPhi) const = 0;
 };
 
 template <class T> class Oracle : public OracleBase
@@ -206,7 +220,28 @@ public:
         sources.clear();
         energySteps.clear();
         energyVals.clear();
+        huyOffset = 0;
+        recordEvery = 0;
+        planeAxis = -1;
+        planeIndex = 0;
+        buildSurfaceFaces();
+        buildHuygens();
         return 0;
+    }
+
+    // Huygens box inset and playback-frame period (TlmConfig::huyOffset,
+    // recordEvery, TlmSolver.h:120-122); rebuilds the Huygens face list.
+    int configureSurface(int huyOffset_, int recordEvery_) override
+    {
+        huyOffset = huyOffset_;
+        recordEvery = recordEvery_;
+        buildHuygens();
+        return 0;
+    }
+    void setFieldPlane(int axis, int index) override
+    {
+        planeAxis = axis;
+        planeIndex = index;
     }
 
     // Lumped port (TlmSolver.cpp:362-374): cells that are out of range or not
@@ -423,7 +458,402 @@ public:
     }
     double dt() const override { return (double)timeStep; }
 
+    int surfaceFaces(uint64_t *cells, int *axis, int *sign, float *center, int cap) const override
+    {
+        for (int f = 0; f < (int)surf.size() && f < cap; ++f)
+        {
+            if (cells) cells[f] = surf[f].airCell;
+            if (axis) axis[f] = surf[f].axis;
+            if (sign) sign[f] = surf[f].sign;
+            if (center)
+                for (int a = 0; a < 3; ++a) center[f * 3 + a] = surf[f].center[a];
+        }
+        return (int)surf.size();
+    }
+    int jsInstant(double *out, int cap) const override
+    {
+        for (int f = 0; f < (int)jsInst.size() && f < cap; ++f) out[f] = (double)jsInst[f];
+        return (int)jsInst.size();
+    }
+    // Raw accumulators and the magnitude finalizeDft would produce
+    // (TlmSolver.cpp:467-481): 2/dftSamples * |(Re1, Im1, Re2, Im2)|.
+    int jsDft(double *re, double *im, double *mag, int cap, int *samples) const override
+    {
+        const int nf = (int)surf.size();
+        for (int f = 0; f < nf && f < cap; ++f)
+        {
+            if (re) { re[2 * f] = (double)jsRe[2 * f]; re[2 * f + 1] = (double)jsRe[2 * f + 1]; }
+            if (im) { im[2 * f] = (double)jsIm[2 * f]; im[2 * f + 1] = (double)jsIm[2 * f + 1]; }
+            if (mag)
+            {
+                T m = T(0);
+                if (dftSamples > 0)
+                {
+                    T norm = T(2) / T(dftSamples);
+                    T r1 = jsRe[2 * f], i1 = jsIm[2 * f], r2 = jsRe[2 * f + 1], i2 = jsIm[2 * f + 1];
+                    m = norm * std::sqrt(r1 * r1 + i1 * i1 + r2 * r2 + i2 * i2);
+                }
+                mag[f] = (double)m;
+            }
+        }
+        if (samples) *samples = dftSamples;
+        return nf;
+    }
+    int huygensFaces(uint64_t *cells, int *axis, int *outSign, float *pos, int cap) const override
+    {
+        for (int f = 0; f < (int)huy.size() && f < cap; ++f)
+        {
+            if (cells) cells[f] = huy[f].cell;
+            if (axis) axis[f] = huy[f].axis;
+            if (outSign) outSign[f] = huy[f].outSign;
+            if (pos)
+                for (int a = 0; a < 3; ++a) pos[f * 3 + a] = huy[f].pos[a];
+        }
+        return (int)huy.size();
+    }
+    int huygensDft(double *acc, int cap, int *samples) const override
+    {
+        for (size_t t = 0; t < huyAcc.size() && (int)(t / 8) < cap; ++t) acc[t] = (double)huyAcc[t];
+        if (samples) *samples = huySamples;
+        return (int)huy.size();
+    }
+    int fieldPlane(double *out, size_t cap, int *axis, int *index, int *n1, int *n2) const override
+    {
+        if (planeAxis < 0 || planeBuf.empty()) return -1;
+        for (size_t t = 0; t < planeBuf.size() && t < cap; ++t) out[t] = (double)planeBuf[t];
+        *axis = planeAxis;
+        *index = planeIndex;
+        *n1 = planeN1;
+        *n2 = planeN2;
+        return 0;
+    }
+    int frameCount() const override { return (int)frames.size(); }
+    int getFrame(int idx, int *step, double *js, int jsCap, double *plane, size_t planeCap, int *axis,
+                 int *pidx, int *n1, int *n2) const override
+    {
+        if (idx < 0 || idx >= (int)frames.size()) return -1;
+        const Frame &fr = frames[idx];
+        *step = fr.step;
+        for (int f = 0; f < (int)fr.js.size() && f < jsCap; ++f) js[f] = (double)fr.js[f];
+        for (size_t t = 0; t < fr.plane.size() && t < planeCap; ++t) plane[t] = (double)fr.plane[t];
+        *axis = fr.axis;
+        *pidx = fr.idx;
+        *n1 = fr.n1;
+        *n2 = fr.n2;
+        return (int)fr.plane.size();
+    }
+
+    // Near-to-far-field transform of the Huygens phasors at f0
+    // (ComputeFarFieldFromHuygens, TlmSolver.cpp:805-916): equivalent
+    // currents J' = n x (eta0 H), M = -(n x E) per face, radiation vectors
+    // summed face by face with e^{+j k0 r.pos}, U = |L_phi + N_theta|^2 +
+    // |L_theta - N_phi|^2 over a theta/phi grid, directivity by the
+    // trapezoidal rule in FP64.
+    int farField(int nTheta, int nPhi, double *U, double *uMax, double *directivity,
+                 double *peakTheta, double *peakPhi) const override
+    {
+        if (huy.empty() || huySamples == 0 || nTheta < 2 || nPhi < 2) return -1;
+        const T pi = T(kPi);
+        const T k0 = T(2) * pi * T(f0) / T(kC0f);
+        const int nh = (int)huy.size();
+        struct Cur
+        {
+            T pos[3], jRe[3], jIm[3], mRe[3], mIm[3];
+        };
+        std::vector<Cur> fc(nh);
+        for (int f = 0; f < nh; ++f)
+        {
+            const T *a = &huyAcc[(size_t)f * 8];
+            const int ax = huy[f].axis;
+            const int t1 = firstTransverse(ax), t2 = secondTransverse(ax);
+            const T sa = (ax == 1) ? T(-1) : T(1);
+            const T sg = T(huy[f].outSign);
+            Cur &q = fc[f];
+            for (int c = 0; c < 3; ++c)
+            {
+                q.pos[c] = T(huy[f].pos[c]);
+                q.jRe[c] = q.jIm[c] = q.mRe[c] = q.mIm[c] = T(0);
+            }
+            q.jRe[t2] = sg * sa * a[4];
+            q.jIm[t2] = sg * sa * a[5];
+            q.jRe[t1] = -sg * sa * a[6];
+            q.jIm[t1] = -sg * sa * a[7];
+            q.mRe[t2] = -sg * sa * a[0];
+            q.mIm[t2] = -sg * sa * a[1];
+            q.mRe[t1] = sg * sa * a[2];
+            q.mIm[t1] = sg * sa * a[3];
+        }
+        std::vector<T> u((size_t)nTheta * nPhi);
+        for (int ti = 0; ti < nTheta; ++ti)
+        {
+            const T th = pi * T(ti) / T(nTheta - 1);
+            const T st = std::sin(th), ct = std::cos(th);
+            for (int pj = 0; pj < nPhi; ++pj)
+            {
+                const T ph = T(2) * pi * T(pj) / T(nPhi - 1);
+                const T cp = std::cos(ph), sp = std::sin(ph);
+                const T rh[3] = { st * cp, st * sp, ct };
+                const T th3[3] = { ct * cp, ct * sp, -st };
+                const T ph3[2] = { -sp, cp };
+                T NtR = 0, NtI = 0, NpR = 0, NpI = 0, LtR = 0, LtI = 0, LpR = 0, LpI = 0;
+                for (int f = 0; f < nh; ++f)
+                {
+                    const Cur &q = fc[f];
+                    const T pha = k0 * (rh[0] * q.pos[0] + rh[1] * q.pos[1] + rh[2] * q.pos[2]);
+                    const T c = std::cos(pha), sn = std::sin(pha);
+                    const T jtR = q.jRe[0] * th3[0] + q.jRe[1] * th3[1] + q.jRe[2] * th3[2];
+                    const T jtI = q.jIm[0] * th3[0] + q.jIm[1] * th3[1] + q.jIm[2] * th3[2];
+                    const T jpR = q.jRe[0] * ph3[0] + q.jRe[1] * ph3[1];
+                    const T jpI = q.jIm[0] * ph3[0] + q.jIm[1] * ph3[1];
+                    const T mtR = q.mRe[0] * th3[0] + q.mRe[1] * th3[1] + q.mRe[2] * th3[2];
+                    const T mtI = q.mIm[0] * th3[0] + q.mIm[1] * th3[1] + q.mIm[2] * th3[2];
+                    const T mpR = q.mRe[0] * ph3[0] + q.mRe[1] * ph3[1];
+                    const T mpI = q.mIm[0] * ph3[0] + q.mIm[1] * ph3[1];
+                    NtR += jtR * c - jtI * sn;
+                    NtI += jtR * sn + jtI * c;
+                    NpR += jpR * c - jpI * sn;
+                    NpI += jpR * sn + jpI * c;
+                    LtR += mtR * c - mtI * sn;
+                    LtI += mtR * sn + mtI * c;
+                    LpR += mpR * c - mpI * sn;
+                    LpI += mpR * sn + mpI * c;
+                }
+                const T aR = LpR + NtR, aI = LpI + NtI;
+                const T bR = LtR - NpR, bI = LtI - NpI;
+                u[(size_t)ti * nPhi + pj] = aR * aR + aI * aI + bR * bR + bI * bI;
+            }
+        }
+        T um = T(0);
+        int iMax = 0;
+        double prad = 0.0;
+        const T dTh = pi / T(nTheta - 1);
+        const T dPh = T(2) * pi / T(nPhi - 1);
+        for (int ti = 0; ti < nTheta; ++ti)
+        {
+            const T th = pi * T(ti) / T(nTheta - 1);
+            const T wTh = (ti == 0 || ti == nTheta - 1) ? T(0.5) : T(1);
+            for (int pj = 0; pj < nPhi; ++pj)
+            {
+                const T wPh = (pj == 0 || pj == nPhi - 1) ? T(0.5) : T(1);
+                const T v = u[(size_t)ti * nPhi + pj];
+                if (v > um)
+                {
+                    um = v;
+                    iMax = ti * nPhi + pj;
+                }
+                prad += (double)v * std::sin(th) * wTh * wPh * dTh * dPh;
+            }
+        }
+        for (size_t t = 0; t < u.size(); ++t) U[t] = (double)u[t];
+        *uMax = (double)um;
+        *directivity = prad > 0 ? (double)(T)(4.0 * kPi * (double)um / prad) : 0.0;
+        *peakTheta = (double)(T(180) * T(iMax / nPhi) / T(nTheta - 1));
+        *peakPhi = (double)(T(360) * T(iMax % nPhi) / T(nPhi - 1));
+        return 0;
+    }
+
 private:
+    struct SurfFace
+    {
+        size_t airCell;
+        int axis, sign;
+        float center[3];
+    };
+    struct HuyFaceO
+    {
+        size_t cell;
+        int axis, outSign;
+        float pos[3];
+    };
+    struct Frame
+    {
+        int step = 0;
+        std::vector<T> js, plane;
+        int axis = -1, idx = 0, n1 = 0, n2 = 0;
+    };
+
+    // Cell centre origin + (i + 0.5) dl per axis in float (Geometry.h:100-105).
+    void cellCenter(int i, int j, int k, float c[3]) const
+    {
+        c[0] = origin[0] + ((float)i + 0.5f) * dl;
+        c[1] = origin[1] + ((float)j + 0.5f) * dl;
+        c[2] = origin[2] + ((float)k + 0.5f) * dl;
+    }
+
+    // Faces between a PEC cell and a non-PEC neighbour, in the order of the
+    // reference's scan (Geometry.cpp:402-436): cells in linear order, then
+    // axis, then side -1 before +1.
+    void buildSurfaceFaces()
+    {
+        surf.clear();
+        const long long stride[3] = { 1, nx, (long long)nx * ny };
+        const int dims[3] = { nx, ny, nz };
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i)
+                {
+                    const size_t c = ((size_t)k * ny + j) * nx + i;
+                    if (mat[c] != kPec) continue;
+                    const int co[3] = { i, j, k };
+                    for (int a = 0; a < 3; ++a)
+                        for (int sd = -1; sd <= 1; sd += 2)
+                        {
+                            const int q = co[a] + sd;
+                            if (q < 0 || q >= dims[a]) continue;
+                            const size_t nb = c + (size_t)((long long)sd * stride[a]);
+                            if (mat[nb] == kPec) continue;
+                            SurfFace f;
+                            f.airCell = nb;
+                            f.axis = a;
+                            f.sign = sd;
+                            cellCenter(i, j, k, f.center);
+                            f.center[a] = f.center[a] + (float)sd * dl * 0.5f;
+                            surf.push_back(f);
+                        }
+                }
+        jsInst.assign(surf.size(), T(0));
+        jsRe.assign(surf.size() * 2, T(0));
+        jsIm.assign(surf.size() * 2, T(0));
+        dftSamples = 0;
+    }
+
+    // Huygens box faces, `huyOffset` cells inside the domain, air cells only,
+    // in the reference's order (TlmSolver.cpp:310-348): x faces over (k, j),
+    // then y faces over (k, i), then z faces over (j, i), low face first.
+    void buildHuygens()
+    {
+        huy.clear();
+        huyAcc.clear();
+        huySamples = 0;
+        const int o = huyOffset;
+        if (o < 2) return;
+        const int nn[3] = { nx, ny, nz };
+        if (2 * o + 2 >= nn[0] || 2 * o + 2 >= nn[1] || 2 * o + 2 >= nn[2]) return;
+        float dom[3];
+        const float half[3] = { ((float)nx * dl) * 0.5f, ((float)ny * dl) * 0.5f, ((float)nz * dl) * 0.5f };
+        for (int a = 0; a < 3; ++a) dom[a] = origin[a] + half[a];
+        auto add = [&](int i, int j, int k, int axis, int outSign) {
+            const size_t c = ((size_t)k * ny + j) * nx + i;
+            if (mat[c] != kAir) return;
+            HuyFaceO f;
+            f.cell = c;
+            f.axis = axis;
+            f.outSign = outSign;
+            float cc[3];
+            cellCenter(i, j, k, cc);
+            for (int a = 0; a < 3; ++a) f.pos[a] = cc[a] - dom[a];
+            huy.push_back(f);
+        };
+        const int x0 = o, x1 = nn[0] - 1 - o, y0 = o, y1 = nn[1] - 1 - o, z0 = o, z1 = nn[2] - 1 - o;
+        for (int k = z0; k <= z1; ++k)
+            for (int j = y0; j <= y1; ++j)
+            {
+                add(x0, j, k, 0, -1);
+                add(x1, j, k, 0, +1);
+            }
+        for (int k = z0; k <= z1; ++k)
+            for (int i = x0; i <= x1; ++i)
+            {
+                add(i, y0, k, 1, -1);
+                add(i, y1, k, 1, +1);
+            }
+        for (int j = y0; j <= y1; ++j)
+            for (int i = x0; i <= x1; ++i)
+            {
+                add(i, j, z0, 2, -1);
+                add(i, j, z1, 2, +1);
+            }
+        huyAcc.assign(huy.size() * 8, T(0));
+    }
+
+    // Surface monitors of one step on the incident pulses after injection
+    // (TlmSolver.cpp:616-675, 715-763).
+    void surfaceMonitors(int stepIndex)
+    {
+        const bool doDft = stepIndex >= settleSteps;
+        const T phase = T(2) * T(kPi) * T(f0) * (T(stepIndex) * timeStep);
+        const T cph = std::cos(phase), sph = std::sin(phase);
+        for (size_t f = 0; f < surf.size(); ++f)
+        {
+            const T *vp = &inc[surf[f].airCell * 12];
+            const int t1 = firstTransverse(surf[f].axis), t2 = secondTransverse(surf[f].axis);
+            const T h1 = circulation(vp, t1), h2 = circulation(vp, t2);
+            jsInst[f] = std::sqrt(h1 * h1 + h2 * h2);
+            if (doDft)
+            {
+                jsRe[f * 2] += h1 * cph;
+                jsIm[f * 2] -= h1 * sph;
+                jsRe[f * 2 + 1] += h2 * cph;
+                jsIm[f * 2 + 1] -= h2 * sph;
+            }
+        }
+        if (doDft) ++dftSamples;
+        if (doDft && !huy.empty())
+        {
+            for (size_t f = 0; f < huy.size(); ++f)
+            {
+                const T *vp = &inc[huy[f].cell * 12];
+                const int t1 = firstTransverse(huy[f].axis), t2 = secondTransverse(huy[f].axis);
+                const T e1 = -nodeVoltage(vp, t1), e2 = -nodeVoltage(vp, t2);
+                const T m1 = -circulation(vp, t1), m2 = -circulation(vp, t2);
+                T *acc = &huyAcc[f * 8];
+                acc[0] += e1 * cph;
+                acc[1] -= e1 * sph;
+                acc[2] += e2 * cph;
+                acc[3] -= e2 * sph;
+                acc[4] += m1 * cph;
+                acc[5] -= m1 * sph;
+                acc[6] += m2 * cph;
+                acc[7] -= m2 * sph;
+            }
+            ++huySamples;
+        }
+        // |E| cut plane every second step
+        if (planeAxis >= 0 && (stepIndex % 2) == 0)
+        {
+            const int nn[3] = { nx, ny, nz };
+            const int pa = planeAxis;
+            const int a1 = (pa == 0) ? 1 : 0, a2 = (pa == 2) ? 1 : 2;
+            planeN1 = nn[a1];
+            planeN2 = nn[a2];
+            planeBuf.assign((size_t)planeN1 * planeN2, T(0));
+            const int idx = std::min(std::max(planeIndex, 0), nn[pa] - 1);
+            for (int q2 = 0; q2 < planeN2; ++q2)
+                for (int q1 = 0; q1 < planeN1; ++q1)
+                {
+                    int co[3];
+                    co[pa] = idx;
+                    co[a1] = q1;
+                    co[a2] = q2;
+                    const size_t c = ((size_t)co[2] * ny + co[1]) * nx + co[0];
+                    if (mat[c] == kPec) continue;
+                    const T *vp = &inc[c * 12];
+                    T e2 = T(0);
+                    for (int j = 0; j < 3; ++j)
+                    {
+                        const T vj = nodeVoltage(vp, j);
+                        e2 += vj * vj;
+                    }
+                    planeBuf[(size_t)q2 * planeN1 + q1] = std::sqrt(e2);
+                }
+        }
+        if (recordEvery > 0 && (stepIndex % recordEvery) == 0)
+        {
+            Frame fr;
+            fr.step = stepIndex;
+            fr.js = jsInst;
+            if (planeAxis >= 0 && !planeBuf.empty())
+            {
+                fr.plane = planeBuf;
+                fr.axis = planeAxis;
+                fr.idx = planeIndex;
+                fr.n1 = planeN1;
+                fr.n2 = planeN2;
+            }
+            frames.push_back(std::move(fr));
+        }
+    }
+
     void inject(size_t c, int pol, float amp, T sv)
     {
         T q = T(0.5) * T(amp) * sv;
@@ -439,6 +869,7 @@ private:
     // Monitors (TlmSolver.cpp:677-713, 766-789).
     void sample(int stepIndex)
     {
+        surfaceMonitors(stepIndex);
         const long long stride[3] = { 1, nx, (long long)nx * ny };
         for (Port &p : ports)
         {
@@ -494,6 +925,13 @@ private:
     std::vector<Source> sources;
     std::vector<int> energySteps;
     std::vector<double> energyVals;
+    int huyOffset = 0, recordEvery = 0;
+    int planeAxis = -1, planeIndex = 0, planeN1 = 0, planeN2 = 0;
+    std::vector<SurfFace> surf;
+    std::vector<HuyFaceO> huy;
+    std::vector<T> jsInst, jsRe, jsIm, huyAcc, planeBuf;
+    int dftSamples = 0, huySamples = 0;
+    std::vector<Frame> frames;
 };
 
 // Unitarity known-answer tests (TlmSolver.cpp:116-169): build the scattering
@@ -611,6 +1049,51 @@ int orc_get_port(void *h, int idx, double *v, double *i, int cap)
 int orc_energy_history(void *h, int *steps, double *vals, int cap)
 {
     return static_cast<OracleBase *>(h)->energyHistory(steps, vals, cap);
+}
+int orc_configure_surface(void *h, int huy_offset, int record_every)
+{
+    return static_cast<OracleBase *>(h)->configureSurface(huy_offset, record_every);
+}
+void orc_set_field_plane(void *h, int axis, int index)
+{
+    static_cast<OracleBase *>(h)->setFieldPlane(axis, index);
+}
+int orc_surface_faces(void *h, uint64_t *cells, int *axis, int *sign, float *center, int cap)
+{
+    return static_cast<OracleBase *>(h)->surfaceFaces(cells, axis, sign, center, cap);
+}
+int orc_js_instant(void *h, double *out, int cap)
+{
+    return static_cast<OracleBase *>(h)->jsInstant(out, cap);
+}
+int orc_js_dft(void *h, double *re, double *im, double *mag, int cap, int *samples)
+{
+    return static_cast<OracleBase *>(h)->jsDft(re, im, mag, cap, samples);
+}
+int orc_huygens_faces(void *h, uint64_t *cells, int *axis, int *out_sign, float *pos, int cap)
+{
+    return static_cast<OracleBase *>(h)->huygensFaces(cells, axis, out_sign, pos, cap);
+}
+int orc_huygens_dft(void *h, double *acc, int cap, int *samples)
+{
+    return static_cast<OracleBase *>(h)->huygensDft(acc, cap, samples);
+}
+int orc_field_plane(void *h, double *out, size_t cap, int *axis, int *index, int *n1, int *n2)
+{
+    return static_cast<OracleBase *>(h)->fieldPlane(out, cap, axis, index, n1, n2);
+}
+int orc_frame_count(void *h) { return static_cast<OracleBase *>(h)->frameCount(); }
+int orc_get_frame(void *h, int idx, int *step, double *js, int js_cap, double *plane, size_t plane_cap,
+                  int *axis, int *pidx, int *n1, int *n2)
+{
+    return static_cast<OracleBase *>(h)->getFrame(idx, step, js, js_cap, plane, plane_cap, axis, pidx, n1,
+                                                  n2);
+}
+int orc_far_field(void *h, int n_theta, int n_phi, double *U, double *u_max, double *directivity,
+                  double *peak_theta, double *peak_phi)
+{
+    return static_cast<OracleBase *>(h)->farField(n_theta, n_phi, U, u_max, directivity, peak_theta,
+                                                  peak_phi);
 }
 double orc_scatter_unitarity(int fp64)
 {

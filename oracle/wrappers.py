@@ -45,10 +45,134 @@ def _setup_args(nx, ny, nz, origin, dl, mat, table):
     return mat, eps, sig, ox, oy, oz
 
 
-class Oracle:
+class _SurfaceMonitors:
+    """Js faces and DFT, Huygens-box DFT, |E| cut plane, playback frames and
+    the far field (TlmSolver.cpp:303-348, 616-675, 715-763, 805-916), shared by
+    ``Oracle`` and ``RefSolver``. Subclasses set ``_p`` (symbol prefix) and
+    ``_rt``/``_rp`` (the library's real type and its pointer type)."""
+
+    def _f(self, name):
+        return getattr(self.L, self._p + name)
+
+    def set_field_plane(self, axis, index):
+        self._f("set_field_plane")(self.h, axis, index)
+
+    def surface_faces(self):
+        n = self._f("surface_faces")(self.h, None, None, None, None, 0)
+        cells = np.empty(max(n, 1), np.uint64)
+        axis = np.empty(max(n, 1), np.int32)
+        sign = np.empty(max(n, 1), np.int32)
+        center = np.empty((max(n, 1), 3), np.float32)
+        self._f("surface_faces")(self.h, _ptr(cells, _u64p), _ptr(axis, _i32p), _ptr(sign, _i32p),
+                                 _ptr(center, _f32p), n)
+        return {"cells": cells[:n], "axis": axis[:n], "sign": sign[:n], "center": center[:n]}
+
+    def js_instant(self):
+        n = self._f("js_instant")(self.h, None, 0)
+        out = np.empty(max(n, 1), self._rt)
+        self._f("js_instant")(self.h, _ptr(out, self._rp), n)
+        return out[:n].astype(self.dtype)
+
+    def js_dft(self):
+        """(re [nf, 2], im [nf, 2], magnitude as finalised after a run [nf], samples)."""
+        n = self._f("js_dft")(self.h, None, None, None, 0, None)
+        re = np.empty(max(2 * n, 2), self._rt)
+        im = np.empty(max(2 * n, 2), self._rt)
+        mag = np.empty(max(n, 1), self._rt)
+        samples = C.c_int(0)
+        self._f("js_dft")(self.h, _ptr(re, self._rp), _ptr(im, self._rp), _ptr(mag, self._rp), n,
+                          C.byref(samples))
+        return (re[:2 * n].reshape(n, 2).astype(self.dtype), im[:2 * n].reshape(n, 2).astype(self.dtype),
+                mag[:n].astype(self.dtype), samples.value)
+
+    def huygens_faces(self):
+        n = self._f("huygens_faces")(self.h, None, None, None, None, 0)
+        cells = np.empty(max(n, 1), np.uint64)
+        axis = np.empty(max(n, 1), np.int32)
+        sign = np.empty(max(n, 1), np.int32)
+        pos = np.empty((max(n, 1), 3), np.float32)
+        self._f("huygens_faces")(self.h, _ptr(cells, _u64p), _ptr(axis, _i32p), _ptr(sign, _i32p),
+                                 _ptr(pos, _f32p), n)
+        return {"cells": cells[:n], "axis": axis[:n], "out_sign": sign[:n], "pos": pos[:n]}
+
+    def huygens_dft(self):
+        """(accumulators [nh, 8]: E1 re/im, E2 re/im, eta0*H1 re/im, eta0*H2 re/im; samples)."""
+        n = self._f("huygens_faces")(self.h, None, None, None, None, 0)
+        acc = np.empty(max(8 * n, 8), self._rt)
+        samples = C.c_int(0)
+        self._f("huygens_dft")(self.h, _ptr(acc, self._rp), n, C.byref(samples))
+        return acc[:8 * n].reshape(n, 8).astype(self.dtype), samples.value
+
+    def field_plane(self):
+        cap = 1 << 22
+        buf = np.empty(cap, self._rt)
+        ax, idx, n1, n2 = (C.c_int(0) for _ in range(4))
+        rc = self._f("field_plane")(self.h, _ptr(buf, self._rp), cap, C.byref(ax), C.byref(idx),
+                                    C.byref(n1), C.byref(n2))
+        if rc != 0:
+            return None
+        return buf[:n1.value * n2.value].reshape(n2.value, n1.value).astype(self.dtype), ax.value, idx.value
+
+    def frames(self):
+        out = []
+        nj = self._f("js_instant")(self.h, None, 0)
+        for f in range(self._f("frame_count")(self.h)):
+            js = np.empty(max(nj, 1), self._rt)
+            plane = np.empty(1 << 22, self._rt)
+            st, ax, pi, n1, n2 = (C.c_int(0) for _ in range(5))
+            npl = self._f("get_frame")(self.h, f, C.byref(st), _ptr(js, self._rp), nj, _ptr(plane, self._rp),
+                                       plane.size, C.byref(ax), C.byref(pi), C.byref(n1), C.byref(n2))
+            out.append({"step": st.value, "js": js[:nj].astype(self.dtype),
+                        "plane": plane[:max(npl, 0)].reshape(n2.value, n1.value).astype(self.dtype)
+                        if npl > 0 else None, "axis": ax.value, "index": pi.value})
+        return out
+
+    def far_field(self, n_theta=37, n_phi=73):
+        U = np.empty(n_theta * n_phi, self._rt)
+        um, d, pt, pp = (self._rs(0) for _ in range(4))
+        rc = self._f("far_field")(self.h, n_theta, n_phi, _ptr(U, self._rp), C.byref(um), C.byref(d),
+                                  C.byref(pt), C.byref(pp))
+        if rc != 0:
+            return None
+        return {"U": U.reshape(n_theta, n_phi).astype(self.dtype), "u_max": um.value,
+                "directivity": d.value, "peak_theta_deg": pt.value, "peak_phi_deg": pp.value}
+
+
+def _surface_signatures(L, p, rp, rs):
+    getattr(L, p + "set_field_plane").argtypes = [C.c_void_p, C.c_int, C.c_int]
+    for nm in ("surface_faces", "huygens_faces"):
+        f = getattr(L, p + nm)
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p, _u64p, _i32p, _i32p, _f32p, C.c_int]
+    f = getattr(L, p + "js_instant")
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, rp, C.c_int]
+    f = getattr(L, p + "js_dft")
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, rp, rp, rp, C.c_int, _i32p]
+    f = getattr(L, p + "huygens_dft")
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, rp, C.c_int, _i32p]
+    f = getattr(L, p + "field_plane")
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, rp, C.c_size_t, _i32p, _i32p, _i32p, _i32p]
+    f = getattr(L, p + "frame_count")
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p]
+    f = getattr(L, p + "get_frame")
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_int, _i32p, rp, C.c_int, rp, C.c_size_t, _i32p, _i32p, _i32p, _i32p]
+    f = getattr(L, p + "far_field")
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_int, C.c_int, rp, C.POINTER(rs), C.POINTER(rs), C.POINTER(rs),
+                  C.POINTER(rs)]
+
+
+class Oracle(_SurfaceMonitors):
     """The CPU restatement; ``fp64=False`` is bitwise the reference's float step."""
 
     _lib = None
+    _p, _rt, _rp, _rs = "orc_", np.float64, _f64p, C.c_double
 
     @classmethod
     def lib(cls):
@@ -94,6 +218,9 @@ class Oracle:
             L.orc_scatter_unitarity.argtypes = [C.c_int]
             L.orc_stub_unitarity.restype = C.c_double
             L.orc_stub_unitarity.argtypes = [C.c_int, C.c_double]
+            L.orc_configure_surface.restype = C.c_int
+            L.orc_configure_surface.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            _surface_signatures(L, "orc_", _f64p, C.c_double)
             cls._lib = L
         return cls._lib
 
@@ -112,13 +239,14 @@ class Oracle:
             self.h = None
 
     def setup(self, nx, ny, nz, mat, table=(), origin=(0.0, 0.0, 0.0), dl=1e-3, f0=1e9,
-              waveform=2, total_steps=2000, settle_steps=600, rho=0.0):
+              waveform=2, total_steps=2000, settle_steps=600, rho=0.0, huy_offset=0, record_every=0):
         mat, eps, sig, ox, oy, oz = _setup_args(nx, ny, nz, origin, dl, mat, table)
         rc = self.L.orc_setup(self.h, nx, ny, nz, ox, oy, oz, dl, _ptr(mat, _u8p), _ptr(eps, _f32p),
                               _ptr(sig, _f32p), len(table), f0, waveform, total_steps,
                               settle_steps, rho)
         if rc != 0:
             raise ValueError(f"oracle setup rejected the inputs (code {rc})")
+        self.L.orc_configure_surface(self.h, huy_offset, record_every)
         self.n = nx * ny * nz
         self.step_index = 0
 
@@ -201,10 +329,11 @@ class Oracle:
         return cls.lib().orc_stub_unitarity(1 if fp64 else 0, epsr)
 
 
-class RefSolver:
+class RefSolver(_SurfaceMonitors):
     """The reference's own TlmSolver (compiled headless), same methods as ``Oracle``."""
 
     _lib = None
+    _p, _rt, _rp, _rs = "ref_", np.float32, _f32p, C.c_float
 
     @classmethod
     def lib(cls):
@@ -258,6 +387,9 @@ class RefSolver:
             L.ref_diel_unitarity.restype = C.c_float
             L.ref_diel_unitarity.argtypes = [C.c_float]
             L.ref_hw_concurrency.restype = C.c_uint
+            L.ref_setup_ex.restype = C.c_int
+            L.ref_setup_ex.argtypes = L.ref_setup.argtypes + [C.c_int, C.c_int]
+            _surface_signatures(L, "ref_", _f32p, C.c_float)
             cls._lib = L
         return cls._lib
 
@@ -279,10 +411,11 @@ class RefSolver:
         return self.L.ref_threads(self.h)
 
     def setup(self, nx, ny, nz, mat, table=(), origin=(0.0, 0.0, 0.0), dl=1e-3, f0=1e9,
-              waveform=2, total_steps=2000, settle_steps=600, rho=0.0):
+              waveform=2, total_steps=2000, settle_steps=600, rho=0.0, huy_offset=0, record_every=0):
         mat, eps, sig, ox, oy, oz = _setup_args(nx, ny, nz, origin, dl, mat, table)
-        self.L.ref_setup(self.h, nx, ny, nz, ox, oy, oz, dl, _ptr(mat, _u8p), _ptr(eps, _f32p),
-                         _ptr(sig, _f32p), len(table), f0, waveform, total_steps, settle_steps, rho)
+        self.L.ref_setup_ex(self.h, nx, ny, nz, ox, oy, oz, dl, _ptr(mat, _u8p), _ptr(eps, _f32p),
+                            _ptr(sig, _f32p), len(table), f0, waveform, total_steps, settle_steps, rho,
+                            huy_offset, record_every)
         self.n = nx * ny * nz
         self.step_index = 0
 

@@ -134,3 +134,18 @@ def interior_tiles(w, V=4, block=256):
         i, r = c % nx, c // nx
         gen[(r * px + i) // T] = True
     return int((~gen).sum())
+
+
+def surface_cases():
+    """Dipole grids with every surface monitor on: PEC-surface currents, a
+    Huygens box, an |E| cut plane and playback frames, DFT from a settle step."""
+    out = []
+    for name, dims, length, slab, steps, settle, huy, every, plane in (
+        ("surface_dipole_slab", (24, 26, 30), 13, (2, 6, 3.0), 90, 20, 3, 7, (1, 13)),
+        ("surface_dipole_odd", (21, 23, 27), 11, None, 70, 30, 2, 5, (2, 9)),
+    ):
+        w = workloads.dipole(*dims, length, slab=slab, steps=steps, nfreq=4, name=name)
+        w.meta.update(settle_steps=settle, huy_offset=huy, record_every=every, field_plane=plane,
+                      surface_monitors=True)
+        out.append(w)
+    return out

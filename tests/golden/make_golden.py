@@ -12,6 +12,10 @@ on seeded synthetic workloads and stores its outputs:
   small_<name>.npz       small grids (PEC, dielectrics, rho != 0, plane wave,
                          odd x extents): full final pulse and stub state plus
                          all records
+  surface_<name>.npz     dipoles with the surface monitors on: PEC faces,
+                         |Js| and its DFT (raw and finalised), Huygens faces
+                         and phasors, the |E| cut plane, playback frames and
+                         the far field (19 x 37 directions)
 
 Run:  python tests/golden/make_golden.py [--skip-large]
 (needs the reference sources to build oracle/_ref; takes ~3 minutes)
@@ -31,7 +35,7 @@ sys.path.insert(0, ROOT)
 from emsolver_b200 import workloads  # noqa: E402
 from oracle import RefSolver, build_oracle  # noqa: E402
 from oracle import drive  # noqa: E402
-from tests.golden.cases import small_cases  # noqa: E402
+from tests.golden.cases import small_cases, surface_cases  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 
@@ -45,6 +49,30 @@ def run_ref(w, steps=None):
     return S
 
 
+def surface_record(S):
+    """Every surface-monitor output of a solver (reference or oracle)."""
+    sf, hf = S.surface_faces(), S.huygens_faces()
+    re, im, mag, ns = S.js_dft()
+    acc, hs = S.huygens_dft()
+    plane = S.field_plane()
+    frames = S.frames()
+    ff = S.far_field(19, 37)
+    out = {"face_cells": sf["cells"], "face_axis": sf["axis"], "face_sign": sf["sign"],
+           "face_center": sf["center"], "js_instant": S.js_instant(), "js_re": re, "js_im": im,
+           "js_mag": mag, "js_samples": ns, "huy_cells": hf["cells"], "huy_axis": hf["axis"],
+           "huy_sign": hf["out_sign"], "huy_pos": hf["pos"], "huy_acc": acc, "huy_samples": hs,
+           "plane": plane[0], "plane_axis": plane[1], "plane_index": plane[2],
+           "frame_steps": np.array([f["step"] for f in frames]),
+           "frame_js": np.stack([f["js"] for f in frames]),
+           "far_U": ff["U"], "far_u_max": ff["u_max"], "far_directivity": ff["directivity"],
+           "far_peak": np.array([ff["peak_theta_deg"], ff["peak_phi_deg"]])}
+    last = [f for f in frames if f["plane"] is not None]
+    if last:
+        out["frame_last_plane"] = last[-1]["plane"]
+        out["frame_last_plane_step"] = last[-1]["step"]
+    return out
+
+
 def main():
     build_oracle()
     skip_large = "--skip-large" in sys.argv
@@ -54,6 +82,10 @@ def main():
         y, g = S.tables()
         np.savez_compressed(os.path.join(OUT, w.name + ".npz"), pulses=S.pulses(), stubs=S.stubs(),
                             yhat=y, ghat=g, threads=S.threads, **rec)
+        print("wrote", w.name, flush=True)
+    for w in surface_cases():
+        S = run_ref(w)
+        np.savez_compressed(os.path.join(OUT, w.name + ".npz"), **surface_record(S))
         print("wrote", w.name, flush=True)
     if skip_large:
         return

@@ -13,7 +13,7 @@ import pytest
 from tests.conftest import golden
 from emsolver_b200 import workloads
 from oracle import Oracle, RefSolver, drive, ref_available
-from tests.golden.cases import small_cases
+from tests.golden.cases import small_cases, surface_cases
 
 CASES = small_cases()
 
@@ -156,3 +156,43 @@ def test_port_loop_outside_grid_is_refused(built):
     S.setup(5, 5, 5, np.zeros(125, np.uint8), [])
     assert S.add_port(np.array([0], np.uint64), 2, 1.0) == -1
     assert S.add_port(np.array([62], np.uint64), 2, 1.0) == 0
+
+
+SURFACE_KEYS_EXACT = ("face_cells", "face_axis", "face_sign", "face_center", "js_instant", "js_re", "js_im",
+                      "js_mag", "js_samples", "huy_cells", "huy_axis", "huy_sign", "huy_pos", "huy_acc",
+                      "huy_samples", "plane", "plane_axis", "plane_index", "frame_steps", "frame_js", "far_U",
+                      "far_u_max", "far_directivity", "far_peak", "frame_last_plane", "frame_last_plane_step")
+
+
+@pytest.mark.parametrize("w", surface_cases(), ids=[w.name for w in surface_cases()])
+def test_surface_monitors_bitwise_vs_reference_golden(built, w):
+    """PEC-surface |Js| and its DFT, Huygens phasors, the cut plane, frames and
+    the far field of the float oracle equal the reference's, bit for bit."""
+    from tests.golden.make_golden import surface_record
+    g = golden(w.name)
+    O = Oracle(False)
+    drive.setup(O, w)
+    drive.advance(O, w, w.steps)
+    got = surface_record(O)
+    for k in SURFACE_KEYS_EXACT:
+        if k in g:
+            assert np.array_equal(np.asarray(got[k]).astype(np.asarray(g[k]).dtype), g[k]), k
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("seed", [21, 22])
+def test_surface_monitors_live_reference(built, seed):
+    from tests.golden.make_golden import surface_record
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = (int(v) for v in rng.integers(14, 26, 3))
+    w = workloads.random_dipole(rng, nx, ny, nz, 60, name="live")
+    w.meta.update(settle_steps=int(rng.integers(0, 30)), huy_offset=2, record_every=int(rng.integers(3, 9)),
+                  field_plane=(int(rng.integers(0, 3)), int(rng.integers(0, 12))), surface_monitors=True)
+    recs = []
+    for S in (RefSolver(), Oracle(False)):
+        drive.setup(S, w)
+        drive.advance(S, w, w.steps)
+        recs.append(surface_record(S))
+    for k in SURFACE_KEYS_EXACT:
+        if k in recs[0]:
+            assert np.array_equal(np.asarray(recs[1][k]).astype(np.asarray(recs[0][k]).dtype), recs[0][k]), k
