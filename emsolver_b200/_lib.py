@@ -141,6 +141,39 @@ SIGNATURES = {
                             _P(C.c_int), _P(C.c_int), _P(C.c_int), _P(C.c_int)]),
     "tlm_compute_far_field": (_st, [_h, C.c_int, C.c_int, _P(C.c_float), _P(C.c_float), _P(C.c_float),
                                     _P(C.c_float), _P(C.c_float)]),
+    # Yee FDTD (include/fdtd_b200.h)
+    "fdtd_create": (_st, [_P(_h), C.c_int]),
+    "fdtd_destroy": (_st, [_h]),
+    "fdtd_last_error": (C.c_char_p, [_h]),
+    "fdtd_setup": (_st, [_h, _P(Grid), _P(C.c_uint8), C.c_size_t, _P(MatPropsC), C.c_int, _P(ConfigC)]),
+    "fdtd_add_port": (_st, [_h, _P(C.c_uint64), C.c_int, C.c_int, C.c_float, _P(C.c_int)]),
+    "fdtd_add_plane_wave": (_st, [_h, C.c_int, C.c_int, C.c_int, C.c_float]),
+    "fdtd_add_probe": (_st, [_h, C.c_float, C.c_float, C.c_float, _P(C.c_int)]),
+    "fdtd_set_source_table": (_st, [_h, _P(C.c_float), C.c_int]),
+    "fdtd_step": (_st, [_h, C.c_int]),
+    "fdtd_run": (_st, [_h]),
+    "fdtd_current_step": (C.c_int, [_h]),
+    "fdtd_timestep": (C.c_float, [_h]),
+    "fdtd_get_field": (_st, [_h, C.c_int, _P(C.c_float), C.c_size_t, _P(C.c_size_t)]),
+    "fdtd_get_probe": (_st, [_h, C.c_int, _P(C.c_float), _P(C.c_float), _P(C.c_float), C.c_int, _P(C.c_int)]),
+    "fdtd_get_port": (_st, [_h, C.c_int, _P(C.c_float), _P(C.c_float), C.c_int, _P(C.c_int)]),
+    "fdtd_get_energy_history": (_st, [_h, _P(C.c_int), _P(C.c_float), _P(C.c_double), C.c_int, _P(C.c_int)]),
+    "fdtd_get_surface_faces": (_st, [_h, _P(C.c_uint64), _P(C.c_int), _P(C.c_int), _P(C.c_float), C.c_int,
+                                     _P(C.c_int)]),
+    "fdtd_get_js_instant": (_st, [_h, _P(C.c_float), C.c_int, _P(C.c_int)]),
+    "fdtd_get_js_dft": (_st, [_h, _P(C.c_float), _P(C.c_float), _P(C.c_float), C.c_int, _P(C.c_int),
+                              _P(C.c_int)]),
+    "fdtd_get_huygens_faces": (_st, [_h, _P(C.c_uint64), _P(C.c_int), _P(C.c_int), _P(C.c_float), C.c_int,
+                                     _P(C.c_int)]),
+    "fdtd_get_huygens_dft": (_st, [_h, _P(C.c_float), C.c_int, _P(C.c_int), _P(C.c_int)]),
+    "fdtd_set_field_plane": (_st, [_h, C.c_int, C.c_int]),
+    "fdtd_get_field_plane": (_st, [_h, _P(C.c_float), C.c_size_t, _P(C.c_int), _P(C.c_int), _P(C.c_int),
+                                   _P(C.c_int)]),
+    "fdtd_frame_count": (_st, [_h, _P(C.c_int)]),
+    "fdtd_get_frame": (_st, [_h, C.c_int, _P(C.c_int), _P(C.c_float), C.c_int, _P(C.c_float), C.c_size_t,
+                             _P(C.c_int), _P(C.c_int), _P(C.c_int), _P(C.c_int)]),
+    "fdtd_compute_far_field": (_st, [_h, C.c_int, C.c_int, _P(C.c_float), _P(C.c_float), _P(C.c_float),
+                                     _P(C.c_float), _P(C.c_float)]),
     "tlm_step_planes_noalloc": (_st, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
                                       C.c_void_p, C.c_void_p]),

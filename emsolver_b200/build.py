@@ -26,7 +26,7 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
               "-I" + INCLUDE, "-I" + CSRC]
-CUDA_SOURCES = ["tlm_solver.cu", "tlm_surface.cu", "tlm_noalloc.cu", "tlm_batch.cu", "tlm_server.cu"]
+CUDA_SOURCES = ["tlm_solver.cu", "tlm_surface.cu", "fdtd_solver.cu", "tlm_noalloc.cu", "tlm_batch.cu", "tlm_server.cu"]
 HOST_SOURCES = ["tlm_host_math.cpp"]
 
 LIBS = {

@@ -92,6 +92,26 @@ void dft_phase_f64(float f0, double dt, int n, double *c, double *s)
     *s = std::sin(phase);
 }
 
+// Yee FDTD constants (FdtdSolver.cpp:15-18, 88-89, 143, 452): Courant-limited
+// time step, first-order Mur coefficient, air E update and H update factors.
+static const float kEps0 = 8.8541878128e-12f;
+static const float kMu0 = 1.25663706212e-6f;
+float fdtd_dt(float dl) { return 0.99f * dl / (kC0 * std::sqrt(3.0f)); }
+float fdtd_cmur(float dt, float dl) { return (kC0 * dt - dl) / (kC0 * dt + dl); }
+float fdtd_cb0(float dt, float dl) { return dt / (kEps0 * dl); }
+float fdtd_ch(float dt, float dl) { return dt / (kMu0 * dl); }
+// Lossy-dielectric E coefficients of one edge from the sums of (1 + (epsr -
+// 1)) and sigma over its cnt in-grid neighbour cells (FdtdSolver.cpp:193-206).
+void fdtd_edge_coef(float eAcc, float sAcc, int cnt, float dt, float dl, float *ca, float *cb)
+{
+    const float epsr = eAcc / cnt;
+    const float sigma = sAcc / cnt;
+    const float eps = kEps0 * std::max(1.0f, epsr);
+    const float lf = sigma * dt / (2.0f * eps);
+    *ca = (1.0f - lf) / (1.0f + lf);
+    *cb = (dt / (eps * dl)) / (1.0f + lf);
+}
+
 float probe_scale_f32(float dl) { return -1.0f / dl; }
 double probe_scale_f64(float dl) { return -1.0 / (double)dl; }
 

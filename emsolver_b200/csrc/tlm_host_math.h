@@ -12,6 +12,11 @@ void tables_f32(const float *epsr, const float *sigma, int n, float dl, float *y
 void tables_f64(const float *epsr, const float *sigma, int n, float dl, double *yhat,
                 double *ghat);
 float probe_scale_f32(float dl);
+float fdtd_dt(float dl);
+float fdtd_cmur(float dt, float dl);
+float fdtd_cb0(float dt, float dl);
+float fdtd_ch(float dt, float dl);
+void fdtd_edge_coef(float eAcc, float sAcc, int cnt, float dt, float dl, float *ca, float *cb);
 void dft_phase_f32(float f0, float dt, int n, float *c, float *s);
 void dft_phase_f64(float f0, double dt, int n, double *c, double *s);
 double probe_scale_f64(float dl);

@@ -347,6 +347,15 @@ tlm_status setWindow(tlm_solver *h, int window);
 tlm_status rewind(tlm_solver *h);
 tlm_status reshape(tlm_solver *h, int variant);
 // Surface monitors (defined in tlm_surface.cu).
+void buildFaceLists(int nx, int ny, int nz, const float origin[3], float dl, const uint8_t *mat, bool surfaceOn,
+                    int huyOffset, SurfaceState &s);
+struct FarField
+{
+    float uMax = 0, directivity = 0, peakTheta = 0, peakPhi = 0;
+};
+tlm_status farFieldTransform(cudaStream_t stream, cudaMemPool_t pool, bool f64, const void *dAcc,
+                             const long long *dCode, const float *hostPos, int nh, float f0, int n_theta,
+                             int n_phi, float *U, FarField &out, std::string &err);
 void buildSurfaceLists(tlm_solver *h);
 tlm_status prepareSurface(tlm_solver *h);
 void freeSurface(tlm_solver *h);

@@ -282,14 +282,6 @@ namespace tlmi {
 
 namespace {
 
-// Cell centre origin + (i + 0.5) dl per axis, in float (Geometry.h:100-105).
-void cellCenter(const tlm_solver *h, int i, int j, int k, float c[3])
-{
-    c[0] = h->g.origin[0] + ((float)i + 0.5f) * h->g.dl;
-    c[1] = h->g.origin[1] + ((float)j + 0.5f) * h->g.dl;
-    c[2] = h->g.origin[2] + ((float)k + 0.5f) * h->g.dl;
-}
-
 size_t realSize(const tlm_solver *h) { return realBytes(h->storage); }
 
 } // namespace
@@ -298,9 +290,9 @@ size_t realSize(const tlm_solver *h) { return realBytes(h->storage); }
 // BuildPecSurfaceFaces (Geometry.cpp:402-436; cell, then axis, then side -1
 // before +1), Huygens faces by TlmSolver::buildHuygens (TlmSolver.cpp:310-348;
 // x faces over (k, j), y faces over (k, i), z faces over (j, i), low first).
-void buildSurfaceLists(tlm_solver *h)
+void buildFaceLists(int nx, int ny, int nz, const float origin[3], float dl, const uint8_t *mat, bool surfaceOn,
+                    int huyOffset, SurfaceState &s)
 {
-    SurfaceState &s = h->surf;
     s.jsCell.clear();
     s.jsAxis.clear();
     s.jsSign.clear();
@@ -309,17 +301,21 @@ void buildSurfaceLists(tlm_solver *h)
     s.huyAxis.clear();
     s.huySign.clear();
     s.huyPos.clear();
-    if (!h->cfg.surface_monitors) return;
-    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    if (!surfaceOn) return;
+    auto center = [&](int i, int j, int k, float c[3]) {
+        // origin + (i + 0.5) dl per axis, in float (Geometry.h:100-105)
+        c[0] = origin[0] + ((float)i + 0.5f) * dl;
+        c[1] = origin[1] + ((float)j + 0.5f) * dl;
+        c[2] = origin[2] + ((float)k + 0.5f) * dl;
+    };
     const long long stride[3] = { 1, nx, (long long)nx * ny };
     const int dims[3] = { nx, ny, nz };
-    const float dl = h->g.dl;
     for (int k = 0; k < nz; ++k)
         for (int j = 0; j < ny; ++j)
             for (int i = 0; i < nx; ++i)
             {
                 const size_t c = ((size_t)k * ny + j) * nx + i;
-                if (h->mat[c] != tlmk::kPec) continue;
+                if (mat[c] != tlmk::kPec) continue;
                 const int co[3] = { i, j, k };
                 for (int a = 0; a < 3; ++a)
                     for (int sd = -1; sd <= 1; sd += 2)
@@ -327,9 +323,9 @@ void buildSurfaceLists(tlm_solver *h)
                         const int q = co[a] + sd;
                         if (q < 0 || q >= dims[a]) continue;
                         const size_t nb = c + (size_t)((long long)sd * stride[a]);
-                        if (h->mat[nb] == tlmk::kPec) continue;
+                        if (mat[nb] == tlmk::kPec) continue;
                         float cc[3];
-                        cellCenter(h, i, j, k, cc);
+                        center(i, j, k, cc);
                         cc[a] = cc[a] + (float)sd * dl * 0.5f;
                         s.jsCell.push_back(nb);
                         s.jsAxis.push_back(a);
@@ -337,16 +333,16 @@ void buildSurfaceLists(tlm_solver *h)
                         s.jsCenter.insert(s.jsCenter.end(), cc, cc + 3);
                     }
             }
-    const int o = h->cfg.huy_offset;
+    const int o = huyOffset;
     if (o < 2 || 2 * o + 2 >= nx || 2 * o + 2 >= ny || 2 * o + 2 >= nz) return;
     const float half[3] = { ((float)nx * dl) * 0.5f, ((float)ny * dl) * 0.5f, ((float)nz * dl) * 0.5f };
     float dom[3];
-    for (int a = 0; a < 3; ++a) dom[a] = h->g.origin[a] + half[a];
+    for (int a = 0; a < 3; ++a) dom[a] = origin[a] + half[a];
     auto add = [&](int i, int j, int k, int axis, int outSign) {
         const size_t c = ((size_t)k * ny + j) * nx + i;
-        if (h->mat[c] != tlmk::kAir) return;
+        if (mat[c] != tlmk::kAir) return;
         float cc[3];
-        cellCenter(h, i, j, k, cc);
+        center(i, j, k, cc);
         s.huyCell.push_back(c);
         s.huyAxis.push_back(axis);
         s.huySign.push_back(outSign);
@@ -371,6 +367,12 @@ void buildSurfaceLists(tlm_solver *h)
             add(i, j, z0, 2, -1);
             add(i, j, z1, 2, +1);
         }
+}
+
+void buildSurfaceLists(tlm_solver *h)
+{
+    buildFaceLists(h->nx, h->ny, h->nz, h->g.origin, h->g.dl, h->mat.data(), h->cfg.surface_monitors != 0,
+                   h->cfg.huy_offset, h->surf);
 }
 
 bool surfaceActive(const tlm_solver *h)
@@ -569,6 +571,93 @@ tlm_status launchSurface(tlm_solver *h, int n)
     case TLM_STORE_BFP16: return launchSurfaceT<tlmk::Bfp4>(h, n);
     default: return launchSurfaceT<float>(h, n);
     }
+}
+
+} // namespace tlmi
+
+namespace tlmi {
+
+// Near-to-far-field transform of the Huygens phasors on the device (one block
+// per direction, FP64 sums), then the reference's directivity and peak
+// search on the host (TlmSolver.cpp:893-915). `f64`: the phasors are double.
+tlm_status farFieldTransform(cudaStream_t stream, cudaMemPool_t pool, bool f64, const void *dAcc,
+                             const long long *dCode, const float *hostPos, int nh, float f0, int n_theta,
+                             int n_phi, float *U, FarField &out, std::string &err)
+{
+    const int nd = n_theta * n_phi;
+    float *dPos = nullptr;
+    void *dU = nullptr;
+    const size_t r = f64 ? 8 : 4;
+    cudaError_t e = cudaMallocFromPoolAsync((void **)&dPos, (size_t)nh * 3 * sizeof(float), pool, stream);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&dU, (size_t)nd * r, pool, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dPos, hostPos, (size_t)nh * 3 * sizeof(float), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+    {
+        if (f64)
+        {
+            const double k0 = 2.0 * 3.14159265358979323846 * (double)f0 / (double)299792458.0f;
+            tlmk::farFieldKernel<double><<<nd, 256, 0, stream>>>(static_cast<const double *>(dAcc), dCode, dPos,
+                                                                 nh, k0, n_theta, n_phi,
+                                                                 static_cast<double *>(dU));
+        }
+        else
+        {
+            const float k0 = 2.0f * (float)3.14159265358979323846 * f0 / 299792458.0f;
+            tlmk::farFieldKernel<float><<<nd, 256, 0, stream>>>(static_cast<const float *>(dAcc), dCode, dPos, nh,
+                                                                k0, n_theta, n_phi, static_cast<float *>(dU));
+        }
+        e = cudaGetLastError();
+    }
+    std::vector<float> u(nd);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess)
+    {
+        if (f64)
+        {
+            std::vector<double> t(nd);
+            e = cudaMemcpy(t.data(), dU, (size_t)nd * 8, cudaMemcpyDeviceToHost);
+            for (int i = 0; i < nd; ++i) u[i] = (float)t[i];
+        }
+        else
+            e = cudaMemcpy(u.data(), dU, (size_t)nd * 4, cudaMemcpyDeviceToHost);
+    }
+    if (dPos) cudaFreeAsync(dPos, stream);
+    if (dU) cudaFreeAsync(dU, stream);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        err = std::string("far-field transform: ") + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? TLM_ENOMEM : TLM_ECUDA;
+    }
+    const float pi = (float)3.14159265358979323846;
+    float um = 0.0f;
+    int iMax = 0;
+    double prad = 0.0;
+    const float dTh = pi / (float)(n_theta - 1);
+    const float dPh = 2.0f * pi / (float)(n_phi - 1);
+    for (int ti = 0; ti < n_theta; ++ti)
+    {
+        const float th = pi * (float)ti / (float)(n_theta - 1);
+        const float wTh = (ti == 0 || ti == n_theta - 1) ? 0.5f : 1.0f;
+        for (int pj = 0; pj < n_phi; ++pj)
+        {
+            const float wPh = (pj == 0 || pj == n_phi - 1) ? 0.5f : 1.0f;
+            const float v = u[(size_t)ti * n_phi + pj];
+            if (v > um)
+            {
+                um = v;
+                iMax = ti * n_phi + pj;
+            }
+            prad += (double)v * std::sin(th) * wTh * wPh * dTh * dPh;
+        }
+    }
+    if (U) std::copy(u.begin(), u.end(), U);
+    out.uMax = um;
+    out.directivity = prad > 0 ? (float)(4.0 * 3.14159265358979323846 * um / prad) : 0.0f;
+    out.peakTheta = 180.0f * (float)(iMax / n_phi) / (float)(n_theta - 1);
+    out.peakPhi = 360.0f * (float)(iMax % n_phi) / (float)(n_phi - 1);
+    return TLM_OK;
 }
 
 } // namespace tlmi
@@ -796,81 +885,16 @@ tlm_status tlm_compute_far_field(tlm_handle h, int n_theta, int n_phi, float *U,
                                    "steps past settle_steps)");
     DeviceGuard dg(h->device);
     TLM_TRY(syncState(h));
-    const int nd = n_theta * n_phi;
-    float *dPos = nullptr;
-    void *dU = nullptr;
-    const size_t r = realBytes(h->storage);
-    TLM_TRY(tmpAlloc(h, &dPos, (size_t)nh * 3 * sizeof(float)));
-    tlm_status st = tmpAlloc(h, &dU, (size_t)nd * r);
-    if (st != TLM_OK)
-    {
-        cudaFreeAsync(dPos, h->stream);
-        return st;
-    }
-    cudaError_t e = cudaMemcpyAsync(dPos, s.huyPos.data(), (size_t)nh * 3 * sizeof(float), cudaMemcpyHostToDevice,
-                                    h->stream);
-    if (e == cudaSuccess)
-    {
-        if (h->storage == TLM_STORE_F64)
-        {
-            const double k0 = 2.0 * 3.14159265358979323846 * (double)h->cfg.f0 / (double)299792458.0f;
-            tlmk::farFieldKernel<double><<<nd, 256, 0, h->stream>>>(
-                static_cast<const double *>(s.dHuyAcc), s.dHuyNode, dPos, nh, k0, n_theta, n_phi,
-                static_cast<double *>(dU));
-        }
-        else
-        {
-            const float k0 = 2.0f * (float)3.14159265358979323846 * h->cfg.f0 / 299792458.0f;
-            tlmk::farFieldKernel<float><<<nd, 256, 0, h->stream>>>(static_cast<const float *>(s.dHuyAcc),
-                                                                   s.dHuyNode, dPos, nh, k0, n_theta, n_phi,
-                                                                   static_cast<float *>(dU));
-        }
-        e = cudaGetLastError();
-    }
-    std::vector<float> u(nd);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e == cudaSuccess)
-    {
-        if (h->storage == TLM_STORE_F64)
-        {
-            std::vector<double> t(nd);
-            e = cudaMemcpy(t.data(), dU, (size_t)nd * 8, cudaMemcpyDeviceToHost);
-            for (int i = 0; i < nd; ++i) u[i] = (float)t[i];
-        }
-        else
-            e = cudaMemcpy(u.data(), dU, (size_t)nd * 4, cudaMemcpyDeviceToHost);
-    }
-    cudaFreeAsync(dPos, h->stream);
-    cudaFreeAsync(dU, h->stream);
-    TLM_TRY(h->cuda(e, "far-field transform"));
-    // directivity by the trapezoidal rule (TlmSolver.cpp:893-915)
-    const float pi = (float)3.14159265358979323846;
-    float um = 0.0f;
-    int iMax = 0;
-    double prad = 0.0;
-    const float dTh = pi / (float)(n_theta - 1);
-    const float dPh = 2.0f * pi / (float)(n_phi - 1);
-    for (int ti = 0; ti < n_theta; ++ti)
-    {
-        const float th = pi * (float)ti / (float)(n_theta - 1);
-        const float wTh = (ti == 0 || ti == n_theta - 1) ? 0.5f : 1.0f;
-        for (int pj = 0; pj < n_phi; ++pj)
-        {
-            const float wPh = (pj == 0 || pj == n_phi - 1) ? 0.5f : 1.0f;
-            const float v = u[(size_t)ti * n_phi + pj];
-            if (v > um)
-            {
-                um = v;
-                iMax = ti * n_phi + pj;
-            }
-            prad += (double)v * std::sin(th) * wTh * wPh * dTh * dPh;
-        }
-    }
-    if (U) std::copy(u.begin(), u.end(), U);
-    if (u_max) *u_max = um;
-    if (directivity) *directivity = prad > 0 ? (float)(4.0 * 3.14159265358979323846 * um / prad) : 0.0f;
-    if (peak_theta_deg) *peak_theta_deg = 180.0f * (float)(iMax / n_phi) / (float)(n_theta - 1);
-    if (peak_phi_deg) *peak_phi_deg = 360.0f * (float)(iMax % n_phi) / (float)(n_phi - 1);
+    FarField out;
+    std::string err;
+    const tlm_status st = farFieldTransform(h->stream, h->pool, h->storage == TLM_STORE_F64, s.dHuyAcc,
+                                            s.dHuyNode, s.huyPos.data(), nh, h->cfg.f0, n_theta, n_phi, U,
+                                            out, err);
+    if (st != TLM_OK) return h->fail(st, err);
+    if (u_max) *u_max = out.uMax;
+    if (directivity) *directivity = out.directivity;
+    if (peak_theta_deg) *peak_theta_deg = out.peakTheta;
+    if (peak_phi_deg) *peak_phi_deg = out.peakPhi;
     return TLM_OK;
 }
 

@@ -11,4 +11,4 @@ Two CPU implementations of the reference's TLM time step, loaded with ctypes:
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` import this package, and only as the checker.
 """
-from .wrappers import Oracle, RefSolver, ref_available, build_oracle  # noqa: F401
+from .wrappers import Oracle, RefFdtd, RefSolver, ref_available, build_oracle  # noqa: F401

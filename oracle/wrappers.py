@@ -502,3 +502,115 @@ class RefSolver(_SurfaceMonitors):
     @classmethod
     def stub_unitarity(cls, epsr):
         return cls.lib().ref_diel_unitarity(epsr)
+
+
+class RefFdtd(_SurfaceMonitors):
+    """The reference's own Yee FDTD solver (FdtdSolver.cpp, compiled headless)."""
+
+    _lib = None
+    _p, _rt, _rp, _rs = "fdr_", np.float32, _f32p, C.c_float
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            L = RefSolver.lib()
+            L.fdr_create.restype = C.c_void_p
+            L.fdr_destroy.argtypes = [C.c_void_p]
+            L.fdr_setup.restype = C.c_int
+            L.fdr_setup.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                    C.c_float, _u8p, _f32p, _f32p, C.c_int, C.c_float, C.c_int, C.c_int,
+                                    C.c_int, C.c_int, C.c_int]
+            L.fdr_add_port.restype = C.c_int
+            L.fdr_add_port.argtypes = [C.c_void_p, _u64p, C.c_int, C.c_int, C.c_float]
+            L.fdr_add_probe.restype = C.c_int
+            L.fdr_add_probe.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float]
+            L.fdr_add_plane_wave.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float]
+            L.fdr_steps.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            L.fdr_steps_sv.argtypes = [C.c_void_p, C.c_int, C.c_int, _f32p]
+            L.fdr_dt.restype = C.c_float
+            L.fdr_dt.argtypes = [C.c_void_p]
+            L.fdr_get_field.restype = C.c_size_t
+            L.fdr_get_field.argtypes = [C.c_void_p, C.c_int, _f32p, C.c_size_t]
+            L.fdr_get_probe.restype = C.c_int
+            L.fdr_get_probe.argtypes = [C.c_void_p, C.c_int, _f32p, _f32p, _f32p, C.c_int]
+            L.fdr_get_port.restype = C.c_int
+            L.fdr_get_port.argtypes = [C.c_void_p, C.c_int, _f32p, _f32p, C.c_int]
+            L.fdr_energy_history.restype = C.c_int
+            L.fdr_energy_history.argtypes = [C.c_void_p, _i32p, _f32p, C.c_int]
+            _surface_signatures(L, "fdr_", _f32p, C.c_float)
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self):
+        self.L = self.lib()
+        self.h = self.L.fdr_create()
+        self.n = 0
+        self.step_index = 0
+        self.dtype = np.float32
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.L.fdr_destroy(h)
+            self.h = None
+
+    def setup(self, nx, ny, nz, mat, table=(), origin=(0.0, 0.0, 0.0), dl=1e-3, f0=1e9,
+              waveform=2, total_steps=2000, settle_steps=600, rho=0.0, huy_offset=0, record_every=0):
+        mat, eps, sig, ox, oy, oz = _setup_args(nx, ny, nz, origin, dl, mat, table)
+        self.L.fdr_setup(self.h, nx, ny, nz, ox, oy, oz, dl, _ptr(mat, _u8p), _ptr(eps, _f32p),
+                         _ptr(sig, _f32p), len(table), f0, waveform, total_steps, settle_steps, huy_offset,
+                         record_every)
+        self.n = nx * ny * nz
+        self.step_index = 0
+
+    def add_port(self, cells, pol, amp=1.0):
+        c = np.ascontiguousarray(cells, dtype=np.uint64).reshape(-1)
+        return self.L.fdr_add_port(self.h, _ptr(c, _u64p), c.size, pol, amp)
+
+    def add_probe(self, x, y, z):
+        return self.L.fdr_add_probe(self.h, x, y, z)
+
+    def add_plane_wave(self, prop_axis, plane_index, pol_axis, amp=1.0):
+        self.L.fdr_add_plane_wave(self.h, prop_axis, plane_index, pol_axis, amp)
+
+    @property
+    def dt(self):
+        return self.L.fdr_dt(self.h)
+
+    def steps(self, count, sv=None):
+        if sv is not None:
+            sv = np.ascontiguousarray(sv, dtype=np.float32).reshape(-1)
+            assert sv.size >= count
+            self.L.fdr_steps_sv(self.h, self.step_index, count, _ptr(sv, _f32p))
+        else:
+            self.L.fdr_steps(self.h, self.step_index, count)
+        self.step_index += count
+
+    def fields(self):
+        """Ex, Ey, Ez, Hx, Hy, Hz in the reference's Yee layouts (flat)."""
+        out = {}
+        for w, name in enumerate(("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")):
+            n = self.L.fdr_get_field(self.h, w, None, 0)
+            a = np.empty(n, np.float32)
+            self.L.fdr_get_field(self.h, w, _ptr(a, _f32p), n)
+            out[name] = a
+        return out
+
+    def probe(self, idx):
+        cap = self.step_index
+        ex, ey, ez = (np.empty(max(cap, 1), np.float32) for _ in range(3))
+        n = self.L.fdr_get_probe(self.h, idx, _ptr(ex, _f32p), _ptr(ey, _f32p), _ptr(ez, _f32p), cap)
+        return ex[:n].copy(), ey[:n].copy(), ez[:n].copy()
+
+    def port(self, idx):
+        cap = self.step_index
+        v, i = (np.empty(max(cap, 1), np.float32) for _ in range(2))
+        n = self.L.fdr_get_port(self.h, idx, _ptr(v, _f32p), _ptr(i, _f32p), cap)
+        return v[:n].copy(), i[:n].copy()
+
+    def energy_history(self):
+        cap = self.step_index // 16 + 2
+        st = np.empty(cap, np.int32)
+        va = np.empty(cap, np.float32)
+        n = self.L.fdr_energy_history(self.h, _ptr(st, _i32p), _ptr(va, _f32p), cap)
+        return st[:n].copy(), va[:n].astype(np.float64)

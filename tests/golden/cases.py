@@ -149,3 +149,31 @@ def surface_cases():
                       surface_monitors=True)
         out.append(w)
     return out
+
+
+def fdtd_cases():
+    """Yee FDTD grids: a dipole with a lossy slab and every monitor on (ports,
+    probes, PEC-surface currents, Huygens box, cut plane, frames), and a
+    plane wave through overlapping lossy boxes with a PEC plate."""
+    out = []
+    w = workloads.dipole(16, 18, 20, 9, slab=(2, 5, 3.0), steps=70, nfreq=4, name="fdtd_dipole")
+    w.meta.update(settle_steps=10, huy_offset=2, record_every=9, field_plane=(1, 9), surface_monitors=True)
+    w.probes_cell = [(4, 9, 10), (12, 3, 15)]
+    out.append(w)
+    rng = np.random.default_rng(31)
+    nx, ny, nz = 17, 14, 19
+    mat = np.zeros((nz, ny, nx), np.uint8)
+    table = []
+    for b in range(3):
+        lo = [int(rng.integers(0, d - 3)) for d in (nz, ny, nx)]
+        hi = [min(d, l + int(rng.integers(3, 9))) for l, d in zip(lo, (nz, ny, nx))]
+        mat[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = 2 + b
+        table.append((float(np.float32(rng.uniform(1, 8))), float(np.float32(rng.uniform(0, 0.04)))))
+    mat[12:14, 3:11, 4:13] = 1                      # PEC plate
+    w = workloads.Workload("fdtd_planewave", nx, ny, nz, mat.reshape(-1), table, dl=1e-3, f0=2e10, waveform=1,
+                           steps=60)
+    w.meta["plane_wave"] = (2, 3, 0, 0.8)
+    w.probes_cell = [(8, 7, 9), (2, 2, 16)]
+    w.meta.update(settle_steps=5, record_every=11, field_plane=(2, 6), surface_monitors=True)
+    out.append(w)
+    return out

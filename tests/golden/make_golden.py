@@ -12,6 +12,9 @@ on seeded synthetic workloads and stores its outputs:
   small_<name>.npz       small grids (PEC, dielectrics, rho != 0, plane wave,
                          odd x extents): full final pulse and stub state plus
                          all records
+  fdtd_<name>.npz        the reference's Yee FDTD solver: final E and H
+                         fields, port, probe and energy records and every
+                         surface monitor (a dipole and a plane-wave case)
   surface_<name>.npz     dipoles with the surface monitors on: PEC faces,
                          |Js| and its DFT (raw and finalised), Huygens faces
                          and phasors, the |E| cut plane, playback frames and
@@ -33,15 +36,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 from emsolver_b200 import workloads  # noqa: E402
-from oracle import RefSolver, build_oracle  # noqa: E402
+from oracle import RefFdtd, RefSolver, build_oracle  # noqa: E402
 from oracle import drive  # noqa: E402
-from tests.golden.cases import small_cases, surface_cases  # noqa: E402
+from tests.golden.cases import fdtd_cases, small_cases, surface_cases  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
-def run_ref(w, steps=None):
-    S = RefSolver()
+def run_ref(w, steps=None, solver=RefSolver):
+    S = solver()
     drive.setup(S, w)
     if "plane_wave" in w.meta:
         S.add_plane_wave(*w.meta["plane_wave"])
@@ -49,14 +52,15 @@ def run_ref(w, steps=None):
     return S
 
 
-def surface_record(S):
+def surface_record(S, far=True):
     """Every surface-monitor output of a solver (reference or oracle)."""
     sf, hf = S.surface_faces(), S.huygens_faces()
     re, im, mag, ns = S.js_dft()
     acc, hs = S.huygens_dft()
     plane = S.field_plane()
     frames = S.frames()
-    ff = S.far_field(19, 37)
+    ff = S.far_field(19, 37) if far else {"U": np.zeros((0, 0), np.float32), "u_max": 0.0, "directivity": 0.0,
+                                          "peak_theta_deg": 0.0, "peak_phi_deg": 0.0}
     out = {"face_cells": sf["cells"], "face_axis": sf["axis"], "face_sign": sf["sign"],
            "face_center": sf["center"], "js_instant": S.js_instant(), "js_re": re, "js_im": im,
            "js_mag": mag, "js_samples": ns, "huy_cells": hf["cells"], "huy_axis": hf["axis"],
@@ -73,6 +77,19 @@ def surface_record(S):
     return out
 
 
+def fdtd_record(S, w):
+    """Fields, records and surface monitors of an FDTD solver run on `w`."""
+    out = {k: v for k, v in S.fields().items()}
+    for p in range(len(w.ports)):
+        out[f"port{p}_v"], out[f"port{p}_i"] = S.port(p)
+    for q in range(len(w.probes_cell)):
+        out[f"probe{q}_ex"], out[f"probe{q}_ey"], out[f"probe{q}_ez"] = S.probe(q)
+    st, ev = S.energy_history()
+    out["energy_steps"], out["energy"] = st, ev
+    out.update(surface_record(S, far=S.huygens_faces()["cells"].size > 0))
+    return out
+
+
 def main():
     build_oracle()
     skip_large = "--skip-large" in sys.argv
@@ -86,6 +103,9 @@ def main():
     for w in surface_cases():
         S = run_ref(w)
         np.savez_compressed(os.path.join(OUT, w.name + ".npz"), **surface_record(S))
+        print("wrote", w.name, flush=True)
+    for w in fdtd_cases():
+        np.savez_compressed(os.path.join(OUT, w.name + ".npz"), **fdtd_record(run_ref(w, solver=RefFdtd), w))
         print("wrote", w.name, flush=True)
     if skip_large:
         return
