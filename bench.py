@@ -40,7 +40,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=20)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="heterogeneous",
-                   choices=["heterogeneous", "plain", "precision", "batched", "served"])
+                   choices=["heterogeneous", "plain", "precision", "batched", "served", "fdtd"])
     p.add_argument("--instances", type=int, default=256, help="batched: number of instances")
     p.add_argument("--requests", type=int, default=200, help="served: number of requests")
     p.add_argument("--rate", type=float, default=200.0, help="served: mean arrivals per second")
@@ -315,6 +315,70 @@ def run_ours(args):
     dist.close()
 
 
+def run_fdtd(args):
+    """The Yee FDTD solver on the 192^3 heterogeneous grid (same materials,
+    source and probes as the TLM default): cell-updates/s of the whole step
+    (sources, monitors, H and E updates, Mur boundary), against the
+    reference's own FdtdSolver on the host cores."""
+    import torch
+    from emsolver_b200 import workloads
+    from emsolver_b200.fdtd import build_fdtd
+    from oracle import RefFdtd, drive
+    w = workloads.heterogeneous(steps=args.warmup + args.steps)
+    s = build_fdtd(w)
+    s.step(args.warmup)
+    ext = torch.cuda.ExternalStream(s.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    e0.record(ext)
+    s.step(args.steps)
+    e1.record(ext)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    s.close()
+    n = w.ncells
+    bytes_step = n * (75 + 24)   # H: E read + H read/write; E: H read + E read/write + masks + lossy coefficients
+    achieved = bytes_step / (ms / args.steps / 1000.0) / 1e9
+    peak, kind = peaks()
+    t0 = time.perf_counter()
+    s2 = build_fdtd(w)
+    s2.step(args.steps)
+    recs = [s2.probe(q) for q in range(len(w.probes_cell))]
+    t1 = time.perf_counter()
+    s2.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        R = RefFdtd()
+        drive.setup(R, w)
+        if w.waveform == 3:
+            R.steps(2, sv=w.sv[:2])
+        done, tc = 0, time.perf_counter()
+        while done < 200 and time.perf_counter() - tc < 20.0:
+            drive.advance(R, w, 5)
+            done += 5
+        dtc = time.perf_counter() - tc
+        cpu = {"value": n * done / dtc, "unit": "cell-updates/s", "cores": max(1, min(16, (os.cpu_count() or 2) - 1)),
+               "kind": "reference", "sample": f"{done} full-grid FDTD steps of {w.nx}x{w.ny}x{w.nz} in {dtc:.1f}s"}
+    line = {"metric": "FDTD cell-updates/s", "value": n * args.steps / (ms / 1000.0), "unit": "cell-updates/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"fdtd heterogeneous {w.nx}x{w.ny}x{w.nz}, {len(w.table)} lossy dielectric boxes",
+                       "cells": n},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": kind, "traffic": None, "algorithmic_bytes_per_step": bytes_step},
+            "cpu_baseline": cpu,
+            "e2e": {"value": n * args.steps / (t1 - t0), "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": w.mat.nbytes / args.steps,
+                    "d2h_bytes_per_step": sum(12 * r[0].size for r in recs) / args.steps, "seconds": t1 - t0},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def sequential_solves(ws):
     """Each instance alone through the plain API, one after the other:
     setup, all steps, port DFT back to the host, free. Returns per-solve
@@ -477,6 +541,8 @@ def main():
         run_batched(args)
     elif args.workload == "served":
         run_served(args)
+    elif args.workload == "fdtd":
+        run_fdtd(args)
     else:
         run_ours(args)
 

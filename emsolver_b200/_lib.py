@@ -153,6 +153,7 @@ SIGNATURES = {
     "fdtd_step": (_st, [_h, C.c_int]),
     "fdtd_run": (_st, [_h]),
     "fdtd_current_step": (C.c_int, [_h]),
+    "fdtd_get_stream": (_st, [_h, _P(C.c_void_p)]),
     "fdtd_timestep": (C.c_float, [_h]),
     "fdtd_get_field": (_st, [_h, C.c_int, _P(C.c_float), C.c_size_t, _P(C.c_size_t)]),
     "fdtd_get_probe": (_st, [_h, C.c_int, _P(C.c_float), _P(C.c_float), _P(C.c_float), C.c_int, _P(C.c_int)]),

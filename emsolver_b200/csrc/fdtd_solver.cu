@@ -268,19 +268,46 @@ __global__ void __launch_bounds__(256) energyPartialKernel(Fields f, long long n
         part[blockIdx.x] = t;
     }
 }
-__global__ void energyFinalKernel(const double *part, int n, double *out)
+__global__ void __launch_bounds__(256) energyFinalKernel(const double *part, int n, double *out)
 {
+    __shared__ double red[8];
     double t = 0.0;
-    for (int b = 0; b < n; ++b) t += part[b];
-    *out = t;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) t += part[b];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        *out = s;
+    }
 }
 
 // ---- 3. H update (FdtdSolver.cpp:449-484) ---------------------------------
-__global__ void __launch_bounds__(256) updateHKernel(Fields f, Dims d, float ch)
+// One thread per Yee cell (i, j, k) of the (nx+1) x (ny+1) x (nz+1) index
+// box, flattened (x fastest) so that no block is padded per row.
+struct Box
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    if (i > d.nx) return;
+    unsigned total;
+    tlmk::FastDiv divX, divY;  // by nx + 1 and ny + 1
+};
+__device__ __forceinline__ bool boxCell(const Box &b, const Dims &d, int *i, int *j, int *k)
+{
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.total) return false;
+    const unsigned r = tlmk::fastDiv(t, b.divX);
+    *i = (int)(t - r * (unsigned)(d.nx + 1));
+    const unsigned kk = tlmk::fastDiv(r, b.divY);
+    *j = (int)(r - kk * (unsigned)(d.ny + 1));
+    *k = (int)kk;
+    return true;
+}
+
+__global__ void __launch_bounds__(256) updateHKernel(Fields f, Dims d, Box b, float ch)
+{
+    int i, j, k;
+    if (!boxCell(b, d, &i, &j, &k)) return;
     const float *Ex = f.E[0], *Ey = f.E[1], *Ez = f.E[2];
     if (j < d.ny && k < d.nz)
     {
@@ -360,11 +387,10 @@ __global__ void murSnapKernel(Fields f, Dims d, Mur m)
 }
 
 // E update of the interior edges (FdtdSolver.cpp:487-555).
-__global__ void __launch_bounds__(256) updateEKernel(Fields f, Dims d, float cb0)
+__global__ void __launch_bounds__(256) updateEKernel(Fields f, Dims d, Box b, float cb0)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    if (i > d.nx) return;
+    int i, j, k;
+    if (!boxCell(b, d, &i, &j, &k)) return;
     const float *Hx = f.H[0], *Hy = f.H[1], *Hz = f.H[2];
     if (i < d.nx && j >= 1 && j < d.ny && k >= 1 && k < d.nz)
     {
@@ -812,7 +838,7 @@ tlm_status launchStep(fdtd_solver *h, int n)
         const double eta = (double)tlmh::eta0_f32();
         fdk::energyPartialKernel<<<h->nEpart, 256, 0, h->stream>>>(f, h->len[0], h->len[1], h->len[2], h->len[3],
                                                                   h->len[4], h->len[5], eta * eta, h->dEpart);
-        fdk::energyFinalKernel<<<1, 1, 0, h->stream>>>(h->dEpart, h->nEpart, h->dEhist + n / 16);
+        fdk::energyFinalKernel<<<1, 256, 0, h->stream>>>(h->dEpart, h->nEpart, h->dEhist + n / 16);
     }
     if (h->cfg.record_every > 0 && (n % h->cfg.record_every) == 0)
     {
@@ -845,12 +871,16 @@ tlm_status launchStep(fdtd_solver *h, int n)
         s.framesUsed = need;
     }
     // 3. H, 4. Mur snapshot, E, Mur
-    const dim3 grid((d.nx + 1 + 127) / 128, d.ny + 1, d.nz + 1);
-    fdk::updateHKernel<<<grid, 128, 0, h->stream>>>(f, d, h->ch);
+    fdk::Box box;
+    box.total = (unsigned)((long long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1));
+    box.divX = tlmk::makeFastDiv((unsigned)(d.nx + 1));
+    box.divY = tlmk::makeFastDiv((unsigned)(d.ny + 1));
+    const unsigned grid = (box.total + 255) / 256;
+    fdk::updateHKernel<<<grid, 256, 0, h->stream>>>(f, d, box, h->ch);
     long long snapItems = 0;
     for (int F = 0; F < 6; ++F) snapItems += (long long)h->mur.n1[F] * h->mur.n2[F];
     fdk::murSnapKernel<<<(unsigned)((snapItems + 255) / 256), 256, 0, h->stream>>>(f, d, h->mur);
-    fdk::updateEKernel<<<grid, 128, 0, h->stream>>>(f, d, h->cb0);
+    fdk::updateEKernel<<<grid, 256, 0, h->stream>>>(f, d, box, h->cb0);
     long long aItems = 0, bItems = 0;
     for (int F = 0; F < 3; ++F) aItems += (long long)h->mur.n1[F] * h->mur.n2[F];
     for (int F = 3; F < 6; ++F) bItems += (long long)h->mur.n1[F] * h->mur.n2[F];
@@ -932,6 +962,8 @@ tlm_status fdtd_setup(fdtd_handle h, const tlm_grid *grid, const uint8_t *mat, s
     if (!grid || !mat || !cfg || (n_table > 0 && !table) || n_table < 0)
         return h->fail(TLM_EINVAL, "null grid, material map, table or config");
     if (grid->nx < 2 || grid->ny < 2 || grid->nz < 2) return h->fail(TLM_EINVAL, "grid must be at least 2 cells per axis");
+    if ((long long)(grid->nx + 1) * (grid->ny + 1) * (grid->nz + 1) >= (1LL << 31))
+        return h->fail(TLM_EINVAL, "grid too large");
     if (!(grid->dl > 0.0f)) return h->fail(TLM_EINVAL, "dl must be positive");
     const size_t n = (size_t)grid->nx * grid->ny * grid->nz;
     if (n_cells != n) return h->fail(TLM_EINVAL, "material map does not match the grid");
@@ -1171,6 +1203,16 @@ tlm_status fdtd_run(fdtd_handle h)
 }
 
 int fdtd_current_step(fdtd_handle h) { return h ? h->curStep : 0; }
+tlm_status fdtd_get_stream(fdtd_handle h, void **stream)
+{
+    if (!h || !stream)
+    {
+        g_fdtdErr = "null handle or output";
+        return TLM_EINVAL;
+    }
+    *stream = (void *)h->stream;
+    return TLM_OK;
+}
 float fdtd_timestep(fdtd_handle h) { return h ? h->dt : 0.0f; }
 
 tlm_status fdtd_get_field(fdtd_handle h, int which, float *out, size_t cap, size_t *n)

@@ -93,6 +93,11 @@ class FdtdSolver:
     def timestep(self) -> float:
         return self._L.fdtd_timestep(self._h)
 
+    def stream(self) -> int:
+        st = C.c_void_p()
+        self._c(self._L.fdtd_get_stream(self._h, C.byref(st)))
+        return st.value or 0
+
     # -- state and records
     def field(self, which) -> np.ndarray:
         w = FIELDS.index(which) if isinstance(which, str) else int(which)

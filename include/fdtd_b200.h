@@ -57,6 +57,8 @@ TLM_API tlm_status fdtd_step(fdtd_handle h, int n_steps);
 /* run (FdtdSolver.cpp:361-380): steps up to total_steps. */
 TLM_API tlm_status fdtd_run(fdtd_handle h);
 TLM_API int fdtd_current_step(fdtd_handle h);
+/* The CUDA stream (cudaStream_t) the handle's work is queued on. */
+TLM_API tlm_status fdtd_get_stream(fdtd_handle h, void **stream);
 TLM_API float fdtd_timestep(fdtd_handle h);
 
 /* Field component `which` (0..5 = Ex Ey Ez Hx Hy Hz) in its Yee layout;
