@@ -47,6 +47,14 @@ struct Dims
     __host__ __device__ long long iHx(int i, int j, int k) const { return ((long long)k * ny + j) * (nx + 1) + i; }
     __host__ __device__ long long iHy(int i, int j, int k) const { return ((long long)k * (ny + 1) + j) * nx + i; }
     __host__ __device__ long long iHz(int i, int j, int k) const { return ((long long)k * ny + j) * nx + i; }
+    // 32-bit forms for the update sweeps: setup refuses grids whose
+    // (nx+1)(ny+1)(nz+1) index box reaches 2^31, so every component fits.
+    __device__ int jEx(int i, int j, int k) const { return (k * (ny + 1) + j) * nx + i; }
+    __device__ int jEy(int i, int j, int k) const { return (k * ny + j) * (nx + 1) + i; }
+    __device__ int jEz(int i, int j, int k) const { return (k * (ny + 1) + j) * (nx + 1) + i; }
+    __device__ int jHx(int i, int j, int k) const { return (k * ny + j) * (nx + 1) + i; }
+    __device__ int jHy(int i, int j, int k) const { return (k * (ny + 1) + j) * nx + i; }
+    __device__ int jHz(int i, int j, int k) const { return (k * ny + j) * nx + i; }
 };
 
 struct Fields
@@ -86,9 +94,10 @@ __global__ void injectKernel(Fields f, const long long *__restrict__ edge, const
     const long long code = edge[e];
     const int c = (int)(code >> 60);
     const long long idx = code & ((1LL << 60) - 1);
-    float v = f.E[c][idx];
+    float *E = c == 0 ? f.E[0] : c == 1 ? f.E[1] : f.E[2];
+    float v = E[idx];
     for (int t = off[e]; t < off[e + 1]; ++t) v = v + (-0.25f * amps[t]) * sv;
-    f.E[c][idx] = v;
+    E[idx] = v;
 }
 
 // ---- 2. monitors ----------------------------------------------------------
@@ -239,24 +248,37 @@ __global__ void __launch_bounds__(256) monitorKernel(const MonArgs a)
 }
 
 // Energy (FdtdSolver.cpp:836-870): sum E^2 + eta0^2 sum H^2 in FP64, block
-// partials in a fixed order.
+// partials in a fixed order. Every component is swept as 16-byte vectors
+// (device allocations are 256-byte aligned), four in flight per thread.
+__device__ __forceinline__ double sumSquares(const float *arr, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const float4 *a4 = reinterpret_cast<const float4 *>(arr);
+    const long long n4 = n >> 2;
+    double acc = 0.0;
+#pragma unroll 4
+    for (long long i = t0; i < n4; i += stride)
+    {
+        const float4 v = a4[i];
+        const double x = v.x, y = v.y, z = v.z, w = v.w;
+        acc += ((x * x + y * y) + z * z) + w * w;
+    }
+    const long long r = (n4 << 2) + t0;
+    if (r < n)
+    {
+        const double x = arr[r];
+        acc += x * x;
+    }
+    return acc;
+}
 __global__ void __launch_bounds__(256) energyPartialKernel(Fields f, long long nE0, long long nE1, long long nE2,
                                                            long long nH0, long long nH1, long long nH2,
                                                            double eta2, double *part)
 {
     __shared__ double red[8];
-    const long long lens[6] = { nE0, nE1, nE2, nH0, nH1, nH2 };
-    double se = 0.0, sh = 0.0;
-    for (int a = 0; a < 6; ++a)
-    {
-        const float *arr = a < 3 ? f.E[a] : f.H[a - 3];
-        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < lens[a];
-             i += (long long)gridDim.x * blockDim.x)
-        {
-            const double v = (double)arr[i];
-            if (a < 3) se += v * v; else sh += v * v;
-        }
-    }
+    const double se = (sumSquares(f.E[0], nE0) + sumSquares(f.E[1], nE1)) + sumSquares(f.E[2], nE2);
+    const double sh = (sumSquares(f.H[0], nH0) + sumSquares(f.H[1], nH1)) + sumSquares(f.H[2], nH2);
     double s = se + sh * eta2;
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -284,52 +306,7 @@ __global__ void __launch_bounds__(256) energyFinalKernel(const double *part, int
     }
 }
 
-// ---- 3. H update (FdtdSolver.cpp:449-484) ---------------------------------
-// One thread per Yee cell (i, j, k) of the (nx+1) x (ny+1) x (nz+1) index
-// box, flattened (x fastest) so that no block is padded per row.
-struct Box
-{
-    unsigned total;
-    tlmk::FastDiv divX, divY;  // by nx + 1 and ny + 1
-};
-__device__ __forceinline__ bool boxCell(const Box &b, const Dims &d, int *i, int *j, int *k)
-{
-    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= b.total) return false;
-    const unsigned r = tlmk::fastDiv(t, b.divX);
-    *i = (int)(t - r * (unsigned)(d.nx + 1));
-    const unsigned kk = tlmk::fastDiv(r, b.divY);
-    *j = (int)(r - kk * (unsigned)(d.ny + 1));
-    *k = (int)kk;
-    return true;
-}
-
-__global__ void __launch_bounds__(256) updateHKernel(Fields f, Dims d, Box b, float ch)
-{
-    int i, j, k;
-    if (!boxCell(b, d, &i, &j, &k)) return;
-    const float *Ex = f.E[0], *Ey = f.E[1], *Ez = f.E[2];
-    if (j < d.ny && k < d.nz)
-    {
-        const long long q = d.iHx(i, j, k);
-        f.H[0][q] = f.H[0][q] - ch * ((Ez[d.iEz(i, j + 1, k)] - Ez[d.iEz(i, j, k)]) -
-                                      (Ey[d.iEy(i, j, k + 1)] - Ey[d.iEy(i, j, k)]));
-    }
-    if (i < d.nx && k < d.nz)
-    {
-        const long long q = d.iHy(i, j, k);
-        f.H[1][q] = f.H[1][q] - ch * ((Ex[d.iEx(i, j, k + 1)] - Ex[d.iEx(i, j, k)]) -
-                                      (Ez[d.iEz(i + 1, j, k)] - Ez[d.iEz(i, j, k)]));
-    }
-    if (i < d.nx && j < d.ny)
-    {
-        const long long q = d.iHz(i, j, k);
-        f.H[2][q] = f.H[2][q] - ch * ((Ey[d.iEy(i + 1, j, k)] - Ey[d.iEy(i, j, k)]) -
-                                      (Ex[d.iEx(i, j + 1, k)] - Ex[d.iEx(i, j, k)]));
-    }
-}
-
-// ---- 4. Mur snapshot, E update, Mur boundary ------------------------------
+// ---- Mur boundary state ----------------------------------------------------
 // Face planes: 0 x-faces Ey, 1 x-faces Ez, 2 y-faces Ex, 3 y-faces Ez,
 // 4 z-faces Ex, 5 z-faces Ey. Plane position (q1, q2) over the two other
 // axes; layers 0, 1, N-1, N along the face normal (N = grid size on it).
@@ -352,96 +329,217 @@ __device__ __forceinline__ long long murIndex(const Dims &d, int F, int L, int q
     default: return d.iEy(q1, q2, L);
     }
 }
-__device__ __forceinline__ int murComp(int F) { return (F == 0 || F == 5) ? 1 : (F == 1 || F == 3) ? 2 : 0; }
+__device__ __forceinline__ float *murField(const Fields &f, int F)
+{
+    return (F == 0 || F == 5) ? f.E[1] : (F == 1 || F == 3) ? f.E[2] : f.E[0];
+}
 __device__ __forceinline__ int murN(const Dims &d, int F) { return F < 2 ? d.nx : F < 4 ? d.ny : d.nz; }
 
-// Map a flat item index over planes [F0, F0 + nplanes) to (F, q1, q2).
-__device__ __forceinline__ bool murItem(const Mur &m, int F0, int nplanes, long long t, int *F, int *q1, int *q2)
-{
-    for (int p = F0; p < F0 + nplanes; ++p)
-    {
-        const long long n = (long long)m.n1[p] * m.n2[p];
-        if (t < n)
-        {
-            *F = p;
-            *q1 = (int)(t % m.n1[p]);
-            *q2 = (int)(t / m.n1[p]);
-            return true;
-        }
-        t -= n;
-    }
-    return false;
-}
-
-__global__ void murSnapKernel(Fields f, Dims d, Mur m)
+// A flat item index over planes [F0, F0 + NP) resolved to its plane F, the
+// position (q1, q2), and that position's first layer in `snap` (with the
+// layer stride pl). Unrolled so that the plane tables stay in parameter space.
+struct MurAt
 {
     int F, q1, q2;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (!murItem(m, 0, 6, t, &F, &q1, &q2)) return;
-    const int N = murN(d, F);
-    const float *E = f.E[murComp(F)];
-    const long long pl = (long long)m.n1[F] * m.n2[F];
-    float *s = m.snap + m.off[F] + (long long)q2 * m.n1[F] + q1;
-    const int layers[4] = { 0, 1, N - 1, N };
-    for (int L = 0; L < 4; ++L) s[L * pl] = E[murIndex(d, F, layers[L], q1, q2)];
+    long long pl;
+    float *s;
+};
+template <int F0, int NP>
+__device__ __forceinline__ bool murItem(const Mur &m, long long t, MurAt *a)
+{
+    bool found = false;
+#pragma unroll
+    for (int p = F0; p < F0 + NP; ++p)
+    {
+        const long long n = (long long)m.n1[p] * m.n2[p];
+        if (!found)
+        {
+            if (t < n)
+            {
+                found = true;
+                a->F = p;
+                a->q1 = (int)(t % m.n1[p]);
+                a->q2 = (int)(t / m.n1[p]);
+                a->pl = n;
+                a->s = m.snap + m.off[p] + (long long)a->q2 * m.n1[p] + a->q1;
+            }
+            else
+                t -= n;
+        }
+    }
+    return found;
 }
 
-// E update of the interior edges (FdtdSolver.cpp:487-555).
+// Copy of layers 0, 1, N-1, N of every face plane, taken before the E
+// update (it runs as extra blocks of the H update, which leaves E unchanged).
+__device__ __forceinline__ void murSnapItem(const Fields &f, const Dims &d, const Mur &m, long long t)
+{
+    MurAt a;
+    if (!murItem<0, 6>(m, t, &a)) return;
+    const int N = murN(d, a.F);
+    const float *E = murField(f, a.F);
+    const float e0 = E[murIndex(d, a.F, 0, a.q1, a.q2)], e1 = E[murIndex(d, a.F, 1, a.q1, a.q2)];
+    const float e2 = E[murIndex(d, a.F, N - 1, a.q1, a.q2)], e3 = E[murIndex(d, a.F, N, a.q1, a.q2)];
+    a.s[0] = e0;
+    a.s[a.pl] = e1;
+    a.s[2 * a.pl] = e2;
+    a.s[3 * a.pl] = e3;
+}
+
+// ---- 3. H update (FdtdSolver.cpp:449-484) and the Mur snapshot ------------
+// One thread per Yee cell (i, j, k) of the (nx+1) x (ny+1) x (nz+1) index
+// box, flattened (x fastest) so that no block is padded per row.
+struct Box
+{
+    unsigned total;
+    tlmk::FastDiv divX, divY;  // by nx + 1 and ny + 1
+};
+__device__ __forceinline__ bool boxCell(const Box &b, const Dims &d, int *i, int *j, int *k)
+{
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.total) return false;
+    const unsigned r = tlmk::fastDiv(t, b.divX);
+    *i = (int)(t - r * (unsigned)(d.nx + 1));
+    const unsigned kk = tlmk::fastDiv(r, b.divY);
+    *j = (int)(r - kk * (unsigned)(d.ny + 1));
+    *k = (int)kk;
+    return true;
+}
+
+// Every load of the thread is issued before its first store (the three H
+// components share E operands: 9 distinct E loads and 3 H loads), so one
+// memory round trip covers the cell. Operation order per component is the
+// reference's.
+__global__ void __launch_bounds__(256) updateHKernel(Fields f, Dims d, Box b, float ch, Mur m, unsigned hBlocks)
+{
+    if (blockIdx.x >= hBlocks)
+    {
+        murSnapItem(f, d, m, (long long)(blockIdx.x - hBlocks) * blockDim.x + threadIdx.x);
+        return;
+    }
+    int i, j, k;
+    if (!boxCell(b, d, &i, &j, &k)) return;
+    const float *__restrict__ Ex = f.E[0];
+    const float *__restrict__ Ey = f.E[1];
+    const float *__restrict__ Ez = f.E[2];
+    const bool ax = j < d.ny && k < d.nz, ay = i < d.nx && k < d.nz, az = i < d.nx && j < d.ny;
+    float hx = 0.f, hy = 0.f, hz = 0.f;
+    float ez0 = 0.f, ezj = 0.f, ezi = 0.f, ey0 = 0.f, eyk = 0.f, eyi = 0.f, ex0 = 0.f, exk = 0.f, exj = 0.f;
+    const int qx = ax ? d.jHx(i, j, k) : 0, qy = ay ? d.jHy(i, j, k) : 0, qz = az ? d.jHz(i, j, k) : 0;
+    if (ax)
+    {
+        hx = f.H[0][qx];
+        ezj = Ez[d.jEz(i, j + 1, k)];
+        eyk = Ey[d.jEy(i, j, k + 1)];
+    }
+    if (ay)
+    {
+        hy = f.H[1][qy];
+        exk = Ex[d.jEx(i, j, k + 1)];
+        ezi = Ez[d.jEz(i + 1, j, k)];
+    }
+    if (az)
+    {
+        hz = f.H[2][qz];
+        eyi = Ey[d.jEy(i + 1, j, k)];
+        exj = Ex[d.jEx(i, j + 1, k)];
+    }
+    if (ax || ay) ez0 = Ez[d.jEz(i, j, k)];
+    if (ax || az) ey0 = Ey[d.jEy(i, j, k)];
+    if (ay || az) ex0 = Ex[d.jEx(i, j, k)];
+    if (ax) f.H[0][qx] = hx - ch * ((ezj - ez0) - (eyk - ey0));
+    if (ay) f.H[1][qy] = hy - ch * ((exk - ex0) - (ezi - ez0));
+    if (az) f.H[2][qz] = hz - ch * ((eyi - ey0) - (exj - ex0));
+}
+
+// E update of the interior edges (FdtdSolver.cpp:487-555). As for H, all
+// loads (masks, 6 distinct H values shared by the three components, the
+// edges' own E and lossy coefficients) come before the stores.
 __global__ void __launch_bounds__(256) updateEKernel(Fields f, Dims d, Box b, float cb0)
 {
     int i, j, k;
     if (!boxCell(b, d, &i, &j, &k)) return;
-    const float *Hx = f.H[0], *Hy = f.H[1], *Hz = f.H[2];
-    if (i < d.nx && j >= 1 && j < d.ny && k >= 1 && k < d.nz)
+    const float *__restrict__ Hx = f.H[0];
+    const float *__restrict__ Hy = f.H[1];
+    const float *__restrict__ Hz = f.H[2];
+    const bool ix = i >= 1 && i < d.nx, jy = j >= 1 && j < d.ny, kz = k >= 1 && k < d.nz;
+    const bool ax = i < d.nx && jy && kz, ay = ix && j < d.ny && kz, az = ix && jy && k < d.nz;
+    const bool lossy = f.ca[0] != nullptr;
+    const int qx = ax ? d.jEx(i, j, k) : 0, qy = ay ? d.jEy(i, j, k) : 0, qz = az ? d.jEz(i, j, k) : 0;
+    uint8_t mx = 0, my = 0, mz = 0;
+    float ex = 0.f, ey = 0.f, ez = 0.f, cax = 0.f, cbx = 0.f, cay = 0.f, cby = 0.f, caz = 0.f, cbz = 0.f;
+    float hz0 = 0.f, hzj = 0.f, hzi = 0.f, hy0 = 0.f, hyk = 0.f, hyi = 0.f, hx0 = 0.f, hxk = 0.f, hxj = 0.f;
+    if (ax)
     {
-        const long long q = d.iEx(i, j, k);
-        if (!f.mE[0][q])
-            f.E[0][q] = 0.0f;
-        else
+        mx = f.mE[0][qx];
+        ex = f.E[0][qx];
+        hzj = Hz[d.jHz(i, j - 1, k)];
+        hyk = Hy[d.jHy(i, j, k - 1)];
+        if (lossy)
         {
-            const float curl = (Hz[d.iHz(i, j, k)] - Hz[d.iHz(i, j - 1, k)]) - (Hy[d.iHy(i, j, k)] - Hy[d.iHy(i, j, k - 1)]);
-            f.E[0][q] = f.ca[0] ? f.ca[0][q] * f.E[0][q] + f.cb[0][q] * curl : f.E[0][q] + cb0 * curl;
+            cax = f.ca[0][qx];
+            cbx = f.cb[0][qx];
         }
     }
-    if (i >= 1 && i < d.nx && j < d.ny && k >= 1 && k < d.nz)
+    if (ay)
     {
-        const long long q = d.iEy(i, j, k);
-        if (!f.mE[1][q])
-            f.E[1][q] = 0.0f;
-        else
+        my = f.mE[1][qy];
+        ey = f.E[1][qy];
+        hxk = Hx[d.jHx(i, j, k - 1)];
+        hzi = Hz[d.jHz(i - 1, j, k)];
+        if (lossy)
         {
-            const float curl = (Hx[d.iHx(i, j, k)] - Hx[d.iHx(i, j, k - 1)]) - (Hz[d.iHz(i, j, k)] - Hz[d.iHz(i - 1, j, k)]);
-            f.E[1][q] = f.ca[1] ? f.ca[1][q] * f.E[1][q] + f.cb[1][q] * curl : f.E[1][q] + cb0 * curl;
+            cay = f.ca[1][qy];
+            cby = f.cb[1][qy];
         }
     }
-    if (i >= 1 && i < d.nx && j >= 1 && j < d.ny && k < d.nz)
+    if (az)
     {
-        const long long q = d.iEz(i, j, k);
-        if (!f.mE[2][q])
-            f.E[2][q] = 0.0f;
-        else
+        mz = f.mE[2][qz];
+        ez = f.E[2][qz];
+        hyi = Hy[d.jHy(i - 1, j, k)];
+        hxj = Hx[d.jHx(i, j - 1, k)];
+        if (lossy)
         {
-            const float curl = (Hy[d.iHy(i, j, k)] - Hy[d.iHy(i - 1, j, k)]) - (Hx[d.iHx(i, j, k)] - Hx[d.iHx(i, j - 1, k)]);
-            f.E[2][q] = f.ca[2] ? f.ca[2][q] * f.E[2][q] + f.cb[2][q] * curl : f.E[2][q] + cb0 * curl;
+            caz = f.ca[2][qz];
+            cbz = f.cb[2][qz];
         }
+    }
+    if (ax || ay) hz0 = Hz[d.jHz(i, j, k)];
+    if (ax || az) hy0 = Hy[d.jHy(i, j, k)];
+    if (ay || az) hx0 = Hx[d.jHx(i, j, k)];
+    if (ax)
+    {
+        const float curl = (hz0 - hzj) - (hy0 - hyk);
+        f.E[0][qx] = !mx ? 0.0f : lossy ? cax * ex + cbx * curl : ex + cb0 * curl;
+    }
+    if (ay)
+    {
+        const float curl = (hx0 - hxk) - (hz0 - hzi);
+        f.E[1][qy] = !my ? 0.0f : lossy ? cay * ey + cby * curl : ey + cb0 * curl;
+    }
+    if (az)
+    {
+        const float curl = (hy0 - hyi) - (hx0 - hxj);
+        f.E[2][qz] = !mz ? 0.0f : lossy ? caz * ez + cbz * curl : ez + cb0 * curl;
     }
 }
 
 // Mur on planes [F0, F0 + 3): per plane position the low face, then the high
 // face (FdtdSolver.cpp:624-670): E_b = E_1(old) + cMur (E_1(new) - E_b(old)).
-__global__ void murApplyKernel(Fields f, Dims d, Mur m, int F0)
+template <int F0>
+__global__ void murApplyKernel(Fields f, Dims d, Mur m)
 {
-    int F, q1, q2;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (!murItem(m, F0, 3, t, &F, &q1, &q2)) return;
-    const int N = murN(d, F);
-    float *E = f.E[murComp(F)];
-    const long long pl = (long long)m.n1[F] * m.n2[F];
-    const float *s = m.snap + m.off[F] + (long long)q2 * m.n1[F] + q1;
-    const long long b0 = murIndex(d, F, 0, q1, q2), b1 = murIndex(d, F, 1, q1, q2);
-    E[b0] = s[1 * pl] + m.cMur * (E[b1] - s[0]);
-    const long long bN = murIndex(d, F, N, q1, q2), bN1 = murIndex(d, F, N - 1, q1, q2);
-    E[bN] = s[2 * pl] + m.cMur * (E[bN1] - s[3 * pl]);
+    MurAt a;
+    if (!murItem<F0, 3>(m, (long long)blockIdx.x * blockDim.x + threadIdx.x, &a)) return;
+    const int N = murN(d, a.F);
+    float *E = murField(f, a.F);
+    const long long b0 = murIndex(d, a.F, 0, a.q1, a.q2), b1 = murIndex(d, a.F, 1, a.q1, a.q2);
+    const long long bN = murIndex(d, a.F, N, a.q1, a.q2), bN1 = murIndex(d, a.F, N - 1, a.q1, a.q2);
+    const float s0 = a.s[0], s1 = a.s[a.pl], s2 = a.s[2 * a.pl], s3 = a.s[3 * a.pl];
+    const float e1 = E[b1], eN1 = E[bN1];
+    E[b0] = s1 + m.cMur * (e1 - s0);
+    E[bN] = s2 + m.cMur * (eN1 - s3);
 }
 
 } // namespace fdk
@@ -876,16 +974,16 @@ tlm_status launchStep(fdtd_solver *h, int n)
     box.divX = tlmk::makeFastDiv((unsigned)(d.nx + 1));
     box.divY = tlmk::makeFastDiv((unsigned)(d.ny + 1));
     const unsigned grid = (box.total + 255) / 256;
-    fdk::updateHKernel<<<grid, 256, 0, h->stream>>>(f, d, box, h->ch);
     long long snapItems = 0;
     for (int F = 0; F < 6; ++F) snapItems += (long long)h->mur.n1[F] * h->mur.n2[F];
-    fdk::murSnapKernel<<<(unsigned)((snapItems + 255) / 256), 256, 0, h->stream>>>(f, d, h->mur);
+    const unsigned snapBlocks = (unsigned)((snapItems + 255) / 256);
+    fdk::updateHKernel<<<grid + snapBlocks, 256, 0, h->stream>>>(f, d, box, h->ch, h->mur, grid);
     fdk::updateEKernel<<<grid, 256, 0, h->stream>>>(f, d, box, h->cb0);
     long long aItems = 0, bItems = 0;
     for (int F = 0; F < 3; ++F) aItems += (long long)h->mur.n1[F] * h->mur.n2[F];
     for (int F = 3; F < 6; ++F) bItems += (long long)h->mur.n1[F] * h->mur.n2[F];
-    fdk::murApplyKernel<<<(unsigned)((aItems + 255) / 256), 256, 0, h->stream>>>(f, d, h->mur, 0);
-    fdk::murApplyKernel<<<(unsigned)((bItems + 255) / 256), 256, 0, h->stream>>>(f, d, h->mur, 3);
+    fdk::murApplyKernel<0><<<(unsigned)((aItems + 255) / 256), 256, 0, h->stream>>>(f, d, h->mur);
+    fdk::murApplyKernel<3><<<(unsigned)((bItems + 255) / 256), 256, 0, h->stream>>>(f, d, h->mur);
     return h->cuda(cudaGetLastError(), "FDTD step launch");
 }
 
@@ -1067,6 +1165,8 @@ tlm_status fdtd_setup(fdtd_handle h, const tlm_grid *grid, const uint8_t *mat, s
     for (int c = 0; c < 6; ++c)
     {
         FD_TRY(alloc(h, &h->dField[c], (size_t)h->len[c] * 4));
+        if (reinterpret_cast<uintptr_t>(h->dField[c]) & 15)  // the energy sweep reads 16-byte vectors
+            return h->fail(TLM_ECUDA, "field allocation not 16-byte aligned");
         FD_CU(h, cudaMemsetAsync(h->dField[c], 0, (size_t)h->len[c] * 4, h->stream));
     }
     for (int c = 0; c < 3; ++c)
