@@ -1,4 +1,5 @@
-"""ctypes binding of the in-tree C ABI (include/tlm_b200.h).
+"""ctypes binding of the in-tree C ABI (include/tlm_b200.h, fdtd_b200.h,
+emsim_b200.h).
 
 The library is loaded from this package directory. There is no fallback: if
 ``libtlm_b200.so`` is missing or cannot be loaded, importing the binding
@@ -43,6 +44,61 @@ class ConfigC(C.Structure):
                 ("pulse_scale", C.c_float), ("steps_per_launch", C.c_int),
                 ("kernel_variant", C.c_int), ("rounding", C.c_int), ("general_tiles", C.c_int),
                 ("surface_monitors", C.c_int)]
+
+
+class EmsimFaceC(C.Structure):
+    _fields_ = [("air_cell", C.c_int32), ("center", C.c_float * 3), ("axis", C.c_int8), ("sign", C.c_int8)]
+
+
+class EmsimToolbarC(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("solver", "excitation", "waveform", "currents", "db_range", "gpu",
+                                       "show_model", "db_scale", "plane_on", "mesh_on")]
+
+
+class EmsimObjectC(C.Structure):
+    _fields_ = [("kind", C.c_int), ("name", C.c_char_p), ("position", C.c_float * 3), ("rot_deg", C.c_float * 3),
+                ("dielectric", C.c_int), ("epsr", C.c_float), ("sigma", C.c_float),
+                ("design_freq_hz", C.c_double), ("is_stl", C.c_int), ("n_stl_verts", C.c_uint32),
+                ("stl_verts", C.POINTER(C.c_float)), ("n_stl_idx", C.c_uint32), ("stl_idx", C.POINTER(C.c_int32)),
+                ("n_params", C.c_uint32)]
+
+
+class EmsimPatternC(C.Structure):
+    _fields_ = [("n_theta", C.c_int), ("n_phi", C.c_int), ("n_u", C.c_uint32), ("U", C.POINTER(C.c_float)),
+                ("u_max", C.c_float), ("directivity", C.c_float), ("peak_theta_deg", C.c_float),
+                ("peak_phi_deg", C.c_float)]
+
+
+class EmsimResultC(C.Structure):
+    _fields_ = [("n_faces", C.c_uint32), ("faces", C.POINTER(EmsimFaceC)),
+                ("n_face_vals", C.c_uint32), ("face_vals", C.POINTER(C.c_float)), ("face_dl", C.c_float),
+                ("n_tri_v", C.c_uint32), ("tri_v", C.POINTER(C.c_float)),
+                ("n_tri_idx", C.c_uint32), ("tri_idx", C.POINTER(C.c_int32)),
+                ("n_tri_mag", C.c_uint32), ("tri_mag", C.POINTER(C.c_float)),
+                ("n_wire_pts", C.c_uint32), ("wire_pts", C.POINTER(C.c_float)),
+                ("n_wire_mag", C.c_uint32), ("wire_mag", C.POINTER(C.c_float)),
+                ("has_plane", C.c_int), ("plane_grid", Grid), ("plane_axis", C.c_int), ("plane_index", C.c_int),
+                ("plane_n1", C.c_int), ("plane_n2", C.c_int),
+                ("n_plane_vals", C.c_uint32), ("plane_vals", C.POINTER(C.c_float)),
+                ("has_pattern", C.c_int), ("pattern", EmsimPatternC), ("pat_center", C.c_float * 3),
+                ("pat_scale", C.c_float), ("domain_lo", C.c_float * 3), ("domain_hi", C.c_float * 3),
+                ("domain_visible", C.c_int), ("n_probe_markers", C.c_uint32),
+                ("probe_markers", C.POINTER(C.c_float))]
+
+
+class EmsimCurveC(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("color", C.c_uint32), ("n_x", C.c_uint32), ("x", C.POINTER(C.c_double)),
+                ("n_y", C.c_uint32), ("y", C.POINTER(C.c_double))]
+
+
+class EmsimFrameC(C.Structure):
+    _fields_ = [("step", C.c_int), ("plane_axis", C.c_int), ("plane_index", C.c_int), ("plane_n1", C.c_int),
+                ("plane_n2", C.c_int), ("n_js", C.c_uint32), ("js", C.POINTER(C.c_float)),
+                ("n_plane", C.c_uint32), ("plane", C.POINTER(C.c_float))]
+
+
+class EmsimCaptureC(C.Structure):
+    _fields_ = [("js_dft", C.c_int), ("n_theta", C.c_int), ("n_phi", C.c_int), ("playback", C.c_int)]
 
 
 class BatchTuningC(C.Structure):
@@ -209,6 +265,43 @@ SIGNATURES = {
     "tlm_server_stats": (_st, [_h, _P(ServerStatsC)]),
     "tlm_request_footprint": (_st, [_P(RequestC), _P(C.c_size_t)]),
     "tlm_get_stream": (_st, [_h, _P(C.c_void_p)]),
+    "tlm_get_grid": (_st, [_h, _P(Grid)]),
+    "fdtd_get_grid": (_st, [_h, _P(Grid)]),
+    "emsim_new": (_st, [_P(_h)]),
+    "emsim_load": (_st, [C.c_char_p, _P(_h), C.c_char_p, C.c_size_t]),
+    "emsim_save": (_st, [_h, C.c_char_p]),
+    "emsim_free": (None, [_h]),
+    "emsim_last_error": (C.c_char_p, [_h]),
+    "emsim_file_version": (C.c_int, [_h]),
+    "emsim_setting_count": (C.c_int, [_h]),
+    "emsim_get_setting": (_st, [_h, C.c_int, _P(C.c_char_p), _P(C.c_char_p)]),
+    "emsim_add_setting": (_st, [_h, C.c_char_p, C.c_char_p]),
+    "emsim_clear_settings": (_st, [_h]),
+    "emsim_get_toolbar": (_st, [_h, _P(EmsimToolbarC)]),
+    "emsim_set_toolbar": (_st, [_h, _P(EmsimToolbarC)]),
+    "emsim_object_count": (C.c_int, [_h]),
+    "emsim_get_object": (_st, [_h, C.c_int, _P(EmsimObjectC)]),
+    "emsim_get_object_param": (_st, [_h, C.c_int, C.c_int, _P(C.c_char_p), _P(C.c_double)]),
+    "emsim_add_object": (_st, [_h, _P(EmsimObjectC), _P(C.c_int)]),
+    "emsim_add_object_param": (_st, [_h, C.c_int, C.c_char_p, C.c_double]),
+    "emsim_clear_objects": (_st, [_h]),
+    "emsim_result_default": (None, [_P(EmsimResultC)]),
+    "emsim_get_result": (_st, [_h, _P(EmsimResultC)]),
+    "emsim_set_result": (_st, [_h, _P(EmsimResultC)]),
+    "emsim_page_count": (C.c_int, [_h]),
+    "emsim_get_page": (_st, [_h, C.c_int, _P(C.c_char_p), _P(C.c_char_p), _P(C.c_char_p), _P(C.c_int)]),
+    "emsim_get_curve": (_st, [_h, C.c_int, C.c_int, _P(EmsimCurveC)]),
+    "emsim_add_page": (_st, [_h, C.c_char_p, C.c_char_p, C.c_char_p, _P(C.c_int)]),
+    "emsim_add_curve": (_st, [_h, C.c_int, _P(EmsimCurveC)]),
+    "emsim_clear_pages": (_st, [_h]),
+    "emsim_get_playback": (_st, [_h, _P(C.c_int), _P(Grid), _P(C.c_float), _P(_P(EmsimFaceC)),
+                                 _P(C.c_uint32), _P(C.c_uint32)]),
+    "emsim_set_playback": (_st, [_h, _P(Grid), C.c_float, _P(EmsimFaceC), C.c_uint32]),
+    "emsim_get_frame": (_st, [_h, C.c_uint32, _P(EmsimFrameC)]),
+    "emsim_add_frame": (_st, [_h, _P(EmsimFrameC)]),
+    "emsim_clear_playback": (_st, [_h]),
+    "emsim_from_tlm": (_st, [_h, _h, _P(EmsimCaptureC)]),
+    "emsim_from_fdtd": (_st, [_h, _h, _P(EmsimCaptureC)]),
     "tlm_device_bytes": (_st, [_h, _P(C.c_size_t)]),
     "tlm_set_kernel_timing": (_st, [_h, C.c_int]),
     "tlm_kernel_time": (_st, [_h, _P(C.c_double), _P(C.c_longlong)]),

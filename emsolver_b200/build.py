@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
               "-I" + INCLUDE, "-I" + CSRC]
 CUDA_SOURCES = ["tlm_solver.cu", "tlm_surface.cu", "fdtd_solver.cu", "tlm_noalloc.cu", "tlm_batch.cu", "tlm_server.cu"]
-HOST_SOURCES = ["tlm_host_math.cpp"]
+HOST_SOURCES = ["tlm_host_math.cpp", "emsim_io.cpp"]
 
 LIBS = {
     "libtlm_b200.so": [],
@@ -62,12 +62,13 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     """Compile every library; returns {name: path}. Rebuilds only what changed."""
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "tlm_b200.h")]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + \
+        [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     host_objs = []
     for src in HOST_SOURCES:
         obj = os.path.join(BUILD, src.replace(".cpp", ".o"))
         if force or _stale(obj, deps):
-            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-I" + CSRC,
+            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-I" + CSRC, "-I" + INCLUDE,
                   "-c", os.path.join(CSRC, src), "-o", obj], verbose)
         host_objs.append(obj)
     out = {}

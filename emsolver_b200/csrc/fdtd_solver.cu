@@ -180,7 +180,11 @@ __global__ void __launch_bounds__(256) monitorKernel(const MonArgs a)
         int co[3];
         cellCo(a.probeCell[t], d, co);
         float *o = a.prec + ((long long)a.step * a.nprobes + t) * 3;
-        for (int c = 0; c < 3; ++c) o[c] = ecAt(f, d, co[0], co[1], co[2], c);
+        const float ex = ecAt(f, d, co[0], co[1], co[2], 0), ey = ecAt(f, d, co[0], co[1], co[2], 1);
+        const float ez = ecAt(f, d, co[0], co[1], co[2], 2);
+        o[0] = ex;
+        o[1] = ey;
+        o[2] = ez;
         return;
     }
     t -= a.nprobes;
@@ -1314,6 +1318,14 @@ tlm_status fdtd_get_stream(fdtd_handle h, void **stream)
     return TLM_OK;
 }
 float fdtd_timestep(fdtd_handle h) { return h ? h->dt : 0.0f; }
+
+tlm_status fdtd_get_grid(fdtd_handle h, tlm_grid *grid)
+{
+    FD_TRY(ready(h));
+    if (!grid) return h->fail(TLM_EINVAL, "null output");
+    *grid = h->g;
+    return TLM_OK;
+}
 
 tlm_status fdtd_get_field(fdtd_handle h, int which, float *out, size_t cap, size_t *n)
 {

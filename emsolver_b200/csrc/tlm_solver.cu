@@ -1199,6 +1199,15 @@ tlm_status tlm_timestep(tlm_handle h, float *dt)
     return TLM_OK;
 }
 
+tlm_status tlm_get_grid(tlm_handle h, tlm_grid *grid)
+{
+    TLM_TRY(checkHandle(h));
+    if (!h->configured) return h->fail(TLM_ESTATE, "tlm_setup has not been called");
+    if (!grid) return h->fail(TLM_EINVAL, "null output");
+    *grid = h->g;
+    return TLM_OK;
+}
+
 int tlm_probe_count(tlm_handle h) { return h ? (int)h->probeCells.size() : 0; }
 int tlm_port_count(tlm_handle h) { return h ? (int)h->ports.size() : 0; }
 

@@ -60,6 +60,8 @@ TLM_API int fdtd_current_step(fdtd_handle h);
 /* The CUDA stream (cudaStream_t) the handle's work is queued on. */
 TLM_API tlm_status fdtd_get_stream(fdtd_handle h, void **stream);
 TLM_API float fdtd_timestep(fdtd_handle h);
+/* The grid given to fdtd_setup. */
+TLM_API tlm_status fdtd_get_grid(fdtd_handle h, tlm_grid *grid);
 
 /* Field component `which` (0..5 = Ex Ey Ez Hx Hy Hz) in its Yee layout;
  * *n = its length. */

@@ -214,6 +214,8 @@ TLM_API int tlm_is_running(tlm_handle h);
 TLM_API int tlm_is_finished(tlm_handle h);
 TLM_API int tlm_total_steps(tlm_handle h);
 TLM_API tlm_status tlm_timestep(tlm_handle h, float *dt);
+/* grid() (TlmSolver.h:171, 229): the grid given to tlm_setup. */
+TLM_API tlm_status tlm_get_grid(tlm_handle h, tlm_grid *grid);
 
 /* ---- results ------------------------------------------------------- */
 

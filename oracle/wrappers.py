@@ -614,3 +614,50 @@ class RefFdtd(_SurfaceMonitors):
         va = np.empty(cap, np.float32)
         n = self.L.fdr_energy_history(self.h, _ptr(st, _i32p), _ptr(va, _f32p), cap)
         return st[:n].copy(), va[:n].astype(np.float64)
+
+
+class RefEmsim:
+    """The reference's own SaveProject / LoadProject (ProjectIO.cpp, compiled
+    headless into _ref/libtlmref.so) for checking the .emsim code."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            L = RefSolver.lib()
+            L.ref_emsim_resave.restype = C.c_int
+            L.ref_emsim_resave.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]
+            L.ref_emsim_write_sample.restype = C.c_int
+            L.ref_emsim_write_sample.argtypes = [C.c_char_p, C.c_int, C.c_int]
+            L.ref_emsim_summary.restype = C.c_int
+            L.ref_emsim_summary.argtypes = [C.c_char_p, C.POINTER(C.c_int64), C.c_char_p, C.c_int]
+            cls._lib = L
+        return cls._lib
+
+    @classmethod
+    def write_sample(cls, path, seed, playback=True):
+        """A project with every section filled from `seed`, written by SaveProject."""
+        if cls.lib().ref_emsim_write_sample(str(path).encode(), int(seed), int(bool(playback))) != 1:
+            raise OSError(f"reference SaveProject failed for {path}")
+
+    @classmethod
+    def resave(cls, src, dst):
+        """LoadProject(src) then SaveProject(dst): "" on success, else the
+        reference's load error."""
+        err = C.create_string_buffer(256)
+        r = cls.lib().ref_emsim_resave(str(src).encode(), str(dst).encode(), err, 256)
+        if r == -1:
+            raise OSError(f"reference SaveProject failed for {dst}")
+        return "" if r == 1 else err.value.decode()
+
+    @classmethod
+    def summary(cls, path):
+        """Section sizes as LoadProject reads them (see ref_emsim_summary)."""
+        out = (C.c_int64 * 12)()
+        err = C.create_string_buffer(256)
+        if cls.lib().ref_emsim_summary(str(path).encode(), out, err, 256) != 1:
+            raise OSError(err.value.decode())
+        keys = ("settings", "objects", "faces", "face_vals", "plane_vals", "pattern_u", "pages",
+                "page0_curves", "playback_valid", "playback_faces", "frames", "frame0_js")
+        return dict(zip(keys, list(out)))

@@ -1,5 +1,5 @@
 """The C ABI library on a machine without a GPU: it loads, exports every
-symbol include/tlm_b200.h and include/fdtd_b200.h declare, its host-only math matches the
+symbol include/tlm_b200.h, fdtd_b200.h and emsim_b200.h declare, its host-only math matches the
 reference bit for bit, and compute entry points fail loudly (no fallback)."""
 import ctypes as C
 import os
@@ -12,12 +12,12 @@ from tests.conftest import ROOT
 from emsolver_b200 import _lib
 from oracle import Oracle, RefSolver, ref_available
 
-HEADERS = [os.path.join(ROOT, "include", n) for n in ("tlm_b200.h", "fdtd_b200.h")]
+HEADERS = [os.path.join(ROOT, "include", n) for n in ("tlm_b200.h", "fdtd_b200.h", "emsim_b200.h")]
 
 
 def declared_symbols():
     src = "".join(open(h).read() for h in HEADERS)
-    return sorted(set(re.findall(r"TLM_API\s+[\w\s\*]+?\b((?:tlm|fdtd)_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"TLM_API\s+[\w\s\*]+?\b((?:tlm|fdtd|emsim)_\w+)\s*\(", src)))
 
 
 def test_header_declares_entry_points():
