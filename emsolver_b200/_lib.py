@@ -266,6 +266,10 @@ SIGNATURES = {
     "tlm_request_footprint": (_st, [_P(RequestC), _P(C.c_size_t)]),
     "tlm_get_stream": (_st, [_h, _P(C.c_void_p)]),
     "tlm_get_grid": (_st, [_h, _P(Grid)]),
+    "tlm_set_slab": (_st, [_h, C.c_int, C.c_int]),
+    "tlm_halo_bytes": (_st, [_h, _P(C.c_size_t)]),
+    "tlm_halo_pack": (_st, [_h, C.c_void_p, C.c_void_p]),
+    "tlm_halo_unpack": (_st, [_h, C.c_void_p, C.c_void_p]),
     "fdtd_get_grid": (_st, [_h, _P(Grid)]),
     "emsim_new": (_st, [_P(_h)]),
     "emsim_load": (_st, [C.c_char_p, _P(_h), C.c_char_p, C.c_size_t]),

@@ -605,6 +605,8 @@ tlm_status tlm_batch_attach(tlm_batch b, tlm_handle h)
     if (h->device != b->device) return b->fail(TLM_EINVAL, "handle and batch are on different devices");
     if (h->stateIncident)
         return b->fail(TLM_ESTATE, "a state set by tlm_set_pulses must be stepped once before batching");
+    if (h->ghostLo || h->ghostHi)
+        return b->fail(TLM_EINVAL, "a slab exchanges halos after every step: step it on its own");
     if (surfaceActive(h))
         return b->fail(TLM_EINVAL, "surface monitors, cut planes and frames are not recorded in a batch "
                                    "(surface_monitors = 0, record_every = 0, no field plane)");

@@ -102,6 +102,8 @@ __global__ void __launch_bounds__(kBlock, MINB)
                     sa.sv = d.sv[n];
                     sa.samples = d.samples + (long long)i * d.nsamp * 6;
                     sa.epart = (n % 16 == 0) ? d.epart + ((n - eFirst) / 16) * d.nblocks : nullptr;
+                    sa.e_lo = 0;
+                    sa.e_hi = LLONG_MAX;
                     sa.fault = fault;
                     sa.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
                     sa.stochastic = d.stochastic;

@@ -230,6 +230,10 @@ struct tlm_solver
     int curBuf = 0;        // pulse buffer holding the current state
     bool stateIncident = false;
 
+    // z-slab of a grid split over several solvers (tlm_set_slab): the first
+    // and/or last plane is a ghost copy of the neighbouring slab's plane
+    int ghostLo = 0, ghostHi = 0;
+
     // device memory
     void *dPulses[2] = { nullptr, nullptr };
     void *dStub = nullptr;

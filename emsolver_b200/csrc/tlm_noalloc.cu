@@ -159,6 +159,8 @@ tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_planes, fl
     a.sv = 0.0f;
     a.samples = nullptr;
     a.epart = energy_out ? scratch : nullptr;
+    a.e_lo = 0;
+    a.e_hi = LLONG_MAX;
     a.fault = fault;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (input_is_incident)

@@ -160,9 +160,35 @@ std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tile
 // Build the device tables of sources and monitors once, before the first
 // step: the node-sorted entry list, per-block ranges, sample slots, port
 // and probe descriptors, records and DFT accumulators.
+// A slab's ghost planes are copies of the neighbours' planes whose pulses
+// are only correct on the faces the halo exchange rewrites: nothing may be
+// monitored there (sources are harmless: the owning slab injects them).
+tlm_status checkSlabMonitors(tlm_solver *h)
+{
+    if (!h->ghostLo && !h->ghostHi) return TLM_OK;
+    const long long plane = (long long)h->nx * h->ny;
+    auto ghost = [&](long long cell) {
+        const long long k = cell / plane;
+        return (h->ghostLo && k == 0) || (h->ghostHi && k == h->nz - 1);
+    };
+    for (uint64_t c : h->probeCells)
+        if (ghost((long long)c)) return h->fail(TLM_EINVAL, "a probe lies in a ghost plane of the slab");
+    for (const PortInfo &p : h->ports)
+    {
+        for (uint64_t c : p.cells)
+            if (ghost((long long)c)) return h->fail(TLM_EINVAL, "a port cell lies in a ghost plane of the slab");
+        if (!p.cells.empty())
+            for (int t = 0; t < 4; ++t)
+                if (ghost(p.nb[t]))
+                    return h->fail(TLM_EINVAL, "a port's current loop reaches a ghost plane of the slab");
+    }
+    return TLM_OK;
+}
+
 tlm_status prepare(tlm_solver *h)
 {
     if (h->prepared) return TLM_OK;
+    TLM_TRY(checkSlabMonitors(h));
     freeMonitors(h);
     // unique monitored nodes -> sample slots
     std::vector<long long> monNodes;
@@ -356,6 +382,9 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
     a.sv = (R)sourceValue(h, n);
     a.samples = static_cast<R *>(h->dSamples) + (size_t)i * h->nsamp * 6;
     a.epart = (n % 16 == 0) ? h->dEpart + (size_t)((n - eFirst) / 16) * h->nblocks : nullptr;
+    const long long planeNodes = (long long)h->ny * h->px;
+    a.e_lo = h->ghostLo ? planeNodes : 0;
+    a.e_hi = h->ghostHi ? (long long)(h->nz - 1) * planeNodes : LLONG_MAX;
     a.fault = h->dFault;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (h->timing)
@@ -1206,6 +1235,79 @@ tlm_status tlm_get_grid(tlm_handle h, tlm_grid *grid)
     if (!grid) return h->fail(TLM_EINVAL, "null output");
     *grid = h->g;
     return TLM_OK;
+}
+
+// ---- z-slabs ----------------------------------------------------------------
+tlm_status tlm_set_slab(tlm_handle h, int ghost_lo, int ghost_hi)
+{
+    TLM_TRY(checkReady(h));
+    if (h->curStep != 0 || h->prepared) return h->fail(TLM_ESTATE, "tlm_set_slab must come before the first step");
+    if (h->batch) return h->fail(TLM_ESTATE, "the handle is attached to a batch");
+    if ((ghost_lo != 0 && ghost_lo != 1) || (ghost_hi != 0 && ghost_hi != 1))
+        return h->fail(TLM_EINVAL, "ghost_lo and ghost_hi are 0 or 1");
+    if (h->nz < ghost_lo + ghost_hi + 1) return h->fail(TLM_EINVAL, "a slab needs at least one plane of its own");
+    if (surfaceActive(h) || h->cfg.surface_monitors || h->cfg.record_every > 0)
+        return h->fail(TLM_EINVAL, "slabs do not run surface monitors, cut planes or frames");
+    if ((h->storage == TLM_STORE_F16 || h->storage == TLM_STORE_BF16) && !(h->cfg.pulse_scale > 0.0f))
+        return h->fail(TLM_EINVAL, "16-bit slabs need an explicit pulse_scale shared by every slab");
+    h->ghostLo = ghost_lo;
+    h->ghostHi = ghost_hi;
+    return TLM_OK;
+}
+
+tlm_status tlm_halo_bytes(tlm_handle h, size_t *bytes)
+{
+    TLM_TRY(checkReady(h));
+    if (!bytes) return h->fail(TLM_EINVAL, "null output");
+    *bytes = 2 * (size_t)h->ny * h->px * tlmi::storageBytes(h->storage);
+    return TLM_OK;
+}
+
+namespace {
+// Byte offset of the pulse plane (slot s, z-plane k) in a state buffer: a
+// z-plane of one slot is ny * px consecutive nodes of every storage type.
+size_t haloOffset(const tlm_solver *h, int slot, int k)
+{
+    return ((size_t)slot * h->P + (size_t)k * h->ny * h->px) * tlmi::storageBytes(h->storage);
+}
+
+tlm_status haloCopy(tlm_solver *h, bool pack, void *lo, void *hi)
+{
+    TLM_TRY(checkReady(h));
+    if ((lo != nullptr) != (h->ghostLo != 0) || (hi != nullptr) != (h->ghostHi != 0))
+        return h->fail(TLM_EINVAL, "pass a buffer exactly for each side that has a ghost plane");
+    if (!lo && !hi) return TLM_OK;  // a slab without neighbours
+    if (h->stateIncident) return h->fail(TLM_ESTATE, "the state is incident pulses (tlm_set_pulses): step first");
+    DeviceGuard dg(h->device);
+    char *state = static_cast<char *>(h->dPulses[h->curBuf]);
+    const size_t half = (size_t)h->ny * h->px * tlmi::storageBytes(h->storage);
+    const int first = h->ghostLo, last = h->nz - 1 - h->ghostHi;
+    // slot = axis * 4 + side * 2 + pol: 8, 9 leave a node through its -z
+    // face, 10, 11 through its +z face.
+    struct Side { char *buf; int slot, plane; };
+    const Side sides[2] = {
+        { static_cast<char *>(lo), pack ? 8 : 10, pack ? first : 0 },
+        { static_cast<char *>(hi), pack ? 10 : 8, pack ? last : h->nz - 1 },
+    };
+    for (const Side &sd : sides)
+    {
+        if (!sd.buf) continue;
+        for (int t = 0; t < 2; ++t)
+        {
+            char *dev = state + haloOffset(h, sd.slot + t, sd.plane);
+            char *msg = sd.buf + t * half;
+            TLM_CU(h, cudaMemcpyAsync(pack ? msg : dev, pack ? dev : msg, half, cudaMemcpyDeviceToDevice, h->stream));
+        }
+    }
+    return TLM_OK;
+}
+} // namespace
+
+tlm_status tlm_halo_pack(tlm_handle h, void *send_lo, void *send_hi) { return haloCopy(h, true, send_lo, send_hi); }
+
+tlm_status tlm_halo_unpack(tlm_handle h, const void *recv_lo, const void *recv_hi)
+{
+    return haloCopy(h, false, const_cast<void *>(recv_lo), const_cast<void *>(recv_hi));
 }
 
 int tlm_probe_count(tlm_handle h) { return h ? (int)h->probeCells.size() : 0; }

@@ -18,6 +18,7 @@
 
 #include "tlm_device.cuh"
 
+#include <climits>
 #include <type_traits>
 
 namespace tlmk {
@@ -43,6 +44,7 @@ template <class S> struct StepArgs
     R sv;                          // source value of this step
     R *__restrict__ samples;       // [nsamp][6] of this step
     double *__restrict__ epart;    // [gridDim.x] energy partials (energy steps)
+    long long e_lo, e_hi;          // nodes [e_lo, e_hi) count towards the energy (a slab's own planes)
     unsigned int *__restrict__ fault;  // bounds-check record (checked builds)
     unsigned int round_seed;       // per-step seed of stochastic rounding
     int stochastic;                // BF16/F16: round stochastically
@@ -253,7 +255,7 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
 #pragma unroll
         for (int c = 0; c < V; ++c)
         {
-            if ((liveMask >> c) & 1u)
+            if (((liveMask >> c) & 1u) && node0 + c >= a.e_lo && node0 + c < a.e_hi)
             {
 #pragma unroll
                 for (int s = 0; s < 12; ++s) e += (double)inc[s][c] * (double)inc[s][c];
@@ -687,7 +689,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
 #pragma unroll
         for (int c = 0; c < V; ++c)
         {
-            if ((nodeLive >> c) & 1u)
+            if (((nodeLive >> c) & 1u) && node0 + c >= a.e_lo && node0 + c < a.e_hi)
             {
 #pragma unroll
                 for (int s = 0; s < 12; ++s) e += (double)inc[s][c] * (double)inc[s][c];

@@ -485,6 +485,25 @@ class TlmSolver:
         self._c(self._L.tlm_get_stream(self._h, C.byref(s)))
         return s.value
 
+    # -- z-slabs (tlm_set_slab) -------------------------------------------
+    def setSlab(self, ghostLo: bool, ghostHi: bool):
+        """Mark the first / last plane as ghost copies of the neighbouring
+        slabs' planes (before the first step)."""
+        self._c(self._L.tlm_set_slab(self._h, int(bool(ghostLo)), int(bool(ghostHi))))
+
+    def haloBytes(self) -> int:
+        b = C.c_size_t(0)
+        self._c(self._L.tlm_halo_bytes(self._h, C.byref(b)))
+        return b.value
+
+    def haloPack(self, send_lo: int | None, send_hi: int | None):
+        """Queue copies of the own boundary planes' outgoing z pulses into
+        the device buffers at send_lo / send_hi (addresses, or None)."""
+        self._c(self._L.tlm_halo_pack(self._h, send_lo, send_hi))
+
+    def haloUnpack(self, recv_lo: int | None, recv_hi: int | None):
+        self._c(self._L.tlm_halo_unpack(self._h, recv_lo, recv_hi))
+
     def deviceBytes(self):
         b = C.c_size_t(0)
         self._c(self._L.tlm_device_bytes(self._h, C.byref(b)))

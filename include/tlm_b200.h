@@ -437,6 +437,35 @@ TLM_API tlm_status tlm_get_frame(tlm_handle h, int idx, int *step, float *js, in
 TLM_API tlm_status tlm_compute_far_field(tlm_handle h, int n_theta, int n_phi, float *U, float *u_max,
                                          float *directivity, float *peak_theta_deg, float *peak_phi_deg);
 
+/* ---- one grid split into z-slabs over several solvers ------------------ */
+
+/* No single counterpart in the reference: its z-slab worker threads
+ * (TlmSolver.cpp:174-240, 516-613) split one grid in one address space;
+ * here each slab is its own solver (one per GPU) and the slabs trade the
+ * z-directed link pulses that cross their shared faces once per step.
+ *
+ * A slab's handle is set up on its planes plus one ghost plane on each side
+ * that has a neighbouring slab (the neighbour's boundary plane, with its true
+ * material), then tlm_set_slab(h, ghost_lo, ghost_hi) before the first step.
+ * Ghost planes are stepped but excluded from the energy; probes and ports
+ * (with their current loops) must lie in the slab's own planes (TLM_EINVAL at
+ * the first step otherwise); sources may lie anywhere, since only the owning
+ * slab's copy of a plane reaches the results. Not with surface monitors,
+ * frames or batches; F16/BF16 need an explicit pulse_scale shared by all
+ * slabs. Between two tlm_step_async(h, 1) calls, exchange:
+ *   tlm_halo_pack(h, send_lo, send_hi)     this slab's first and last own
+ *                                          planes' outgoing z pulses,
+ *   send_lo to the slab below / send_hi to the slab above, receive theirs,
+ *   tlm_halo_unpack(h, recv_lo, recv_hi)   into the ghost planes.
+ * Buffers are device memory of tlm_halo_bytes each (NULL on a side without
+ * a ghost plane); copies are queued on the handle's stream (tlm_get_stream).
+ * Stepped this way every pulse of the own planes, every probe and port
+ * record is bitwise what the undivided grid gives; energies add up. */
+TLM_API tlm_status tlm_set_slab(tlm_handle h, int ghost_lo, int ghost_hi);
+TLM_API tlm_status tlm_halo_bytes(tlm_handle h, size_t *bytes);
+TLM_API tlm_status tlm_halo_pack(tlm_handle h, void *send_lo, void *send_hi);
+TLM_API tlm_status tlm_halo_unpack(tlm_handle h, const void *recv_lo, const void *recv_hi);
+
 /* ---- one step over caller-owned device memory, no allocation -------- */
 
 /* No counterpart in the reference. For callers that may not allocate device
