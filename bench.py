@@ -249,6 +249,7 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     kern_ms, launches = s.kernelTime()
     s.setKernelTiming(False)
+    per_step_kernels = s.stepLaunches()
     ms_max = dist.max(ms)
     kern_max = dist.max(kern_ms)
     s.close()
@@ -304,11 +305,11 @@ def run_ours(args):
                        "l2": f"state {2 * 12 * sbytes * n / 1e6:.0f} MB > L2 (126 MB); no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": tr, "algorithmic_bytes_per_launch": bytes_step,
-                         "kernel_ms_per_launch": per_launch_ms},
+                         "traffic": tr, "algorithmic_bytes_per_step": bytes_step,
+                         "kernel_ms_per_step": per_launch_ms, "kernels_per_step": per_step_kernels},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": launches + epilogues,
+            "gpu_launches": launches * per_step_kernels + epilogues,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

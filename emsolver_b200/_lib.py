@@ -43,7 +43,7 @@ class ConfigC(C.Structure):
                 ("use_gpu", C.c_int), ("record_every", C.c_int), ("storage", C.c_int),
                 ("pulse_scale", C.c_float), ("steps_per_launch", C.c_int),
                 ("kernel_variant", C.c_int), ("rounding", C.c_int), ("general_tiles", C.c_int),
-                ("surface_monitors", C.c_int)]
+                ("surface_monitors", C.c_int), ("no_staging", C.c_int)]
 
 
 class EmsimFaceC(C.Structure):
@@ -309,6 +309,7 @@ SIGNATURES = {
     "tlm_device_bytes": (_st, [_h, _P(C.c_size_t)]),
     "tlm_set_kernel_timing": (_st, [_h, C.c_int]),
     "tlm_kernel_time": (_st, [_h, _P(C.c_double), _P(C.c_longlong)]),
+    "tlm_step_launches": (_st, [_h, _P(C.c_int)]),
 }
 
 

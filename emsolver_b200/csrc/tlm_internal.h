@@ -241,7 +241,11 @@ struct tlm_solver
     void *dYhat = nullptr, *dGhat = nullptr;
     tlmk::SpecEntry *dSpec = nullptr;
     int *dTile = nullptr;
-    uint8_t *dTileFlags = nullptr;  // per step-kernel tile: tlmk::kTileGeneral / kTileDiel
+    uint8_t *dTileFlags = nullptr;  // per step-kernel tile: tlmk::kTileGeneral / kTileDiel / kTileEdge
+    int *dStaged = nullptr, *dListed = nullptr;  // tiles of the staged kernel / of the list kernel
+    int nStaged = 0, nListed = 0, stagedGrid = 0;
+    cudaStream_t side = nullptr;      // the list kernel's stream (forked from and joined to `stream`)
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     void *dSamples = nullptr;
     double *dEpart = nullptr;
     int *dPortOff = nullptr, *dPortSlots = nullptr, *dPortPol = nullptr, *dPortNb = nullptr;

@@ -61,6 +61,9 @@ void freeMonitors(tlm_solver *h)
     devFree(h, h->dSpec);
     devFree(h, h->dTile);
     devFree(h, h->dTileFlags);
+    devFree(h, h->dStaged);
+    devFree(h, h->dListed);
+    h->nStaged = h->nListed = 0;
     devFree(h, h->dSamples);
     devFree(h, h->dEpart);
     devFree(h, h->dPortOff);
@@ -125,6 +128,19 @@ std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tile
         if (node >= 0 && node < h->P) f[(size_t)(node / T)] |= bit;
     };
     if (h->nquads % kBlock) f[(size_t)nb - 1] |= tlmk::kTileGeneral;
+    // outer y and z faces: the first and last plane, the first and last row
+    // of every plane
+    const long long planeN = (long long)h->px * h->ny;
+    auto markRange = [&](long long n0, long long n1) {
+        for (long long t = n0 / T; t * T < n1 && t < nb; ++t) f[(size_t)t] |= tlmk::kTileEdge;
+    };
+    markRange(0, planeN);
+    markRange((long long)(h->nz - 1) * planeN, (long long)h->nz * planeN);
+    for (int k = 0; k < h->nz; ++k)
+    {
+        markRange((long long)k * planeN, (long long)k * planeN + h->px);
+        markRange((long long)k * planeN + (long long)(h->ny - 1) * h->px, (long long)(k + 1) * planeN);
+    }
     for (int b = 0; b < nb; ++b)
         if (tileBegin[b + 1] > tileBegin[b]) f[(size_t)b] |= tlmk::kTileGeneral;
     const long long sy = h->px, sz = (long long)h->px * h->ny;
@@ -185,6 +201,42 @@ tlm_status checkSlabMonitors(tlm_solver *h)
     return TLM_OK;
 }
 
+// FP32 in the default tile shape: interior tiles off the outer y/z faces go
+// to the staged kernel, every other tile to the list kernel, both launched
+// every step (tlm_config.no_staging = 1: the single step kernel as before).
+tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
+{
+    h->nStaged = h->nListed = 0;
+    if (h->storage != TLM_STORE_F32 || h->variant != 0 || h->cfg.no_staging || h->V != 2) return TLM_OK;
+    std::vector<int> staged, listed;
+    for (int t = 0; t < h->nblocks; ++t)
+        ((flags[(size_t)t] & (tlmk::kTileGeneral | tlmk::kTileEdge)) ? listed : staged).push_back(t);
+    if (staged.empty()) return TLM_OK;
+    int sms = 0;
+    TLM_CU(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    TLM_CU(h, cudaFuncSetAttribute(tlmk::stepKernelStaged<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tlmk::kStages * tlmk::kStageBytes));
+    if (!h->side)
+    {
+        TLM_CU(h, cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        TLM_CU(h, cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming));
+        TLM_CU(h, cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming));
+    }
+    TLM_TRY(devAlloc(h, &h->dStaged, staged.size() * sizeof(int)));
+    TLM_CU(h, cudaMemcpyAsync(h->dStaged, staged.data(), staged.size() * sizeof(int), cudaMemcpyHostToDevice,
+                              h->stream));
+    if (!listed.empty())
+    {
+        TLM_TRY(devAlloc(h, &h->dListed, listed.size() * sizeof(int)));
+        TLM_CU(h, cudaMemcpyAsync(h->dListed, listed.data(), listed.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                  h->stream));
+    }
+    h->nStaged = (int)staged.size();
+    h->nListed = (int)listed.size();
+    h->stagedGrid = std::min(h->nStaged, 2 * sms);
+    return TLM_OK;
+}
+
 tlm_status prepare(tlm_solver *h)
 {
     if (h->prepared) return TLM_OK;
@@ -234,6 +286,7 @@ tlm_status prepare(tlm_solver *h)
         TLM_TRY(devAlloc(h, &h->dTileFlags, flags.size()));
         TLM_CU(h, cudaMemcpyAsync(h->dTileFlags, flags.data(), flags.size(), cudaMemcpyHostToDevice,
                                   h->stream));
+        TLM_TRY(prepareStaging(h, flags));
     }
     h->specCount = (int)ents.size();
     if (!ents.empty())
@@ -403,7 +456,28 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
     a.round_seed = tlmk::mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
     a.stochastic = h->cfg.rounding == 1 ? 1 : 0;
     if (surfaceActive(h)) TLM_TRY(launchSurface(h, n));  // reads the same input buffer, first
-    launchShaped<S>(a, h->variant, h->stateIncident, h->nblocks, h->stream);
+    if constexpr (std::is_same<S, float>::value)
+    {
+        if (h->nStaged > 0 && !h->stateIncident)
+        {
+            // the listed tiles run beside the staged ones (disjoint outputs,
+            // the same input), on the side stream between a fork and a join
+            if (h->nListed > 0)
+            {
+                TLM_CU(h, cudaEventRecord(h->evFork, h->stream));
+                TLM_CU(h, cudaStreamWaitEvent(h->side, h->evFork, 0));
+                tlmk::stepKernelList<float, 2, 4, true><<<h->nListed, kBlock, 0, h->side>>>(a, h->dListed);
+                TLM_CU(h, cudaEventRecord(h->evJoin, h->side));
+            }
+            tlmk::stepKernelStaged<2><<<h->stagedGrid, tlmk::kStagedThreads, tlmk::kStages * tlmk::kStageBytes,
+                                        h->stream>>>(a, h->dStaged, h->nStaged);
+            if (h->nListed > 0) TLM_CU(h, cudaStreamWaitEvent(h->stream, h->evJoin, 0));
+        }
+        else
+            launchShaped<S>(a, h->variant, h->stateIncident, h->nblocks, h->stream);
+    }
+    else
+        launchShaped<S>(a, h->variant, h->stateIncident, h->nblocks, h->stream);
     TLM_CU(h, cudaGetLastError());
     if (h->timing) TLM_CU(h, cudaEventRecord(e1, h->stream));
     h->stateIncident = false;
@@ -502,6 +576,7 @@ tlm_status syncState(tlm_solver *h)
     {
         unsigned f = 0;
         TLM_CU(h, cudaMemcpy(&f, h->dFault, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (f & tlmk::kStageTimeout) return h->fail(TLM_ECUDA, "a staged tile's bulk copies never arrived");
         if (f) return h->fail(TLM_ECUDA, "bounds check tripped, code mask " + std::to_string(f));
     }
     h->doneStep.store(h->curStep);
@@ -765,6 +840,7 @@ void tlm_config_default(tlm_config *c)
     c->kernel_variant = 0;
     c->rounding = 0;
     c->general_tiles = 0;
+    c->no_staging = 0;
     c->surface_monitors = 0;
 }
 
@@ -835,10 +911,10 @@ tlm_status tlm_create(tlm_handle *out, int device)
     }
     e = cudaMallocFromPoolAsync((void **)&h->dElatest, sizeof(double), h->pool, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->dElatest, 0, sizeof(double), h->stream);
-#ifdef TLM_CHECKED
+    // error flags of the kernels: bounds checks (checked build), staged-tile
+    // waits that ran out (every build)
     if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&h->dFault, sizeof(unsigned), h->pool, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->dFault, 0, sizeof(unsigned), h->stream);
-#endif
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess)
     {
@@ -862,6 +938,13 @@ tlm_status tlm_destroy(tlm_handle h)
     if (h->dElatest) cudaFreeAsync(h->dElatest, h->stream);
     if (h->dFault) cudaFreeAsync(h->dFault, h->stream);
     for (cudaEvent_t ev : h->evs) cudaEventDestroy(ev);
+    if (h->side)
+    {
+        cudaStreamSynchronize(h->side);
+        cudaEventDestroy(h->evFork);
+        cudaEventDestroy(h->evJoin);
+        cudaStreamDestroy(h->side);
+    }
     cudaStreamDestroy(h->stream);
     delete h;
     return TLM_OK;
@@ -900,6 +983,7 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     if (cfg->rounding < 0 || cfg->rounding > 1) return h->fail(TLM_EINVAL, "rounding must be 0 or 1");
     if (cfg->general_tiles < 0 || cfg->general_tiles > 1)
         return h->fail(TLM_EINVAL, "general_tiles must be 0 or 1");
+    if (cfg->no_staging < 0 || cfg->no_staging > 1) return h->fail(TLM_EINVAL, "no_staging must be 0 or 1");
     if (cfg->surface_monitors < 0 || cfg->surface_monitors > 1)
         return h->fail(TLM_EINVAL, "surface_monitors must be 0 or 1");
     if (cfg->record_every < 0 || cfg->huy_offset < 0)
@@ -1607,6 +1691,15 @@ tlm_status tlm_set_kernel_timing(tlm_handle h, int enable)
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->timing = enable != 0;
     h->evUsed = 0;
+    return TLM_OK;
+}
+
+tlm_status tlm_step_launches(tlm_handle h, int *per_step)
+{
+    TLM_TRY(checkHandle(h));
+    if (!per_step) return h->fail(TLM_EINVAL, "null output");
+    TLM_TRY(prepare(h));
+    *per_step = (h->nStaged > 0 ? (h->nListed > 0 ? 2 : 1) : 1) + (surfaceActive(h) ? 1 : 0);
     return TLM_OK;
 }
 

@@ -57,7 +57,8 @@ template <class S> struct StepArgs
 // thread of it is live, neither its nodes nor their six neighbours are PEC,
 // and it holds no source or monitor. kTileDiel: the tile has stub-loaded
 // nodes.
-enum : uint8_t { kTileGeneral = 1, kTileDiel = 2 };
+// kTileEdge: the tile has a node on an outer y or z face.
+enum : uint8_t { kTileGeneral = 1, kTileDiel = 2, kTileEdge = 4 };
 
 #ifdef TLM_CHECKED
 #define TLM_GUARD(idx, limit, code)                                                         \
@@ -147,15 +148,73 @@ template <int V> __device__ __forceinline__ unsigned pecMask(const uint8_t (&m)[
     return r;
 }
 
+// Shared-memory stage of one FP32 tile of kBlock node pairs, filled by bulk
+// copies (stepKernelStaged): slots 0..3 at the tile's own nodes with 4 nodes
+// of halo on each side (the x neighbours), then the eight y/z neighbour
+// segments in the order of inc[4..11] (slot 6+t one row below, 4+t one row
+// above, 10+t one plane below, 8+t one plane above), the three stub planes,
+// and the material bytes. Offsets in floats, except kStageOffMat (bytes).
+constexpr int kStageNodes = kBlock * 2;
+constexpr int kStageSegX = kStageNodes + 8;
+constexpr int kStageOffYZ = 4 * kStageSegX;
+constexpr int kStageOffStub = kStageOffYZ + 8 * kStageNodes;
+constexpr int kStageOffMat = (kStageOffStub + 3 * kStageNodes) * 4;
+constexpr int kStageBytes = kStageOffMat + kStageNodes;
+static_assert(kStageBytes % 16 == 0 && (kStageSegX * 4) % 16 == 0, "bulk copies need 16-byte multiples");
+
+constexpr int kStages = 3;
+constexpr int kStagedThreads = kBlock + 32;
+constexpr unsigned kStageTimeout = 1u << 31;
+// try_wait suspends the thread for at most kStageSuspendNs per call, so a
+// wait gives up after about kStageWaitLimit microseconds.
+constexpr long long kStageWaitLimit = 1LL << 21;
+constexpr unsigned kStageSuspendNs = 1000;
+
+__device__ __forceinline__ unsigned smemAddr(const void *p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbarTryWait(unsigned bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity), "n"(kStageSuspendNs)
+                 : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ bool mbarWaitBounded(unsigned bar, unsigned parity)
+{
+    for (long long it = 0; it < kStageWaitLimit; ++it)
+        if (mbarTryWait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void bulkCopy(unsigned dst, const void *src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :
+                 : "r"(dst), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
 // Interior tile (see kTileGeneral): the gather needs no PEC handling, so
 // every pulse load is issued before any material is read. On the outer faces
 // the load of the neighbour's pulse becomes a load of the own pulse, scaled
 // by rho afterwards (y/z faces: per thread; x faces, the first and last node
 // of a row, and the row padding: fixed up per node). Pairs of nodes scatter
 // with packed FP32x2 arithmetic. The results are bitwise those of the
-// general tile body below.
-template <class S, int V>
-__device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel)
+// general tile body below. kStaged: the tile's inputs are already in the
+// shared-memory stage `sm` (see kStageBytes; FP32, V = 2, and the tile has no
+// node on an outer y or z face); the arithmetic is the same.
+template <class S, int V, bool kStaged = false>
+__device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel,
+                                                 const unsigned char *sm = nullptr, unsigned eBar = 0,
+                                                 unsigned eParity = 0)
 {
     using R = float;
     static_assert(V % 2 == 0, "interior tiles scatter node pairs");
@@ -174,35 +233,65 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     // ---- loads: own x-slots, then the y and z neighbours' opposite faces ----
     R ox[4][V];
     R inc[12][V];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) loadVec<S, V>(a.in, s * P + node0, ox[s], a.scale);
-#pragma unroll
-    for (int t = 0; t < 2; ++t)
-    {
-        // -y face: (y,+) of the row below; +y face: (y,-) of the row above;
-        // on an outer face the own pulse of the face instead
-        loadVec<S, V>(a.in, atYlo ? (4 + t) * P + node0 : (6 + t) * P + node0 - sy, inc[4 + t], a.scale);
-        loadVec<S, V>(a.in, atYhi ? (6 + t) * P + node0 : (4 + t) * P + node0 + sy, inc[6 + t], a.scale);
-        loadVec<S, V>(a.in, atZlo ? (8 + t) * P + node0 : (10 + t) * P + node0 - sz, inc[8 + t], a.scale);
-        loadVec<S, V>(a.in, atZhi ? (10 + t) * P + node0 : (8 + t) * P + node0 + sz, inc[10 + t], a.scale);
-    }
-    // ---- x neighbours: own vector, adjacent lane, or (warp edge) a scalar load ----
     R prevX[2], nextX[2];
-#pragma unroll
-    for (int t = 0; t < 2; ++t)
+    if constexpr (kStaged)
     {
-        prevX[t] = __shfl_up_sync(0xffffffffu, ox[2 + t][V - 1], 1);
-        nextX[t] = __shfl_down_sync(0xffffffffu, ox[t][0], 1);
+        static_assert(std::is_same<S, float>::value && V == 2, "staged tiles hold FP32 node pairs");
+        const float *X = reinterpret_cast<const float *>(sm);
+        const int l = threadIdx.x * V;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+        {
+            const float2 v = *reinterpret_cast<const float2 *>(X + s * kStageSegX + 4 + l);
+            ox[s][0] = v.x;
+            ox[s][1] = v.y;
+        }
+#pragma unroll
+        for (int g = 0; g < 8; ++g)
+        {
+            const float2 v = *reinterpret_cast<const float2 *>(X + kStageOffYZ + g * kStageNodes + l);
+            inc[4 + g][0] = v.x;
+            inc[4 + g][1] = v.y;
+        }
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+        {
+            prevX[t] = X[(2 + t) * kStageSegX + 3 + l];
+            nextX[t] = X[t * kStageSegX + 4 + l + V];
+        }
+        (void)lane;
     }
-    if (lane == 0 && x0 > 0)
+    else
     {
 #pragma unroll
-        for (int t = 0; t < 2; ++t) prevX[t] = loadOne<S>(a.in, (2 + t) * P + node0 - 1, a.scale);
-    }
-    if (lane == 31 && x0 + V <= a.nx - 1)
-    {
+        for (int s = 0; s < 4; ++s) loadVec<S, V>(a.in, s * P + node0, ox[s], a.scale);
 #pragma unroll
-        for (int t = 0; t < 2; ++t) nextX[t] = loadOne<S>(a.in, t * P + node0 + V, a.scale);
+        for (int t = 0; t < 2; ++t)
+        {
+            // -y face: (y,+) of the row below; +y face: (y,-) of the row above;
+            // on an outer face the own pulse of the face instead
+            loadVec<S, V>(a.in, atYlo ? (4 + t) * P + node0 : (6 + t) * P + node0 - sy, inc[4 + t], a.scale);
+            loadVec<S, V>(a.in, atYhi ? (6 + t) * P + node0 : (4 + t) * P + node0 + sy, inc[6 + t], a.scale);
+            loadVec<S, V>(a.in, atZlo ? (8 + t) * P + node0 : (10 + t) * P + node0 - sz, inc[8 + t], a.scale);
+            loadVec<S, V>(a.in, atZhi ? (10 + t) * P + node0 : (8 + t) * P + node0 + sz, inc[10 + t], a.scale);
+        }
+        // ---- x neighbours: own vector, adjacent lane, or (warp edge) a scalar load ----
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+        {
+            prevX[t] = __shfl_up_sync(0xffffffffu, ox[2 + t][V - 1], 1);
+            nextX[t] = __shfl_down_sync(0xffffffffu, ox[t][0], 1);
+        }
+        if (lane == 0 && x0 > 0)
+        {
+#pragma unroll
+            for (int t = 0; t < 2; ++t) prevX[t] = loadOne<S>(a.in, (2 + t) * P + node0 - 1, a.scale);
+        }
+        if (lane == 31 && x0 + V <= a.nx - 1)
+        {
+#pragma unroll
+            for (int t = 0; t < 2; ++t) nextX[t] = loadOne<S>(a.in, t * P + node0 + V, a.scale);
+        }
     }
 #pragma unroll
     for (int t = 0; t < 2; ++t)
@@ -261,8 +350,35 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
                 for (int s = 0; s < 12; ++s) e += (double)inc[s][c] * (double)inc[s][c];
             }
         }
-        const double tot = blockSumDouble(e, red);
-        if (threadIdx.x == 0) a.epart[tile] = tot;
+        if constexpr (kStaged)
+        {
+            // the same per-warp sums in the same order as blockSumDouble, but
+            // gathered through the mbarrier eBar so that no warp waits for
+            // the others (only thread 0 does, bounded)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+            if (lane == 0)
+            {
+                red[threadIdx.x >> 5] = e;
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(eBar) : "memory");
+            }
+            if (threadIdx.x == 0)
+            {
+                if (mbarWaitBounded(eBar, eParity))
+                {
+                    double tot = 0.0;
+                    for (int w = 0; w < kBlock / 32; ++w) tot += red[w];
+                    a.epart[tile] = tot;
+                }
+                else if (a.fault)
+                    atomicOr(a.fault, kStageTimeout);
+            }
+        }
+        else
+        {
+            const double tot = blockSumDouble(e, red);
+            if (threadIdx.x == 0) a.epart[tile] = tot;
+        }
     }
 
     // ---- scatter (pairs of nodes) and store ----
@@ -270,7 +386,13 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     unsigned dielMask = 0;
     if (diel)
     {
-        loadMat<V>(a.mat, node0, m);
+        if constexpr (kStaged)
+        {
+#pragma unroll
+            for (int c = 0; c < V; ++c) m[c] = sm[kStageOffMat + threadIdx.x * V + c];
+        }
+        else
+            loadMat<V>(a.mat, node0, m);
 #pragma unroll
         for (int c = 0; c < V; ++c) dielMask |= ((m[c] >= kDiel0) ? 1u : 0u) << c;
         dielMask &= liveMask;
@@ -287,7 +409,12 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
 #pragma unroll
         for (int jj = 0; jj < 3; ++jj)
         {
-            const Pack<R, V> p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
+            Pack<R, V> p;
+            if constexpr (kStaged)
+                p = *reinterpret_cast<const Pack<R, V> *>(reinterpret_cast<const float *>(sm) + kStageOffStub +
+                                                          jj * kStageNodes + threadIdx.x * V);
+            else
+                p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
 #pragma unroll
             for (int c = 0; c < V; ++c) vs[jj][c] = p.v[c];
         }
@@ -809,6 +936,116 @@ __global__ void __launch_bounds__(kBlock, MINB) stepKernelShaped(const StepArgs<
 {
     __shared__ double red[kBlock / 32];
     stepTile<S, V, kIncident, kSelect>(a, blockIdx.x, red);
+}
+
+// Step kernel over a list of tiles (the tiles that the staged kernel below
+// does not take), one tile per block.
+template <class S, int V, int MINB, bool kSelect>
+__global__ void __launch_bounds__(kBlock, MINB) stepKernelList(const StepArgs<S> a, const int *__restrict__ tiles)
+{
+    __shared__ double red[kBlock / 32];
+    stepTile<S, V, false, kSelect>(a, tiles[blockIdx.x], red);
+}
+
+// ---- staged interior tiles (FP32) -------------------------------------------
+// Interior tiles without a node on an outer y or z face, each staged in shared
+// memory by bulk copies (the tensor-memory-access engine) before the interior
+// body runs on it. A block of kBlock consumer threads and one producer warp
+// owns every gridDim.x-th tile of the list and keeps kStages tiles in
+// flight: the producer refills a stage as soon as every consumer warp has
+// released it (mbarrier `empty`), the consumers start a tile as soon as its
+// bytes are in (mbarrier `full`), and the energy sum of a tile gathers the
+// warps' shares through a third mbarrier (`ered`) that only thread 0 waits
+// on, so no warp waits for another. Every wait is bounded: one that runs out
+// sets kStageTimeout in *a.fault and ends its thread; the producer first lets
+// the copies it issued land (again bounded), and the host reports the error.
+// Issue the copies of `tile` into the stage at `st` (one thread).
+__device__ __forceinline__ void stageTile(const StepArgs<float> &a, int tile, unsigned st, unsigned bar)
+{
+    const long long node0 = (long long)tile * kStageNodes;
+    const long long P = a.P, sy = a.px, sz = (long long)a.px * a.ny;
+    const bool diel = (a.tile_flags[tile] & kTileDiel) != 0 && a.stub != nullptr;
+    const unsigned segX = kStageSegX * 4, seg = kStageNodes * 4;
+    const unsigned bytes = 4 * segX + 8 * seg + (diel ? 3 * seg : 0) + kStageNodes;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" : : "r"(bar), "r"(bytes) : "memory");
+#pragma unroll
+    for (int s = 0; s < 4; ++s) bulkCopy(st + s * segX, a.in + s * P + node0 - 4, segX, bar);
+    const unsigned yz = st + kStageOffYZ * 4;
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+    {
+        bulkCopy(yz + (0 + t) * seg, a.in + (6 + t) * P + node0 - sy, seg, bar);
+        bulkCopy(yz + (2 + t) * seg, a.in + (4 + t) * P + node0 + sy, seg, bar);
+        bulkCopy(yz + (4 + t) * seg, a.in + (10 + t) * P + node0 - sz, seg, bar);
+        bulkCopy(yz + (6 + t) * seg, a.in + (8 + t) * P + node0 + sz, seg, bar);
+    }
+    if (diel)
+    {
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj)
+            bulkCopy(st + (kStageOffStub + jj * kStageNodes) * 4, a.stub + jj * P + node0, seg, bar);
+    }
+    bulkCopy(st + kStageOffMat, a.mat + node0, kStageNodes, bar);
+}
+
+template <int V, int STAGES = kStages, int MINB = 2>
+__global__ void __launch_bounds__(kStagedThreads, MINB)
+    stepKernelStaged(const StepArgs<float> a, const int *__restrict__ tiles, int ntiles)
+{
+    static_assert(V == 2, "a stage holds kBlock node pairs");
+    extern __shared__ __align__(128) unsigned char stage[];
+    __shared__ double red[STAGES][kBlock / 32];
+    __shared__ __align__(8) unsigned long long full[STAGES], empty[STAGES], ered[STAGES];
+    const int mine = ntiles > (int)blockIdx.x ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+    const unsigned st0 = smemAddr(stage), full0 = smemAddr(full), empty0 = smemAddr(empty), ered0 = smemAddr(ered);
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < STAGES; ++s)
+        {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" : : "r"(full0 + 8 * s) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(empty0 + 8 * s), "n"(kBlock / 32) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(ered0 + 8 * s), "n"(kBlock / 32) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" : : : "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x >= kBlock)
+    {
+        // producer warp: one lane issues every copy
+        if (threadIdx.x != kBlock) return;
+        int issued = 0;
+        for (int i = 0; i < mine; ++i)
+        {
+            const int s = i % STAGES;
+            if (i >= STAGES && !mbarWaitBounded(empty0 + 8 * s, (unsigned)(i / STAGES - 1) & 1u))
+            {
+                if (a.fault) atomicOr(a.fault, kStageTimeout);
+                break;
+            }
+            stageTile(a, tiles[blockIdx.x + i * gridDim.x], st0 + s * kStageBytes, full0 + 8 * s);
+            issued = i + 1;
+        }
+        // the copies of the last STAGES tiles may still be landing: stay
+        // until they are in, so that the block's shared memory outlives them
+        for (int i = issued > STAGES ? issued - STAGES : 0; i < issued; ++i)
+            mbarWaitBounded(full0 + 8 * (i % STAGES), (unsigned)(i / STAGES) & 1u);
+        return;
+    }
+    for (int i = 0; i < mine; ++i)
+    {
+        const int s = i % STAGES;
+        if (!mbarWaitBounded(full0 + 8 * s, (unsigned)(i / STAGES) & 1u))
+        {
+            if (a.fault) atomicOr(a.fault, kStageTimeout);
+            return;
+        }
+        const int tile = tiles[blockIdx.x + i * gridDim.x];
+        stepTileInterior<float, V, true>(a, tile, red[s], (a.tile_flags[tile] & kTileDiel) != 0,
+                                          stage + s * kStageBytes, ered0 + 8 * s, (unsigned)(i / STAGES) & 1u);
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0)
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(empty0 + 8 * s) : "memory");
+    }
 }
 
 } // namespace tlmk

@@ -6,7 +6,7 @@ from .solver import MatProps, TlmConfig, TlmSolver, VoxelGridSpec
 
 def build_solver(w, device: int = 0, storage: int | None = None, steps_per_launch: int = 0,
                  variant: str | None = None, pulse_scale: float = 0.0, kernel_variant: int = 0,
-                 rounding: int = 0, general_tiles: bool = False) -> TlmSolver:
+                 rounding: int = 0, general_tiles: bool = False, no_staging: bool = False) -> TlmSolver:
     """Create, set up and populate a solver exactly as the reference would be:
     setup, ports (in order), plane wave, probes at cell centres, port DFT."""
     s = TlmSolver(device, variant)
@@ -16,7 +16,8 @@ def build_solver(w, device: int = 0, storage: int | None = None, steps_per_launc
                     surfaceMonitors=bool(w.meta.get("surface_monitors", False)),
                     boundaryRho=w.rho, storage=w.storage if storage is None else storage,
                     stepsPerLaunch=steps_per_launch, pulseScale=pulse_scale,
-                    kernelVariant=kernel_variant, rounding=rounding, generalTiles=general_tiles)
+                    kernelVariant=kernel_variant, rounding=rounding, generalTiles=general_tiles,
+                    noStaging=no_staging)
     s.setup(grid, w.mat, [MatProps(e, g) for e, g in w.table], cfg)
     if w.waveform == 3 and w.sv is not None:
         s.setSourceTable(w.sv)

@@ -92,6 +92,7 @@ class TlmConfig:
     rounding: int = 0          # 16-bit storage: 0 nearest, 1 stochastic
     generalTiles: bool = False  # True: no interior-tile fast path (cross-checks)
     surfaceMonitors: bool = False  # PEC-surface Js and Huygens-box DFT monitors
+    noStaging: bool = False    # True: no shared-memory staging of FP32 interior tiles (cross-checks)
 
     def to_c(self):
         c = _lib.ConfigC()
@@ -110,6 +111,7 @@ class TlmConfig:
         c.rounding = int(self.rounding)
         c.general_tiles = 1 if self.generalTiles else 0
         c.surface_monitors = 1 if self.surfaceMonitors else 0
+        c.no_staging = 1 if self.noStaging else 0
         return c
 
 
@@ -511,6 +513,12 @@ class TlmSolver:
 
     def setKernelTiming(self, on: bool):
         self._c(self._L.tlm_set_kernel_timing(self._h, 1 if on else 0))
+
+    def stepLaunches(self) -> int:
+        """Kernels launched per step (not counting the window epilogue)."""
+        n = C.c_int(0)
+        self._c(self._L.tlm_step_launches(self._h, C.byref(n)))
+        return n.value
 
     def kernelTime(self):
         ms = C.c_double(0)

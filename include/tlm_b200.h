@@ -119,6 +119,9 @@ typedef struct tlm_config {
                             huy_offset >= 2, the Huygens-box phasors that the
                             far field needs. One extra small launch per step;
                             not available for handles driven by a batch */
+    int no_staging;      /* 1: FP32 interior tiles load their pulses directly
+                            instead of through shared-memory stages filled by
+                            bulk copies; results are identical */
 } tlm_config;
 
 typedef struct tlm_solver *tlm_handle;
@@ -517,11 +520,15 @@ TLM_API tlm_status tlm_kernel_variant_info(int storage, int variant, int *nodes_
 TLM_API tlm_status tlm_get_stream(tlm_handle h, void **stream);
 /* Bytes of device memory the handle holds. */
 TLM_API tlm_status tlm_device_bytes(tlm_handle h, size_t *bytes);
-/* Kernel timing: when enabled, every step-kernel launch is bracketed by CUDA
- * events on the handle's stream; tlm_kernel_time returns the summed
- * duration and launch count since the last enable. */
+/* Kernel timing: when enabled, the kernels of every step are bracketed by
+ * CUDA events on the handle's stream; tlm_kernel_time returns the summed
+ * duration and the number of timed steps since the last enable. */
 TLM_API tlm_status tlm_set_kernel_timing(tlm_handle h, int enable);
 TLM_API tlm_status tlm_kernel_time(tlm_handle h, double *ms, long long *launches);
+/* Kernels one step launches (the FP32 step of large grids runs its staged
+ * interior tiles and the remaining tiles as two kernels; surface monitors add
+ * one); the window epilogue every steps_per_launch steps is not counted. */
+TLM_API tlm_status tlm_step_launches(tlm_handle h, int *per_step);
 
 #ifdef __cplusplus
 }

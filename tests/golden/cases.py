@@ -136,6 +136,51 @@ def interior_tiles(w, V=4, block=256):
     return int((~gen).sum())
 
 
+def staged_tiles(w, block=256):
+    """Number of FP32 tiles (2 nodes per thread) that the staged kernel takes:
+    interior tiles without a node on an outer y or z face."""
+    nx, ny, nz = w.nx, w.ny, w.nz
+    px = (nx + 7) // 8 * 8
+    T = block * 2
+    gen = _general_mask(w, 2, block)
+    edge = np.zeros(gen.size, bool)
+    plane = px * ny
+    for lo, hi in [(0, plane), ((nz - 1) * plane, nz * plane)] + \
+            [(k * plane + r, k * plane + r + px) for k in range(nz) for r in (0, (ny - 1) * px)]:
+        edge[lo // T:(hi - 1) // T + 1] = True
+    return int((~gen & ~edge).sum())
+
+
+def _general_mask(w, V, block):
+    nx, ny, nz = w.nx, w.ny, w.nz
+    px = (nx + 7) // 8 * 8
+    P = px * ny * nz
+    T = block * V
+    nb = (P // V + block - 1) // block
+    gen = np.zeros(nb, bool)
+    if (P // V) % block:
+        gen[-1] = True
+    mat = np.asarray(w.mat).reshape(nz, ny, nx)
+    for k, j, i in zip(*np.nonzero(mat == 1)):
+        n = (k * ny + j) * px + i
+        for m in (n, n - 1 if i > 0 else -1, n + 1 if i < nx - 1 else -1, n - px, n + px, n - px * ny, n + px * ny):
+            if 0 <= m < P:
+                gen[m // T] = True
+    spec = []
+    for cells, _, _ in w.ports:
+        for c in cells:
+            spec.append(c)
+            i, j, k = c % nx, (c // nx) % ny, c // (nx * ny)
+            spec += [(k * ny + j2) * nx + i2 for i2, j2 in ((i, j - 1), (i, j + 1), (i - 1, j), (i + 1, j))
+                     if 0 <= i2 < nx and 0 <= j2 < ny]
+    for (i, j, k) in w.probes_cell:
+        spec.append((k * ny + j) * nx + i)
+    for c in spec:
+        i, r = c % nx, c // nx
+        gen[(r * px + i) // T] = True
+    return gen
+
+
 def surface_cases():
     """Dipole grids with every surface monitor on: PEC-surface currents, a
     Huygens box, an |E| cut plane and playback frames, DFT from a settle step."""

@@ -1,10 +1,12 @@
 """The interior-tile body of the step kernel on a B200.
 
 Tiles away from the y/z faces, PEC and sources take a second step body (all
-pulse loads first, packed FP32x2 scatter of node pairs). On grids that hold
-such tiles: FP32 storage is bitwise the reference's CPU step (oracle), and
-for every storage mode and tile shape the interior body gives bitwise the
-state and records of the general body (tlm_config.general_tiles = 1)."""
+pulse loads first, packed FP32x2 scatter of node pairs); in FP32 those off
+the outer y/z faces are staged in shared memory by bulk copies first. On
+grids that hold such tiles: FP32 storage is bitwise the reference's CPU step
+(oracle), and for every storage mode and tile shape the interior body gives
+bitwise the state and records of the general body (tlm_config.general_tiles
+= 1), staged or not (tlm_config.no_staging = 1)."""
 import numpy as np
 import pytest
 
@@ -12,7 +14,8 @@ from emsolver_b200 import _lib
 from emsolver_b200.runner import build_solver, records
 from emsolver_b200.solver import Storage
 from oracle import Oracle, drive
-from tests.golden.cases import interior_tiles, mid_cases
+from emsolver_b200 import workloads
+from tests.golden.cases import interior_tiles, mid_cases, staged_tiles
 
 pytestmark = pytest.mark.gpu
 
@@ -22,6 +25,32 @@ MID = mid_cases()
 def test_mid_cases_hold_interior_tiles():
     for w in MID:
         assert interior_tiles(w) > 0 and interior_tiles(w, V=2) > 0 and interior_tiles(w, V=8) > 0
+        assert staged_tiles(w) > 0
+
+
+@pytest.mark.parametrize("case", ["heterogeneous", "mid", "air_odd"])
+def test_staged_tiles_equal_direct_loads(built, case):
+    """Staged FP32 interior tiles against the same tiles loading directly:
+    pulses, stubs and every record (energy included) bitwise."""
+    if case == "heterogeneous":
+        w = workloads.heterogeneous(n=96, steps=48)
+    elif case == "mid":
+        w = MID[0]
+    else:
+        w = workloads.dipole(61, 70, 33, 20, slab=(3, 12, 4.0), steps=40, name="odd")
+    assert staged_tiles(w) > 0
+    out = []
+    for no_staging in (True, False):
+        s = build_solver(w, no_staging=no_staging)
+        s.step(w.steps)
+        out.append((s.pulses(), s.stubs() if w.table else None, records(s, w, f64=True)))
+        s.close()
+    (pa, sa, ra), (pb, sb, rb) = out
+    assert np.array_equal(pa, pb)
+    if sa is not None:
+        assert np.array_equal(sa, sb)
+    for k in ra:
+        assert np.array_equal(ra[k], rb[k]), k
 
 
 @pytest.mark.parametrize("w", MID, ids=[w.name for w in MID])
