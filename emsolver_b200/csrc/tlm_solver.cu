@@ -201,21 +201,31 @@ tlm_status checkSlabMonitors(tlm_solver *h)
     return TLM_OK;
 }
 
-// FP32 in the default tile shape: interior tiles off the outer y/z faces go
-// to the staged kernel, every other tile to the list kernel, both launched
-// every step (tlm_config.no_staging = 1: the single step kernel as before).
+template <class S> tlm_status stagedAttributes(tlm_solver *h)
+{
+    return h->cuda(cudaFuncSetAttribute(tlmk::stepKernelStaged<S, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        tlmk::kStages * tlmk::Stage<S>::kBytes),
+                   "cudaFuncSetAttribute(stepKernelStaged)");
+}
+
+// FP32 with 2 nodes per thread (the default shape): interior tiles off the
+// outer y/z faces go to the staged kernel, every other tile to the list
+// kernel, both launched every step (tlm_config.no_staging = 1: the single
+// step kernel as before). The 16-bit storage types are bound by instruction
+// issue, not by load latency: staged, they measured slower than their own
+// default shape, so they keep the single kernel.
 tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
 {
     h->nStaged = h->nListed = 0;
-    if (h->storage != TLM_STORE_F32 || h->variant != 0 || h->cfg.no_staging || h->V != 2) return TLM_OK;
+    if (h->storage != TLM_STORE_F32 || h->cfg.no_staging || h->V != 2 || !shapeOf(h->storage, h->variant).select)
+        return TLM_OK;
     std::vector<int> staged, listed;
     for (int t = 0; t < h->nblocks; ++t)
         ((flags[(size_t)t] & (tlmk::kTileGeneral | tlmk::kTileEdge)) ? listed : staged).push_back(t);
     if (staged.empty()) return TLM_OK;
     int sms = 0;
     TLM_CU(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-    TLM_CU(h, cudaFuncSetAttribute(tlmk::stepKernelStaged<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tlmk::kStages * tlmk::kStageBytes));
+    TLM_TRY(stagedAttributes<float>(h));
     if (!h->side)
     {
         TLM_CU(h, cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
@@ -466,11 +476,11 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
             {
                 TLM_CU(h, cudaEventRecord(h->evFork, h->stream));
                 TLM_CU(h, cudaStreamWaitEvent(h->side, h->evFork, 0));
-                tlmk::stepKernelList<float, 2, 4, true><<<h->nListed, kBlock, 0, h->side>>>(a, h->dListed);
+                tlmk::stepKernelList<S, 2, 4, true><<<h->nListed, kBlock, 0, h->side>>>(a, h->dListed);
                 TLM_CU(h, cudaEventRecord(h->evJoin, h->side));
             }
-            tlmk::stepKernelStaged<2><<<h->stagedGrid, tlmk::kStagedThreads, tlmk::kStages * tlmk::kStageBytes,
-                                        h->stream>>>(a, h->dStaged, h->nStaged);
+            tlmk::stepKernelStaged<S, 2><<<h->stagedGrid, tlmk::kStagedThreads, tlmk::kStages * tlmk::Stage<S>::kBytes,
+                                           h->stream>>>(a, h->dStaged, h->nStaged);
             if (h->nListed > 0) TLM_CU(h, cudaStreamWaitEvent(h->stream, h->evJoin, 0));
         }
         else

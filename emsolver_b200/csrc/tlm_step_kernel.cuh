@@ -148,19 +148,26 @@ template <int V> __device__ __forceinline__ unsigned pecMask(const uint8_t (&m)[
     return r;
 }
 
-// Shared-memory stage of one FP32 tile of kBlock node pairs, filled by bulk
-// copies (stepKernelStaged): slots 0..3 at the tile's own nodes with 4 nodes
-// of halo on each side (the x neighbours), then the eight y/z neighbour
-// segments in the order of inc[4..11] (slot 6+t one row below, 4+t one row
-// above, 10+t one plane below, 8+t one plane above), the three stub planes,
-// and the material bytes. Offsets in floats, except kStageOffMat (bytes).
+// Shared-memory stage of one tile of kBlock node pairs (storage S: FP32,
+// FP16 or BF16), filled by bulk copies (stepKernelStaged): slots 0..3 at the
+// tile's own nodes with 16 bytes of halo on each side (the x neighbours),
+// then the eight y/z neighbour segments in the order of inc[4..11] (slot 6+t
+// one row below, 4+t one row above, 10+t one plane below, 8+t one plane
+// above), the three FP32 stub planes, and the material bytes. Offsets in
+// bytes; every segment starts and ends on a 16-byte boundary.
 constexpr int kStageNodes = kBlock * 2;
-constexpr int kStageSegX = kStageNodes + 8;
-constexpr int kStageOffYZ = 4 * kStageSegX;
-constexpr int kStageOffStub = kStageOffYZ + 8 * kStageNodes;
-constexpr int kStageOffMat = (kStageOffStub + 3 * kStageNodes) * 4;
-constexpr int kStageBytes = kStageOffMat + kStageNodes;
-static_assert(kStageBytes % 16 == 0 && (kStageSegX * 4) % 16 == 0, "bulk copies need 16-byte multiples");
+template <class S> struct Stage
+{
+    static constexpr int kElem = (int)sizeof(S);
+    static constexpr int kHalo = 16 / kElem;                // nodes of x halo on each side
+    static constexpr int kSegX = kStageNodes + 2 * kHalo;   // elements of an x segment
+    static constexpr int kOffYZ = 4 * kSegX * kElem;
+    static constexpr int kOffStub = kOffYZ + 8 * kStageNodes * kElem;
+    static constexpr int kOffMat = kOffStub + 3 * kStageNodes * 4;
+    static constexpr int kBytes = kOffMat + kStageNodes;
+    static_assert(kBytes % 16 == 0 && (kSegX * kElem) % 16 == 0 && kOffYZ % 16 == 0 && kOffStub % 16 == 0,
+                  "bulk copies need 16-byte multiples");
+};
 
 constexpr int kStages = 3;
 constexpr int kStagedThreads = kBlock + 32;
@@ -209,8 +216,8 @@ __device__ __forceinline__ void bulkCopy(unsigned dst, const void *src, unsigned
 // of a row, and the row padding: fixed up per node). Pairs of nodes scatter
 // with packed FP32x2 arithmetic. The results are bitwise those of the
 // general tile body below. kStaged: the tile's inputs are already in the
-// shared-memory stage `sm` (see kStageBytes; FP32, V = 2, and the tile has no
-// node on an outer y or z face); the arithmetic is the same.
+// shared-memory stage `sm` (see Stage; V = 2, and the tile has no node on an
+// outer y or z face); the arithmetic is the same.
 template <class S, int V, bool kStaged = false>
 __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel,
                                                  const unsigned char *sm = nullptr, unsigned eBar = 0,
@@ -236,28 +243,22 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     R prevX[2], nextX[2];
     if constexpr (kStaged)
     {
-        static_assert(std::is_same<S, float>::value && V == 2, "staged tiles hold FP32 node pairs");
-        const float *X = reinterpret_cast<const float *>(sm);
+        static_assert(V == 2 && (std::is_same<S, float>::value || std::is_same<S, __half>::value ||
+                                 std::is_same<S, __nv_bfloat16>::value),
+                      "staged tiles hold node pairs of FP32, FP16 or BF16");
+        using L = Stage<S>;
+        const S *X = reinterpret_cast<const S *>(sm);
+        const S *YZ = reinterpret_cast<const S *>(sm + L::kOffYZ);
         const int l = threadIdx.x * V;
 #pragma unroll
-        for (int s = 0; s < 4; ++s)
-        {
-            const float2 v = *reinterpret_cast<const float2 *>(X + s * kStageSegX + 4 + l);
-            ox[s][0] = v.x;
-            ox[s][1] = v.y;
-        }
+        for (int s = 0; s < 4; ++s) loadVec<S, V>(X + s * L::kSegX + L::kHalo, l, ox[s], a.scale);
 #pragma unroll
-        for (int g = 0; g < 8; ++g)
-        {
-            const float2 v = *reinterpret_cast<const float2 *>(X + kStageOffYZ + g * kStageNodes + l);
-            inc[4 + g][0] = v.x;
-            inc[4 + g][1] = v.y;
-        }
+        for (int g = 0; g < 8; ++g) loadVec<S, V>(YZ + g * kStageNodes, l, inc[4 + g], a.scale);
 #pragma unroll
         for (int t = 0; t < 2; ++t)
         {
-            prevX[t] = X[(2 + t) * kStageSegX + 3 + l];
-            nextX[t] = X[t * kStageSegX + 4 + l + V];
+            prevX[t] = loadOne<S>(X + (2 + t) * L::kSegX + L::kHalo, l - 1, a.scale);
+            nextX[t] = loadOne<S>(X + t * L::kSegX + L::kHalo, l + V, a.scale);
         }
         (void)lane;
     }
@@ -389,7 +390,7 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
         if constexpr (kStaged)
         {
 #pragma unroll
-            for (int c = 0; c < V; ++c) m[c] = sm[kStageOffMat + threadIdx.x * V + c];
+            for (int c = 0; c < V; ++c) m[c] = sm[Stage<S>::kOffMat + threadIdx.x * V + c];
         }
         else
             loadMat<V>(a.mat, node0, m);
@@ -411,7 +412,7 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
         {
             Pack<R, V> p;
             if constexpr (kStaged)
-                p = *reinterpret_cast<const Pack<R, V> *>(reinterpret_cast<const float *>(sm) + kStageOffStub +
+                p = *reinterpret_cast<const Pack<R, V> *>(reinterpret_cast<const float *>(sm + Stage<S>::kOffStub) +
                                                           jj * kStageNodes + threadIdx.x * V);
             else
                 p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
@@ -947,7 +948,7 @@ __global__ void __launch_bounds__(kBlock, MINB) stepKernelList(const StepArgs<S>
     stepTile<S, V, false, kSelect>(a, tiles[blockIdx.x], red);
 }
 
-// ---- staged interior tiles (FP32) -------------------------------------------
+// ---- staged interior tiles (FP32, FP16, BF16) ------------------------------
 // Interior tiles without a node on an outer y or z face, each staged in shared
 // memory by bulk copies (the tensor-memory-access engine) before the interior
 // body runs on it. A block of kBlock consumer threads and one producer warp
@@ -960,17 +961,19 @@ __global__ void __launch_bounds__(kBlock, MINB) stepKernelList(const StepArgs<S>
 // sets kStageTimeout in *a.fault and ends its thread; the producer first lets
 // the copies it issued land (again bounded), and the host reports the error.
 // Issue the copies of `tile` into the stage at `st` (one thread).
-__device__ __forceinline__ void stageTile(const StepArgs<float> &a, int tile, unsigned st, unsigned bar)
+template <class S>
+__device__ __forceinline__ void stageTile(const StepArgs<S> &a, int tile, unsigned st, unsigned bar)
 {
+    using L = Stage<S>;
     const long long node0 = (long long)tile * kStageNodes;
     const long long P = a.P, sy = a.px, sz = (long long)a.px * a.ny;
     const bool diel = (a.tile_flags[tile] & kTileDiel) != 0 && a.stub != nullptr;
-    const unsigned segX = kStageSegX * 4, seg = kStageNodes * 4;
-    const unsigned bytes = 4 * segX + 8 * seg + (diel ? 3 * seg : 0) + kStageNodes;
+    const unsigned segX = L::kSegX * L::kElem, seg = kStageNodes * L::kElem, stubSeg = kStageNodes * 4;
+    const unsigned bytes = 4 * segX + 8 * seg + (diel ? 3 * stubSeg : 0) + kStageNodes;
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" : : "r"(bar), "r"(bytes) : "memory");
 #pragma unroll
-    for (int s = 0; s < 4; ++s) bulkCopy(st + s * segX, a.in + s * P + node0 - 4, segX, bar);
-    const unsigned yz = st + kStageOffYZ * 4;
+    for (int s = 0; s < 4; ++s) bulkCopy(st + s * segX, a.in + s * P + node0 - L::kHalo, segX, bar);
+    const unsigned yz = st + L::kOffYZ;
 #pragma unroll
     for (int t = 0; t < 2; ++t)
     {
@@ -982,16 +985,16 @@ __device__ __forceinline__ void stageTile(const StepArgs<float> &a, int tile, un
     if (diel)
     {
 #pragma unroll
-        for (int jj = 0; jj < 3; ++jj)
-            bulkCopy(st + (kStageOffStub + jj * kStageNodes) * 4, a.stub + jj * P + node0, seg, bar);
+        for (int jj = 0; jj < 3; ++jj) bulkCopy(st + L::kOffStub + jj * stubSeg, a.stub + jj * P + node0, stubSeg, bar);
     }
-    bulkCopy(st + kStageOffMat, a.mat + node0, kStageNodes, bar);
+    bulkCopy(st + L::kOffMat, a.mat + node0, kStageNodes, bar);
 }
 
-template <int V, int STAGES = kStages, int MINB = 2>
+template <class S, int V, int STAGES = kStages, int MINB = 2>
 __global__ void __launch_bounds__(kStagedThreads, MINB)
-    stepKernelStaged(const StepArgs<float> a, const int *__restrict__ tiles, int ntiles)
+    stepKernelStaged(const StepArgs<S> a, const int *__restrict__ tiles, int ntiles)
 {
+    constexpr int kBytes = Stage<S>::kBytes;
     static_assert(V == 2, "a stage holds kBlock node pairs");
     extern __shared__ __align__(128) unsigned char stage[];
     __shared__ double red[STAGES][kBlock / 32];
@@ -1022,7 +1025,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
                 if (a.fault) atomicOr(a.fault, kStageTimeout);
                 break;
             }
-            stageTile(a, tiles[blockIdx.x + i * gridDim.x], st0 + s * kStageBytes, full0 + 8 * s);
+            stageTile(a, tiles[blockIdx.x + i * gridDim.x], st0 + s * kBytes, full0 + 8 * s);
             issued = i + 1;
         }
         // the copies of the last STAGES tiles may still be landing: stay
@@ -1040,8 +1043,8 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             return;
         }
         const int tile = tiles[blockIdx.x + i * gridDim.x];
-        stepTileInterior<float, V, true>(a, tile, red[s], (a.tile_flags[tile] & kTileDiel) != 0,
-                                          stage + s * kStageBytes, ered0 + 8 * s, (unsigned)(i / STAGES) & 1u);
+        stepTileInterior<S, V, true>(a, tile, red[s], (a.tile_flags[tile] & kTileDiel) != 0, stage + s * kBytes,
+                                      ered0 + 8 * s, (unsigned)(i / STAGES) & 1u);
         __syncwarp();
         if ((threadIdx.x & 31) == 0)
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(empty0 + 8 * s) : "memory");

@@ -28,10 +28,23 @@ def test_mid_cases_hold_interior_tiles():
         assert staged_tiles(w) > 0
 
 
+def pair_variant(storage):
+    """The tile shape with 2 nodes per thread and the select scatter (the one
+    staged tiles run in)."""
+    L = _lib.load()
+    for v in range(L.tlm_kernel_variants(int(storage))):
+        V, minb = _lib.C.c_int(0), _lib.C.c_int(0)
+        L.tlm_kernel_variant_info(int(storage), v, _lib.C.byref(V), _lib.C.byref(minb))
+        if V.value == 2 and minb.value == 4:
+            return v
+    raise AssertionError("no 2-node shape")
+
+
+@pytest.mark.parametrize("storage", [Storage.F32])
 @pytest.mark.parametrize("case", ["heterogeneous", "mid", "air_odd"])
-def test_staged_tiles_equal_direct_loads(built, case):
-    """Staged FP32 interior tiles against the same tiles loading directly:
-    pulses, stubs and every record (energy included) bitwise."""
+def test_staged_tiles_equal_direct_loads(built, case, storage):
+    """Staged interior tiles against the same tiles loading directly: pulses,
+    stubs and every record (energy included) bitwise."""
     if case == "heterogeneous":
         w = workloads.heterogeneous(n=96, steps=48)
     elif case == "mid":
@@ -40,8 +53,9 @@ def test_staged_tiles_equal_direct_loads(built, case):
         w = workloads.dipole(61, 70, 33, 20, slab=(3, 12, 4.0), steps=40, name="odd")
     assert staged_tiles(w) > 0
     out = []
+    v = pair_variant(storage)
     for no_staging in (True, False):
-        s = build_solver(w, no_staging=no_staging)
+        s = build_solver(w, storage=storage, kernel_variant=v, no_staging=no_staging)
         s.step(w.steps)
         out.append((s.pulses(), s.stubs() if w.table else None, records(s, w, f64=True)))
         s.close()
