@@ -121,6 +121,127 @@ __global__ void __launch_bounds__(kBlock, MINB)
     }
 }
 
+// Staged tiles of an FP32 batch group (2 nodes per thread): the single-grid
+// staged kernel's pipeline over the (member, tile) pairs of every member's
+// staged tiles. The producer lane builds the tile's member arguments for
+// this step into the stage next to the pulses (so the consumers read them
+// from shared memory), or marks the stage empty when the member is past its
+// last step. Energy steps differ between members, so each consumer counts
+// its own uses of every stage's energy barrier (the same sequence in every
+// thread).
+template <int STAGES = kStages, int MINB = 2>
+__global__ void __launch_bounds__(kStagedThreads, MINB)
+    batchStepKernelStaged(MemberDesc<float> *__restrict__ members, const int2 *__restrict__ tiles,
+                          const int *__restrict__ ntiles, int i, unsigned *fault)
+{
+    constexpr int kData = Stage<float>::kBytes;
+    constexpr int kSlot = kData + (int)((sizeof(StepArgs<float>) + 15) / 16 * 16);
+    extern __shared__ __align__(128) unsigned char stage[];
+    __shared__ double red[STAGES][kBlock / 32];
+    __shared__ __align__(8) unsigned long long full[STAGES], empty[STAGES], ered[STAGES];
+    const int nt = *ntiles;
+    const int mine = nt > (int)blockIdx.x ? (nt - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+    const unsigned st0 = smemAddr(stage), full0 = smemAddr(full), empty0 = smemAddr(empty), ered0 = smemAddr(ered);
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < STAGES; ++s)
+        {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" : : "r"(full0 + 8 * s) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(empty0 + 8 * s), "n"(kBlock / 32) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(ered0 + 8 * s), "n"(kBlock / 32) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" : : : "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x >= kBlock)
+    {
+        if (threadIdx.x != kBlock) return;
+        int issued = 0;
+        for (int it = 0; it < mine; ++it)
+        {
+            const int s = it % STAGES;
+            if (it >= STAGES && !mbarWaitBounded(empty0 + 8 * s, (unsigned)(it / STAGES - 1) & 1u))
+            {
+                if (fault) atomicOr(fault, kStageTimeout);
+                break;
+            }
+            const int2 tl = tiles[blockIdx.x + it * gridDim.x];
+            const MemberDesc<float> &d = members[tl.x];
+            StepArgs<float> *sa = reinterpret_cast<StepArgs<float> *>(stage + s * kSlot + kData);
+            const long long n = d.base + i;
+            const unsigned bar = full0 + 8 * s;
+            if (n >= d.total)
+            {
+                sa->nquads = -1;  // the member has finished: an empty stage
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(bar) : "memory");
+            }
+            else
+            {
+                StepArgs<float> a;
+                const long long eFirst = (d.base + 15) / 16 * 16;
+                a.in = d.buf[n & 1];
+                a.out = d.buf[(n + 1) & 1];
+                a.stub = d.stub;
+                a.mat = d.mat;
+                a.yhat = d.yhat;
+                a.ghat = d.ghat;
+                a.P = d.P;
+                a.nquads = d.nquads;
+                a.nx = d.nx;
+                a.ny = d.ny;
+                a.nz = d.nz;
+                a.px = d.px;
+                a.nq = d.nq;
+                a.div_nq = d.div_nq;
+                a.div_ny = d.div_ny;
+                a.rho = d.rho;
+                a.scale = d.scale;
+                a.inv_scale = d.inv_scale;
+                a.tile_begin = d.tile_begin;
+                a.spec = d.spec;
+                a.tile_flags = d.tile_flags;
+                a.neg_zero = d.neg_zero;
+                a.sv = d.sv[n];
+                a.samples = d.samples + (long long)i * d.nsamp * 6;
+                a.epart = (n % 16 == 0) ? d.epart + ((n - eFirst) / 16) * d.nblocks : nullptr;
+                a.e_lo = 0;
+                a.e_hi = LLONG_MAX;
+                a.fault = fault;
+                a.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
+                a.stochastic = d.stochastic;
+                *sa = a;
+                stageTile(a, tl.y, st0 + s * kSlot, bar);
+            }
+            issued = it + 1;
+        }
+        for (int it = issued > STAGES ? issued - STAGES : 0; it < issued; ++it)
+            mbarWaitBounded(full0 + 8 * (it % STAGES), (unsigned)(it / STAGES) & 1u);
+        return;
+    }
+    unsigned eBits = 0;
+    for (int it = 0; it < mine; ++it)
+    {
+        const int s = it % STAGES;
+        if (!mbarWaitBounded(full0 + 8 * s, (unsigned)(it / STAGES) & 1u))
+        {
+            if (fault) atomicOr(fault, kStageTimeout);
+            return;
+        }
+        const StepArgs<float> &a = *reinterpret_cast<const StepArgs<float> *>(stage + s * kSlot + kData);
+        if (a.nquads >= 0)
+        {
+            const int tile = tiles[blockIdx.x + it * gridDim.x].y;
+            const unsigned ep = (eBits >> s) & 1u;
+            if (a.epart != nullptr) eBits ^= 1u << s;
+            stepTileInterior<float, 2, true>(a, tile, red[s], (a.tile_flags[tile] & kTileDiel) != 0,
+                                             stage + s * kSlot, ered0 + 8 * s, ep);
+        }
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0)
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(empty0 + 8 * s) : "memory");
+    }
+}
+
 // One block of 512 threads per member: the window's records, DFT and energy
 // (the same body and block size as the single-grid epilogue, so even the
 // FP64 energy sums round identically), then the member's base moves to the

@@ -217,6 +217,8 @@ template <class S> tlm_status stagedAttributes(tlm_solver *h)
 tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
 {
     h->nStaged = h->nListed = 0;
+    h->stagedTiles.clear();
+    h->listedTiles.clear();
     if (h->storage != TLM_STORE_F32 || h->cfg.no_staging || h->V != 2 || !shapeOf(h->storage, h->variant).select)
         return TLM_OK;
     std::vector<int> staged, listed;
@@ -243,6 +245,8 @@ tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
     }
     h->nStaged = (int)staged.size();
     h->nListed = (int)listed.size();
+    h->stagedTiles = std::move(staged);
+    h->listedTiles = std::move(listed);
     h->stagedGrid = std::min(h->nStaged, 2 * sms);
     return TLM_OK;
 }
