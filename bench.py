@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--steps-max", type=int, default=2000,
                    help="served: most steps per request (the full stream goes to 8000)")
     p.add_argument("--autotune", action="store_true", help="batched: run the autotuner first")
+    p.add_argument("--chunk", type=int, default=32, help="batched: instances set up per window")
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64", "bfp16"])
     p.add_argument("--steps-per-launch", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
@@ -407,6 +408,14 @@ def run_batched(args):
     bytes_all = sum(w.bytes_per_step() * w.steps for w in ws)
     sequential_solves(ws[:4])                        # warm-up (context, kernels)
     seq = sequential_solves(ws)
+    # the solves through Batch.solve: set-up of the next instances overlaps
+    # the device's windows, finished members leave at once
+    tp = time.perf_counter()
+    with Batch() as bp:
+        dfts = bp.solve(ws, build_solver, lambda s, w: s.portDft(0), chunk=args.chunk)
+    pipelined_s = time.perf_counter() - tp
+    assert len(dfts) == len(ws)
+    # all instances attached at once, the device time of the whole run
     t0 = time.perf_counter()
     solvers = [build_solver(w) for w in ws]
     tb = time.perf_counter()
@@ -433,7 +442,7 @@ def run_batched(args):
     batched_s = t3 - t0
     peak, kind = peaks()
     line = {
-        "metric": "batched solves/s", "value": len(ws) / batched_s, "unit": "solves/s",
+        "metric": "batched solves/s", "value": len(ws) / pipelined_s, "unit": "solves/s",
         "n_gpus": 1, "steps": 1000, "warmup": 4, "ms_per_step": gpu_ms / 1000.0,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
@@ -443,7 +452,11 @@ def run_batched(args):
         "sequential_plain_gpu": {"value": len(ws) / sum(seq), "unit": "solves/s",
                                  "seconds": sum(seq), "p50_s": float(np.percentile(seq, 50)),
                                  "p99_s": float(np.percentile(seq, 99))},
-        "speedup_vs_sequential": sum(seq) / batched_s,
+        "speedup_vs_sequential": sum(seq) / pipelined_s,
+        "pipelined": {"seconds": pipelined_s, "chunk": args.chunk,
+                      "api": "Batch.solve: host set-up of the next chunk overlaps each window"},
+        "all_attached": {"value": len(ws) / batched_s, "unit": "solves/s", "seconds": batched_s,
+                         "speedup_vs_sequential": sum(seq) / batched_s},
         "batched_gpu": {"node_updates_per_s": work / (gpu_ms / 1e3), "seconds": gpu_ms / 1e3,
                         "setup_s": t1 - t0, "setup_build_s": tb - t0, "setup_attach_s": ta - tb,
                         "readback_s": t2 - t1 - gpu_ms / 1e3,

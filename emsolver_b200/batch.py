@@ -67,6 +67,48 @@ class Batch:
     def run(self):
         self._c(self._L.tlm_batch_run(self._b))
 
+    def launch_window(self) -> int:
+        """Queue one window without waiting; returns its length in steps (0
+        when no member is active). Call sync() before attaching, detaching
+        or reading members."""
+        n = C.c_int(0)
+        self._c(self._L.tlm_batch_launch_window(self._b, C.byref(n)))
+        return n.value
+
+    def sync(self):
+        self._c(self._L.tlm_batch_sync(self._b))
+
+    def solve(self, workloads, build, collect, chunk: int = 32):
+        """Solve every workload through this batch and return collect(solver,
+        workload) for each, in order. While the device runs a window for the
+        attached members, the host sets up (build(w), then prepares the
+        solver's tables) the next `chunk` workloads, which join at the next
+        window; a member that reaches its last step is collected, detached
+        and closed at once, so its device memory serves the next ones."""
+        pending = list(enumerate(workloads))
+        running = {}
+        out = [None] * len(pending)
+        while pending or running:
+            launched = self.launch_window() if running else 0
+            fresh = []
+            for k, w in pending[:chunk]:
+                s = build(w)
+                s.stepAsync(0)  # builds the source/monitor and tile tables now, on the host
+                fresh.append((k, w, s))
+            pending = pending[chunk:]
+            if launched:
+                self.sync()
+            for k, w, s in fresh:
+                self.attach(s)
+                running[k] = (w, s)
+            for k, (w, s) in list(running.items()):
+                if s.currentStep() >= s.totalSteps():
+                    out[k] = collect(s, w)
+                    self.detach(s)
+                    s.close()
+                    del running[k]
+        return out
+
     def set_tuning(self, t: BatchTuning):
         c = t.to_c()
         self._c(self._L.tlm_batch_set_tuning(self._b, C.byref(c)))

@@ -764,6 +764,13 @@ tlm_status tlm_batch_sync(tlm_batch b)
     }
     BatchDeviceGuard dg(b->device);
     TLM_BCU(b, cudaStreamSynchronize(b->stream));
+    if (b->dFault)
+    {
+        unsigned f = 0;
+        TLM_BCU(b, cudaMemcpy(&f, b->dFault, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (f & tlmk::kStageTimeout) return b->fail(TLM_ECUDA, "a staged tile's bulk copies never arrived");
+        if (f) return b->fail(TLM_ECUDA, "bounds check tripped in the batched kernel, mask " + std::to_string(f));
+    }
     for (auto &kv : b->groups)
         for (tlm_solver *h : kv.second.members)
         {

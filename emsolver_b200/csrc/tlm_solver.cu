@@ -739,6 +739,14 @@ cudaMemPool_t devicePool(int device)
         }
         uint64_t keep = UINT64_MAX;  // keep freed blocks for reuse
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        // no opportunistic reuse: with it, every allocation weighs the freed
+        // blocks of other streams one by one, and once a few thousand are
+        // cached (256 handles set up and freed) setting up a handle's 25
+        // buffers took 9 ms instead of 0.07 ms (measured on B200). Blocks
+        // freed on other streams are still reused, through an event
+        // dependency on their free.
+        int opportunistic = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &opportunistic);
         pools[device] = pool;
     }
     return pools[device];
