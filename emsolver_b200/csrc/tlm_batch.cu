@@ -236,10 +236,17 @@ tlm_status syncGroupTables(tlm_batch_s *b, Group &g)
         }
         if (h->curStep < h->cfg.total_steps)
         {
-            if (stagedGroup(g) && h->nStaged > 0)
+            if (stagedGroup(g) && h->nStaged + (int)h->edgeTiles.size() > 0)
             {
-                for (int t : h->stagedTiles) staged.push_back(make_int2(m, t));
-                for (int t : h->listedTiles) tiles.push_back(make_int2(m, t));
+                // every interior tile is staged, those on outer faces included
+                std::vector<int> mine(h->stagedTiles);
+                mine.insert(mine.end(), h->edgeTiles.begin(), h->edgeTiles.end());
+                std::sort(mine.begin(), mine.end());
+                for (int t : mine) staged.push_back(make_int2(m, t));
+                std::vector<char> isStaged((size_t)h->nblocks, 0);
+                for (int t : mine) isStaged[(size_t)t] = 1;
+                for (int t = 0; t < h->nblocks; ++t)
+                    if (!isStaged[(size_t)t]) tiles.push_back(make_int2(m, t));
             }
             else
                 for (int t = 0; t < h->nblocks; ++t) tiles.push_back(make_int2(m, t));

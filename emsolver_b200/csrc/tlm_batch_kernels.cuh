@@ -155,14 +155,18 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
     __syncthreads();
     if (threadIdx.x >= kBlock)
     {
-        if (threadIdx.x != kBlock) return;
+        // producer warp: lane 0 writes the member arguments, then every lane
+        // issues its share of the copies
+        const int lane = threadIdx.x - kBlock;
         int issued = 0;
         for (int it = 0; it < mine; ++it)
         {
             const int s = it % STAGES;
-            if (it >= STAGES && !mbarWaitBounded(empty0 + 8 * s, (unsigned)(it / STAGES - 1) & 1u))
+            bool ok = true;
+            if (it >= STAGES && lane == 0) ok = mbarWaitBounded(empty0 + 8 * s, (unsigned)(it / STAGES - 1) & 1u);
+            if (!__shfl_sync(0xffffffffu, ok, 0))
             {
-                if (fault) atomicOr(fault, kStageTimeout);
+                if (lane == 0 && fault) atomicOr(fault, kStageTimeout);
                 break;
             }
             const int2 tl = tiles[blockIdx.x + it * gridDim.x];
@@ -172,50 +176,58 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             const unsigned bar = full0 + 8 * s;
             if (n >= d.total)
             {
-                sa->nquads = -1;  // the member has finished: an empty stage
-                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(bar) : "memory");
+                if (lane == 0)
+                {
+                    sa->nquads = -1;  // the member has finished: an empty stage
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(bar) : "memory");
+                }
             }
             else
             {
-                StepArgs<float> a;
-                const long long eFirst = (d.base + 15) / 16 * 16;
-                a.in = d.buf[n & 1];
-                a.out = d.buf[(n + 1) & 1];
-                a.stub = d.stub;
-                a.mat = d.mat;
-                a.yhat = d.yhat;
-                a.ghat = d.ghat;
-                a.P = d.P;
-                a.nquads = d.nquads;
-                a.nx = d.nx;
-                a.ny = d.ny;
-                a.nz = d.nz;
-                a.px = d.px;
-                a.nq = d.nq;
-                a.div_nq = d.div_nq;
-                a.div_ny = d.div_ny;
-                a.rho = d.rho;
-                a.scale = d.scale;
-                a.inv_scale = d.inv_scale;
-                a.tile_begin = d.tile_begin;
-                a.spec = d.spec;
-                a.tile_flags = d.tile_flags;
-                a.neg_zero = d.neg_zero;
-                a.sv = d.sv[n];
-                a.samples = d.samples + (long long)i * d.nsamp * 6;
-                a.epart = (n % 16 == 0) ? d.epart + ((n - eFirst) / 16) * d.nblocks : nullptr;
-                a.e_lo = 0;
-                a.e_hi = LLONG_MAX;
-                a.fault = fault;
-                a.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
-                a.stochastic = d.stochastic;
-                *sa = a;
-                stageTile(a, tl.y, st0 + s * kSlot, bar);
+                if (lane == 0)
+                {
+                    StepArgs<float> a;
+                    const long long eFirst = (d.base + 15) / 16 * 16;
+                    a.in = d.buf[n & 1];
+                    a.out = d.buf[(n + 1) & 1];
+                    a.stub = d.stub;
+                    a.mat = d.mat;
+                    a.yhat = d.yhat;
+                    a.ghat = d.ghat;
+                    a.P = d.P;
+                    a.nquads = d.nquads;
+                    a.nx = d.nx;
+                    a.ny = d.ny;
+                    a.nz = d.nz;
+                    a.px = d.px;
+                    a.nq = d.nq;
+                    a.div_nq = d.div_nq;
+                    a.div_ny = d.div_ny;
+                    a.rho = d.rho;
+                    a.scale = d.scale;
+                    a.inv_scale = d.inv_scale;
+                    a.tile_begin = d.tile_begin;
+                    a.spec = d.spec;
+                    a.tile_flags = d.tile_flags;
+                    a.neg_zero = d.neg_zero;
+                    a.sv = d.sv[n];
+                    a.samples = d.samples + (long long)i * d.nsamp * 6;
+                    a.epart = (n % 16 == 0) ? d.epart + ((n - eFirst) / 16) * d.nblocks : nullptr;
+                    a.e_lo = 0;
+                    a.e_hi = LLONG_MAX;
+                    a.fault = fault;
+                    a.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
+                    a.stochastic = d.stochastic;
+                    *sa = a;
+                }
+                __syncwarp();
+                stageTile(*sa, tl.y, st0 + s * kSlot, bar, lane);
             }
             issued = it + 1;
         }
-        for (int it = issued > STAGES ? issued - STAGES : 0; it < issued; ++it)
-            mbarWaitBounded(full0 + 8 * (it % STAGES), (unsigned)(it / STAGES) & 1u);
+        if (lane == 0)
+            for (int it = issued > STAGES ? issued - STAGES : 0; it < issued; ++it)
+                mbarWaitBounded(full0 + 8 * (it % STAGES), (unsigned)(it / STAGES) & 1u);
         return;
     }
     unsigned eBits = 0;

@@ -208,9 +208,9 @@ template <class S> tlm_status stagedAttributes(tlm_solver *h)
                    "cudaFuncSetAttribute(stepKernelStaged)");
 }
 
-// FP32 with 2 nodes per thread (the default shape): interior tiles off the
-// outer y/z faces go to the staged kernel, every other tile to the list
-// kernel, both launched every step (tlm_config.no_staging = 1: the single
+// FP32 with 2 nodes per thread (the default shape): interior tiles go to the
+// staged kernel, the others (PEC, sources, monitors, the partial last tile)
+// to the list kernel, both launched every step (tlm_config.no_staging = 1: the single
 // step kernel as before). The 16-bit storage types are bound by instruction
 // issue, not by load latency: staged, they measured slower than their own
 // default shape, so they keep the single kernel.
@@ -219,11 +219,21 @@ tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
     h->nStaged = h->nListed = 0;
     h->stagedTiles.clear();
     h->listedTiles.clear();
+    h->edgeTiles.clear();
     if (h->storage != TLM_STORE_F32 || h->cfg.no_staging || h->V != 2 || !shapeOf(h->storage, h->variant).select)
         return TLM_OK;
-    std::vector<int> staged, listed;
+    std::vector<int> staged, listed, edge;
     for (int t = 0; t < h->nblocks; ++t)
-        ((flags[(size_t)t] & (tlmk::kTileGeneral | tlmk::kTileEdge)) ? listed : staged).push_back(t);
+    {
+        const uint8_t f = flags[(size_t)t];
+        ((f & tlmk::kTileGeneral) ? listed : (f & tlmk::kTileEdge) ? edge : staged).push_back(t);
+    }
+    // interior tiles on an outer face cost the producer more (their segments
+    // come in runs); alone on the device they run in the list kernel, which
+    // overlaps the staged one, while a batch stages them too (edgeTiles)
+    h->edgeTiles = edge;
+    listed.insert(listed.end(), edge.begin(), edge.end());
+    std::sort(listed.begin(), listed.end());
     if (staged.empty()) return TLM_OK;
     int sms = 0;
     TLM_CU(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));

@@ -57,7 +57,8 @@ template <class S> struct StepArgs
 // thread of it is live, neither its nodes nor their six neighbours are PEC,
 // and it holds no source or monitor. kTileDiel: the tile has stub-loaded
 // nodes.
-// kTileEdge: the tile has a node on an outer y or z face.
+// kTileEdge: the tile has a node on an outer y or z face (its stage is
+// assembled from runs, see stageRuns).
 enum : uint8_t { kTileGeneral = 1, kTileDiel = 2, kTileEdge = 4 };
 
 #ifdef TLM_CHECKED
@@ -216,8 +217,8 @@ __device__ __forceinline__ void bulkCopy(unsigned dst, const void *src, unsigned
 // of a row, and the row padding: fixed up per node). Pairs of nodes scatter
 // with packed FP32x2 arithmetic. The results are bitwise those of the
 // general tile body below. kStaged: the tile's inputs are already in the
-// shared-memory stage `sm` (see Stage; V = 2, and the tile has no node on an
-// outer y or z face); the arithmetic is the same.
+// shared-memory stage `sm` (see Stage and stageRuns; V = 2), outer y/z faces
+// included; the arithmetic is the same.
 template <class S, int V, bool kStaged = false>
 __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel,
                                                  const unsigned char *sm = nullptr, unsigned eBar = 0,
@@ -960,34 +961,111 @@ __global__ void __launch_bounds__(kBlock, MINB) stepKernelList(const StepArgs<S>
 // on, so no warp waits for another. Every wait is bounded: one that runs out
 // sets kStageTimeout in *a.fault and ends its thread; the producer first lets
 // the copies it issued land (again bounded), and the host reports the error.
-// Issue the copies of `tile` into the stage at `st` (one thread).
+// The pieces of stage segment g (inc[4 + g]) for the tile at node0, as
+// (tile offset, nodes, source element) runs: a node on the segment's outer
+// face takes its own pulse of that face (the body scales it by rho), every
+// other node its neighbour's opposite pulse; runs that continue each other
+// in both places are merged, so a tile away from the outer faces has one run
+// per segment. Rows (y) and planes (z) hold multiples of 8 nodes, so every
+// run starts and ends on a 16-byte boundary.
+template <class S, class F>
+__device__ __forceinline__ void stageRuns(const StepArgs<S> &a, long long node0, int g, F &&emit)
+{
+    const bool zAxis = g >= 4, hi = ((g >> 1) & 1) != 0;
+    const int t = g & 1;
+    const long long P = a.P, sy = a.px, sz = (long long)a.px * a.ny;
+    const int faceSlot = (zAxis ? 8 : 4) + (hi ? 2 : 0) + t;
+    const int nbSlot = (zAxis ? 8 : 4) + (hi ? 0 : 2) + t;
+    const long long shift = zAxis ? (hi ? sz : -sz) : (hi ? sy : -sy);
+    const long long end = node0 + kStageNodes;
+    // row and plane of the first node (two multiply-high divisions), then
+    // rows (y) or planes (z) one after the other
+    const unsigned row0 = fastDiv((unsigned)(node0 >> 1), a.div_nq);
+    const unsigned k0 = fastDiv(row0, a.div_ny);
+    long long row = row0;
+    int j = (int)(row0 - k0 * (unsigned)a.ny), k = (int)k0;
+    long long rOff = -1, rLen = 0, rSrc = 0;
+    for (long long n = node0; n < end;)
+    {
+        long long pieceEnd;
+        bool face;
+        if (zAxis)
+        {
+            pieceEnd = min((long long)(k + 1) * sz, end);
+            face = hi ? (k == a.nz - 1) : (k == 0);
+            ++k;
+        }
+        else
+        {
+            pieceEnd = min((row + 1) * sy, end);
+            face = hi ? (j == a.ny - 1) : (j == 0);
+            ++row;
+            if (++j == a.ny) j = 0;
+        }
+        const long long src = face ? faceSlot * P + n : nbSlot * P + n + shift;
+        if (rOff >= 0 && src == rSrc + rLen)
+            rLen += pieceEnd - n;
+        else
+        {
+            if (rOff >= 0) emit((int)rOff, (int)rLen, rSrc);
+            rOff = n - node0;
+            rLen = pieceEnd - n;
+            rSrc = src;
+        }
+        n = pieceEnd;
+    }
+    emit((int)rOff, (int)rLen, rSrc);
+}
+
+// Issue the copies of `tile` into the stage at `st`, called by all 32 lanes
+// of the producer warp: lane 0 announces the byte count, then lanes 0-3 copy
+// the x segments, lanes 4-11 one y/z segment each (one copy, or its runs on
+// a tile with outer-face nodes), lanes 12-14 the stubs, lane 15 the material.
 template <class S>
-__device__ __forceinline__ void stageTile(const StepArgs<S> &a, int tile, unsigned st, unsigned bar)
+__device__ __forceinline__ void stageTile(const StepArgs<S> &a, int tile, unsigned st, unsigned bar, int lane)
 {
     using L = Stage<S>;
+    constexpr unsigned E = L::kElem;
     const long long node0 = (long long)tile * kStageNodes;
-    const long long P = a.P, sy = a.px, sz = (long long)a.px * a.ny;
-    const bool diel = (a.tile_flags[tile] & kTileDiel) != 0 && a.stub != nullptr;
-    const unsigned segX = L::kSegX * L::kElem, seg = kStageNodes * L::kElem, stubSeg = kStageNodes * 4;
-    const unsigned bytes = 4 * segX + 8 * seg + (diel ? 3 * stubSeg : 0) + kStageNodes;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" : : "r"(bar), "r"(bytes) : "memory");
-#pragma unroll
-    for (int s = 0; s < 4; ++s) bulkCopy(st + s * segX, a.in + s * P + node0 - L::kHalo, segX, bar);
-    const unsigned yz = st + L::kOffYZ;
-#pragma unroll
-    for (int t = 0; t < 2; ++t)
+    const long long P = a.P;
+    const uint8_t flags = a.tile_flags[tile];
+    const bool diel = (flags & kTileDiel) != 0 && a.stub != nullptr;
+    // x segments: the tile and L::kHalo nodes on each side, clipped to the planes
+    const long long x0 = max(node0 - L::kHalo, 0LL), x1 = min(node0 + kStageNodes + L::kHalo, P);
+    const unsigned segX = L::kSegX * E, xOff = (unsigned)(x0 - (node0 - L::kHalo)) * E;
+    const unsigned xBytes = (unsigned)(x1 - x0) * E, seg = kStageNodes * E, stubSeg = kStageNodes * 4;
+    if (lane == 0)
     {
-        bulkCopy(yz + (0 + t) * seg, a.in + (6 + t) * P + node0 - sy, seg, bar);
-        bulkCopy(yz + (2 + t) * seg, a.in + (4 + t) * P + node0 + sy, seg, bar);
-        bulkCopy(yz + (4 + t) * seg, a.in + (10 + t) * P + node0 - sz, seg, bar);
-        bulkCopy(yz + (6 + t) * seg, a.in + (8 + t) * P + node0 + sz, seg, bar);
+        const unsigned bytes = 4 * xBytes + 8 * seg + (diel ? 3 * stubSeg : 0) + kStageNodes;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" : : "r"(bar), "r"(bytes) : "memory");
     }
-    if (diel)
+    __syncwarp();
+    if (lane < 4)
+        bulkCopy(st + lane * segX + xOff, a.in + lane * P + x0, xBytes, bar);
+    else if (lane < 12)
     {
-#pragma unroll
-        for (int jj = 0; jj < 3; ++jj) bulkCopy(st + L::kOffStub + jj * stubSeg, a.stub + jj * P + node0, stubSeg, bar);
+        const int g = lane - 4;
+        const unsigned dst = st + L::kOffYZ + g * seg;
+        if (flags & kTileEdge)
+            stageRuns(a, node0, g, [&](int off, int len, long long src) {
+                bulkCopy(dst + (unsigned)off * E, a.in + src, (unsigned)len * E, bar);
+            });
+        else
+        {
+            // away from the outer faces every segment is one shifted copy
+            const int t = g & 1;
+            const long long sy = a.px, sz = (long long)a.px * a.ny;
+            const long long src = g < 2 ? (6 + t) * P + node0 - sy : g < 4 ? (4 + t) * P + node0 + sy
+                                : g < 6 ? (10 + t) * P + node0 - sz : (8 + t) * P + node0 + sz;
+            bulkCopy(dst, a.in + src, seg, bar);
+        }
     }
-    bulkCopy(st + L::kOffMat, a.mat + node0, kStageNodes, bar);
+    else if (lane < 15)
+    {
+        if (diel) bulkCopy(st + L::kOffStub + (lane - 12) * stubSeg, a.stub + (lane - 12) * P + node0, stubSeg, bar);
+    }
+    else if (lane == 15)
+        bulkCopy(st + L::kOffMat, a.mat + node0, kStageNodes, bar);
 }
 
 template <class S, int V, int STAGES = kStages, int MINB = 2>
@@ -1014,24 +1092,27 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
     __syncthreads();
     if (threadIdx.x >= kBlock)
     {
-        // producer warp: one lane issues every copy
-        if (threadIdx.x != kBlock) return;
+        // producer warp: every lane issues its share of each tile's copies
+        const int lane = threadIdx.x - kBlock;
         int issued = 0;
         for (int i = 0; i < mine; ++i)
         {
             const int s = i % STAGES;
-            if (i >= STAGES && !mbarWaitBounded(empty0 + 8 * s, (unsigned)(i / STAGES - 1) & 1u))
+            bool ok = true;
+            if (i >= STAGES && lane == 0) ok = mbarWaitBounded(empty0 + 8 * s, (unsigned)(i / STAGES - 1) & 1u);
+            if (!__shfl_sync(0xffffffffu, ok, 0))
             {
-                if (a.fault) atomicOr(a.fault, kStageTimeout);
+                if (lane == 0 && a.fault) atomicOr(a.fault, kStageTimeout);
                 break;
             }
-            stageTile(a, tiles[blockIdx.x + i * gridDim.x], st0 + s * kBytes, full0 + 8 * s);
+            stageTile(a, tiles[blockIdx.x + i * gridDim.x], st0 + s * kBytes, full0 + 8 * s, lane);
             issued = i + 1;
         }
         // the copies of the last STAGES tiles may still be landing: stay
         // until they are in, so that the block's shared memory outlives them
-        for (int i = issued > STAGES ? issued - STAGES : 0; i < issued; ++i)
-            mbarWaitBounded(full0 + 8 * (i % STAGES), (unsigned)(i / STAGES) & 1u);
+        if (lane == 0)
+            for (int i = issued > STAGES ? issued - STAGES : 0; i < issued; ++i)
+                mbarWaitBounded(full0 + 8 * (i % STAGES), (unsigned)(i / STAGES) & 1u);
         return;
     }
     for (int i = 0; i < mine; ++i)

@@ -138,17 +138,9 @@ def interior_tiles(w, V=4, block=256):
 
 def staged_tiles(w, block=256):
     """Number of FP32 tiles (2 nodes per thread) that the staged kernel takes:
-    interior tiles without a node on an outer y or z face."""
-    nx, ny, nz = w.nx, w.ny, w.nz
-    px = (nx + 7) // 8 * 8
-    T = block * 2
-    gen = _general_mask(w, 2, block)
-    edge = np.zeros(gen.size, bool)
-    plane = px * ny
-    for lo, hi in [(0, plane), ((nz - 1) * plane, nz * plane)] + \
-            [(k * plane + r, k * plane + r + px) for k in range(nz) for r in (0, (ny - 1) * px)]:
-        edge[lo // T:(hi - 1) // T + 1] = True
-    return int((~gen & ~edge).sum())
+    the interior tiles (no PEC in reach, no source or monitor, not the partial
+    last tile), outer faces included."""
+    return int((~_general_mask(w, 2, block)).sum())
 
 
 def _general_mask(w, V, block):
