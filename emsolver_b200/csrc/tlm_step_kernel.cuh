@@ -124,6 +124,20 @@ __device__ __forceinline__ void storeVec(S *__restrict__ base, long long node,
             for (int c = 0; c < V; ++c)
                 p.v[c] = encodeStochastic<S>(src[c], inv, mix32((unsigned)((node + c) * 12 + salt) ^ seed));
         }
+        else if constexpr ((std::is_same<S, __half>::value || std::is_same<S, __nv_bfloat16>::value) && V % 2 == 0)
+        {
+            // two nodes per conversion instruction (cvt.rn.{f16,bf16}x2.f32),
+            // rounding each exactly as encode<S> does
+#pragma unroll
+            for (int c = 0; c < V; c += 2)
+            {
+                if constexpr (std::is_same<S, __half>::value)
+                    *reinterpret_cast<__half2 *>(&p.v[c]) = __floats2half2_rn(src[c] * inv, src[c + 1] * inv);
+                else
+                    *reinterpret_cast<__nv_bfloat162 *>(&p.v[c]) =
+                        __floats2bfloat162_rn(src[c] * inv, src[c + 1] * inv);
+            }
+        }
         else
         {
 #pragma unroll
