@@ -103,37 +103,7 @@ def interior_tiles(w, V=4, block=256):
     """Number of interior tiles the step kernel finds in `w` with V nodes per
     thread (mirrors the host rule: no PEC node or PEC neighbour, no source or
     monitor node, not the partial last tile)."""
-    nx, ny, nz = w.nx, w.ny, w.nz
-    px = (nx + 7) // 8 * 8
-    P = px * ny * nz
-    T = block * V
-    nb = (P // V + block - 1) // block
-    gen = np.zeros(nb, bool)
-    if (P // V) % block:
-        gen[-1] = True
-    mat = np.asarray(w.mat).reshape(nz, ny, nx)
-
-    def node(i, j, k):
-        return (k * ny + j) * px + i
-
-    for k, j, i in zip(*np.nonzero(mat == 1)):
-        for n in (node(i, j, k), node(i - 1, j, k) if i > 0 else -1, node(i + 1, j, k) if i < nx - 1 else -1,
-                  node(i, j, k) - px, node(i, j, k) + px, node(i, j, k) - px * ny, node(i, j, k) + px * ny):
-            if 0 <= n < P:
-                gen[n // T] = True
-    spec = []
-    for cells, _, _ in w.ports:
-        for c in cells:
-            spec.append(c)
-            i, j, k = c % nx, (c // nx) % ny, c // (nx * ny)
-            spec += [(k * ny + j2) * nx + i2 for i2, j2 in ((i, j - 1), (i, j + 1), (i - 1, j), (i + 1, j))
-                     if 0 <= i2 < nx and 0 <= j2 < ny]
-    for (i, j, k) in w.probes_cell:
-        spec.append((k * ny + j) * nx + i)
-    for c in spec:
-        i, r = c % nx, c // nx
-        gen[(r * px + i) // T] = True
-    return int((~gen).sum())
+    return int((~_general_mask(w, V, block)).sum())
 
 
 def staged_tiles(w, block=256):
@@ -144,6 +114,7 @@ def staged_tiles(w, block=256):
 
 
 def _general_mask(w, V, block):
+    """Per tile of `block` threads x V nodes: True when the tile is general."""
     nx, ny, nz = w.nx, w.ny, w.nz
     px = (nx + 7) // 8 * 8
     P = px * ny * nz
