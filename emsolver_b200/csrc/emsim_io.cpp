@@ -283,8 +283,8 @@ void writeProject(Out &w, const Project &d)
 
 // ---- reading (LoadProject, ProjectIO.cpp:194-248) ------------------------
 // A short read stores the bytes that remain (as fread does) and fails; every
-// later read fails too, so a count cut off by the end of the file is judged
-// by its partial value exactly as the reference judges it. The limits and
+// later read fails too, so a count cut off by the end of the file is tested
+// by its partial value exactly as the reference tests it. The limits and
 // messages are the reference's. An element count larger than the bytes left
 // fails before anything is allocated.
 struct In

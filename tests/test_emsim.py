@@ -120,7 +120,7 @@ def test_defaults_match_the_reference(tmp_path):
     assert r["plane_axis"] == -1 and r["pat_scale"] == 1.0 and r["domain_lo"][0] == np.float32(1e30)
 
 
-def test_every_truncation_is_judged_like_the_reference(tmp_path):
+def test_every_truncation_is_handled_like_the_reference(tmp_path):
     src = tmp_path / "full.emsim"
     full_project().save(src)
     data = src.read_bytes()
