@@ -135,3 +135,26 @@ def test_batch_state_rules(built):
         assert s.currentStep() == 10
     s.step(5)          # detached by the batch's destruction: steps alone again
     assert s.currentStep() == 15
+
+
+def test_pipelined_solve_equals_alone(built):
+    """Batch.solve (set-up of the next chunk overlapping the device's window,
+    members collected and freed as they finish): every port DFT and record
+    bitwise what the instance gives alone."""
+    ws = workloads.batched_instances(count=10, steps=150, lo=20, hi=40)
+    for k, w in enumerate(ws):
+        w.steps = 100 + 13 * k           # members finish in different windows
+    alone = []
+    for w in ws:
+        s = build_solver(w)
+        s.step(w.steps)
+        alone.append((s.portDft(0), records(s, w, f64=True)))
+        s.close()
+    with Batch() as b:
+        got = b.solve(ws, build_solver, lambda s, w: (s.portDft(0), records(s, w, f64=True)), chunk=3)
+    assert len(got) == len(ws)
+    for (da, ra), (dg, rg) in zip(alone, got):
+        for x, y in zip(da, dg):
+            assert np.array_equal(x, y)
+        for key in ra:
+            assert np.array_equal(ra[key], rg[key]), key
