@@ -232,8 +232,8 @@ SIGNATURES = {
     "fdtd_compute_far_field": (_st, [_h, C.c_int, C.c_int, _P(C.c_float), _P(C.c_float), _P(C.c_float),
                                      _P(C.c_float), _P(C.c_float)]),
     "tlm_step_planes_noalloc": (_st, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                      C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
-                                      C.c_void_p, C.c_void_p]),
+                                      C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                      C.c_int, C.c_void_p, C.c_void_p]),
     "tlm_kernel_variants": (C.c_int, [C.c_int]),
     "tlm_kernel_variant_info": (_st, [C.c_int, C.c_int, _P(C.c_int), _P(C.c_int)]),
     "tlm_batch_create": (_st, [_P(_h), C.c_int]),

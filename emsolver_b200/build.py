@@ -59,21 +59,24 @@ def _stale(target, deps):
 
 
 def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> dict:
-    """Compile every library; returns {name: path}. Rebuilds only what changed."""
+    """Compile every library; returns {name: path}. Rebuilds only what changed;
+    the compilations run in parallel, one per host core."""
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + \
         [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    jobs = []                          # (object, command)
     host_objs = []
     for src in HOST_SOURCES:
         obj = os.path.join(BUILD, src.replace(".cpp", ".o"))
         if force or _stale(obj, deps):
-            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-I" + CSRC, "-I" + INCLUDE,
-                  "-c", os.path.join(CSRC, src), "-o", obj], verbose)
+            jobs.append((obj, ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-I" + CSRC,
+                               "-I" + INCLUDE, "-c", os.path.join(CSRC, src), "-o", obj]))
         host_objs.append(obj)
-    out = {}
+    lib_objs = {}
     for lib, defs in LIBS.items():
-        target = os.path.join(HERE, lib)
         tag = lib.replace(".so", "")
         objs = []
         for src in CUDA_SOURCES:
@@ -82,10 +85,17 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
                 flags = list(NVCC_FLAGS) + defs
                 if ptxas_info:
                     flags += ["-Xptxas", "-v"]
-                log = _run([nvcc] + ARCH + flags + ["-c", os.path.join(CSRC, src), "-o", obj], verbose)
-                if ptxas_info:
-                    print(log)
+                jobs.append((obj, [nvcc] + ARCH + flags + ["-c", os.path.join(CSRC, src), "-o", obj]))
             objs.append(obj)
+        lib_objs[lib] = objs
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        logs = list(ex.map(lambda j: _run(j[1], verbose), jobs))
+    if ptxas_info:
+        for log in logs:
+            print(log)
+    out = {}
+    for lib, objs in lib_objs.items():
+        target = os.path.join(HERE, lib)
         if force or _stale(target, objs + host_objs):
             _run([nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", target] + objs + host_objs,
                  verbose)

@@ -486,25 +486,33 @@ TLM_API tlm_status tlm_halo_unpack(tlm_handle h, const void *recv_lo, const void
  * (or, with input_is_incident != 0, incident pulses such as the reference's
  * V re-laid out); out_planes (12*P floats, not aliasing in_planes) receives
  * the reflected pulses of this step: pass it as in_planes of the next call.
- * stubs: 3 planes read and written on dielectric nodes (NULL if mat has no
- * id >= 2). yhat/ghat: per dielectric id (id - 2). No sources or monitors.
+ * stubs: 3 planes read and written on dielectric nodes. yhat/ghat: n_diel
+ * entries, one per dielectric id (id - 2); with n_diel > 0 stubs, yhat and
+ * ghat must all be given (else TLM_EINVAL), with n_diel = 0 they may be NULL.
+ * The tables are copied into a static table of all 254 dielectric ids whose
+ * entries past n_diel are NaN: a node whose id is 2 + n_diel or more steps to
+ * NaN pulses, and nothing past the caller's buffers is read. No sources or
+ * monitors.
  * energy_out (NULL to skip): the FP64 sum of the squares of all incident
  * link pulses of this step. Planes 16-byte aligned, mat 4-byte aligned.
  * Work is queued on `stream` (a cudaStream_t, NULL = default stream).
  *
  * Limits and sharing: its only scratch, one FP64 energy partial per thread
- * block, is a fixed 512 KiB static device array that every GPU loading this
- * library holds until the process exits; grids above 67,108,864 padded
- * nodes are rejected with TLM_EINVAL. The first call on a device looks up
- * that array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture. Every call shares the array, so calls that
- * overlap on the GPU (other streams, other threads) race: serialise them.
- * Each call overwrites the partials it uses; nothing needs clearing.
+ * block and the padded dielectric table, is a fixed 514 KiB of static device
+ * arrays that every GPU loading this library holds until the process exits;
+ * grids above 67,108,864 padded nodes are rejected with TLM_EINVAL. The
+ * first call on a device looks up those arrays' device addresses
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call shares the arrays, so calls that overlap on the GPU (other
+ * streams, other threads) race: serialise them. Each call rewrites the table
+ * and the partials it uses; nothing needs clearing. The bounds-checked build
+ * of the library (libtlm_b200_checked.so) waits for the step and returns
+ * TLM_ECUDA if any index fell outside its buffer.
  * Errors: status code, message in tlm_last_error(NULL). */
 TLM_API tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_planes,
                                            float *stubs, const uint8_t *mat, const float *yhat,
-                                           const float *ghat, int nx, int ny, int nz, float rho,
-                                           int input_is_incident, double *energy_out,
+                                           const float *ghat, int n_diel, int nx, int ny, int nz,
+                                           float rho, int input_is_incident, double *energy_out,
                                            void *stream);
 
 /* ---- bench / integration helpers ------------------------------------ */

@@ -18,9 +18,18 @@ _i32p = C.POINTER(C.c_int)
 _u64p = C.POINTER(C.c_uint64)
 
 
+# The reference's source tree: $TLM_REFERENCE_SRC, else where this build
+# environment mounts it. Absent (as on a machine that only runs tests), the
+# prebuilt oracle/_ref/ is kept.
+REF_SRC = os.environ.get("TLM_REFERENCE_SRC", "/root/reference")
+
+
 def build_oracle(quiet: bool = True) -> None:
     """Compile liboracle.so (and the reference under _ref/ when its sources exist)."""
-    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    cmd = ["make", "-C", HERE]
+    if os.path.exists(os.path.join(REF_SRC, "TlmSolver.cpp")):
+        cmd.append(f"REF={REF_SRC}")
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:

@@ -7,7 +7,9 @@ and the library advances them with scratch kept in a fixed static device
 array. This test drives it through the C ABI on buffers the test allocates
 (as such a caller would) and checks two calls in a row against the regular
 handle-based entry point on the same state: pulse state and stubs bitwise,
-energy within the energy tolerance the other GPU tests use (relative 1e-6).
+energy within the energy tolerance the other GPU tests use (relative 1e-6),
+in the regular and in the bounds-checked build of the library, and checks
+that further calls leave the device's free memory unchanged.
 """
 import ctypes as C
 
@@ -81,7 +83,8 @@ def connect(refl, mat_p, nx, ny, nz, rho):
     return inc.transpose(1, 2, 3, 0).reshape(-1)
 
 
-def test_no_alloc_step_matches_handle_step(built):
+@pytest.mark.parametrize("variant", ["", "checked"])
+def test_no_alloc_step_matches_handle_step(built, variant):
     torch = pytest.importorskip("torch")
     nx, ny, nz, mat, table, rho, v0 = grid_case()
     g = VoxelGridSpec(nx, ny, nz)
@@ -112,13 +115,14 @@ def test_no_alloc_step_matches_handle_step(built):
     dy = torch.from_numpy(yhat).to(dev)
     dg = torch.from_numpy(ghat).to(dev)
     energy = torch.zeros(2, dtype=torch.float64, device=dev)
-    L = _lib.load()
+    L = _lib.load(variant)
     stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
     def call(src, dst, incident, eslot):
         st = L.tlm_step_planes_noalloc(src.data_ptr(), dst.data_ptr(), stub.data_ptr(),
-                                       dmat.data_ptr(), dy.data_ptr(), dg.data_ptr(), nx, ny, nz,
-                                       float(rho), incident, energy.data_ptr() + 8 * eslot, stream)
+                                       dmat.data_ptr(), dy.data_ptr(), dg.data_ptr(), len(table),
+                                       nx, ny, nz, float(rho), incident,
+                                       energy.data_ptr() + 8 * eslot, stream)
         assert st == _lib.TLM_OK, L.tlm_last_error(None)
 
     call(a, b, 1, 0)        # step 0: incident state in, reflected out
@@ -127,6 +131,16 @@ def test_no_alloc_step_matches_handle_step(built):
     refl0 = b.cpu().numpy().reshape(12, nz, ny, px)
     refl1 = a.cpu().numpy().reshape(12, nz, ny, px)
     e = energy.cpu().numpy()
+
+    # further calls (both kernels already loaded by the two above) leave the
+    # device's free memory where it was: the entry point allocates nothing
+    scratch_a, scratch_b = a.clone(), b.clone()
+    torch.cuda.synchronize(dev)
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    for r in range(4):
+        call(scratch_a if r % 2 == 0 else scratch_b, scratch_b if r % 2 == 0 else scratch_a, r & 1, 0)
+    torch.cuda.synchronize(dev)
+    assert torch.cuda.mem_get_info(dev)[0] == free0
 
     assert np.array_equal(connect(refl0, mat_p, nx, ny, nz, rho), inc1)
     assert np.array_equal(connect(refl1, mat_p, nx, ny, nz, rho), inc2)
@@ -145,7 +159,62 @@ def test_no_alloc_rejects_oversized_grid(built):
     out = torch.zeros(64, dtype=torch.float32, device=dev)
     m = torch.zeros(64, dtype=torch.uint8, device=dev)
     L = _lib.load()
-    st = L.tlm_step_planes_noalloc(buf.data_ptr(), out.data_ptr(), None, m.data_ptr(), None, None,
+    st = L.tlm_step_planes_noalloc(buf.data_ptr(), out.data_ptr(), None, m.data_ptr(), None, None, 0,
                                    1024, 1024, 128, 0.0, 0, None, None)
     assert st == _lib.TLM_EINVAL
     assert b"at most 67108864" in L.tlm_last_error(None)
+    # extents whose product would overflow 64 bits are refused the same way
+    st = L.tlm_step_planes_noalloc(buf.data_ptr(), out.data_ptr(), None, m.data_ptr(), None, None, 0,
+                                   2**31 - 1, 2**31 - 1, 2**31 - 1, 0.0, 0, None, None)
+    assert st == _lib.TLM_EINVAL
+
+
+def test_no_alloc_rejects_missing_tables(built):
+    """A dielectric table without its stubs or entries is refused before
+    anything runs (the step would otherwise read through a null pointer)."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    buf = torch.zeros(12 * 8 * 8 * 8, dtype=torch.float32, device=dev)
+    out = torch.zeros_like(buf)
+    stub = torch.zeros(3 * 8 * 8 * 8, dtype=torch.float32, device=dev)
+    tab = torch.ones(4, dtype=torch.float32, device=dev)
+    m = torch.zeros(8 * 8 * 8, dtype=torch.uint8, device=dev)
+    L = _lib.load()
+    def ptr(t):
+        return None if t is None else t.data_ptr()
+
+    for stubs, yh, gh in ((stub, None, tab), (stub, tab, None), (None, tab, tab)):
+        st = L.tlm_step_planes_noalloc(buf.data_ptr(), out.data_ptr(), ptr(stubs), m.data_ptr(),
+                                       ptr(yh), ptr(gh), 1, 8, 8, 8, 0.0, 0, None, None)
+        assert st == _lib.TLM_EINVAL
+    st = L.tlm_step_planes_noalloc(buf.data_ptr(), out.data_ptr(), None, m.data_ptr(), None, None, -1,
+                                   8, 8, 8, 0.0, 0, None, None)
+    assert st == _lib.TLM_EINVAL
+
+
+def test_no_alloc_ids_past_the_table_step_to_nan(built):
+    """Material ids past the caller's table make those nodes' pulses NaN
+    (the padded static table), while every other node steps as usual."""
+    torch = pytest.importorskip("torch")
+    nx, ny, nz = 8, 8, 8
+    P = nx * ny * nz
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(3)
+    mat = np.zeros((nz, ny, nx), np.uint8)
+    mat[4, 4, 4] = 3                       # id 3: past a one-entry table
+    mat[1, 1, 1] = 2
+    v0 = rng.standard_normal(12 * P).astype(np.float32)
+    a = torch.from_numpy(v0).to(dev)
+    b = torch.zeros_like(a)
+    stub = torch.zeros(3 * P, dtype=torch.float32, device=dev)
+    tab = torch.tensor([4.0], dtype=torch.float32, device=dev)
+    dmat = torch.from_numpy(mat.reshape(-1)).to(dev)
+    L = _lib.load()
+    st = L.tlm_step_planes_noalloc(a.data_ptr(), b.data_ptr(), stub.data_ptr(), dmat.data_ptr(),
+                                   tab.data_ptr(), tab.data_ptr(), 1, nx, ny, nz, 0.0, 1, None, None)
+    assert st == _lib.TLM_OK, L.tlm_last_error(None)
+    torch.cuda.synchronize(dev)
+    out = b.cpu().numpy().reshape(12, P)
+    bad = (4 * ny + 4) * nx + 4
+    assert np.all(np.isnan(out[:, bad]))
+    assert np.all(np.isfinite(np.delete(out, bad, axis=1)))
