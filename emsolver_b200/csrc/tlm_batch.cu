@@ -239,12 +239,15 @@ tlm_status syncGroupTables(tlm_batch_s *b, Group &g)
             if (stagedGroup(g) && h->nStaged + (int)h->edgeTiles.size() > 0)
             {
                 // every interior tile is staged, those on outer faces included
+                // (packed entries: tile | flags << 24), in tile order
+                constexpr int kTileMask = (1 << tlmk::kEntryTileBits) - 1;
                 std::vector<int> mine(h->stagedTiles);
                 mine.insert(mine.end(), h->edgeTiles.begin(), h->edgeTiles.end());
-                std::sort(mine.begin(), mine.end());
-                for (int t : mine) staged.push_back(make_int2(m, t));
+                std::sort(mine.begin(), mine.end(),
+                          [](int x, int y) { return (x & kTileMask) < (y & kTileMask); });
+                for (int e : mine) staged.push_back(make_int2(m, e));
                 std::vector<char> isStaged((size_t)h->nblocks, 0);
-                for (int t : mine) isStaged[(size_t)t] = 1;
+                for (int e : mine) isStaged[(size_t)(e & kTileMask)] = 1;
                 for (int t = 0; t < h->nblocks; ++t)
                     if (!isStaged[(size_t)t]) tiles.push_back(make_int2(m, t));
             }
@@ -291,8 +294,7 @@ template <class S, int V, int MINB, bool SEL>
 tlm_status launchGroupStep(tlm_batch_s *b, Group &g, int i, bool doLaunch)
 {
     constexpr bool kStagedShape = std::is_same<S, float>::value && V == 2 && SEL;
-    constexpr int kSlot = tlmk::Stage<float>::kBytes + (int)((sizeof(tlmk::StepArgs<float>) + 15) / 16 * 16);
-    constexpr int kSmem = tlmk::kStages * kSlot;
+    constexpr int kSmem = tlmk::kStages * tlmk::Stage<float>::kBytes;
     const bool staged = kStagedShape && g.dStaged != nullptr;
     if (g.gridBlocks == 0)
     {
@@ -321,7 +323,7 @@ tlm_status launchGroupStep(tlm_batch_s *b, Group &g, int i, bool doLaunch)
     {
         if (staged)
             tlmk::batchStepKernelStaged<><<<2 * b->smCount, tlmk::kStagedThreads, kSmem, b->stream>>>(
-                static_cast<MemberDesc<float> *>(g.dMembers), g.dStaged, g.dNStaged, i, b->dFault);
+                static_cast<const MemberDesc<float> *>(g.dMembers), g.dStaged, g.dNStaged, i, b->dFault, -0.0f);
     }
     return b->cuda(cudaGetLastError(), "batchStepKernel launch");
 }

@@ -14,23 +14,37 @@
 // single-grid kernel, so a member's results are bitwise those it gets alone.
 #pragma once
 
+#include <cstddef>
+
 #include "tlm_aux_kernels.cuh"
 #include "tlm_step_kernel.cuh"
 
 namespace tlmk {
 
-template <class S> struct MemberDesc
+// One member grid of a batch group. The first 128 bytes (the head, up to
+// nblocks) hold everything the staged batch kernel reads, so that its
+// producer warp loads a member with one coalesced 128-byte load (one 32-bit
+// word per lane); records start on 128-byte boundaries.
+template <class S> struct alignas(128) MemberDesc
 {
     using R = typename Traits<S>::R;
+    // ---- head ----
     S *buf[2];               // ping-pong planes: step n reads buf[n & 1]
     R *stub;
     const uint8_t *mat;
     const R *yhat;
     const R *ghat;
-    long long P, nquads;
+    double *epart;           // [window/16 + 1][nblocks]
+    long long P;
+    long long base;          // absolute step at the start of the current window
+    long long total;         // the member stops before this step
     int nx, ny, nz, px, nq;
     FastDiv div_nq, div_ny;
-    R rho, scale, inv_scale;
+    R rho;
+    int nblocks;
+    // ---- the rest ----
+    long long nquads;
+    R scale, inv_scale;
     const int *tile_begin;
     const SpecEntry *spec;
     const uint8_t *tile_flags;
@@ -38,12 +52,23 @@ template <class S> struct MemberDesc
     const R *sv;             // source value per absolute step, [total]
     R *samples;              // [window][nsamp][6]
     int nsamp;
-    double *epart;           // [window/16 + 1][nblocks]
-    int nblocks;
     int stochastic;
-    long long base;          // absolute step at the start of the current window
-    long long total;         // the member stops before this step
     EpilogueArgs<R> epi;     // monitor outputs (window fields filled per window)
+};
+
+// 32-bit word indices of the head fields of an FP32 member.
+struct HeadWords
+{
+    using D = MemberDesc<float>;
+    static constexpr int kBuf = offsetof(D, buf) / 4, kStub = offsetof(D, stub) / 4, kMat = offsetof(D, mat) / 4,
+                         kYhat = offsetof(D, yhat) / 4, kGhat = offsetof(D, ghat) / 4,
+                         kEpart = offsetof(D, epart) / 4, kP = offsetof(D, P) / 4, kBase = offsetof(D, base) / 4,
+                         kTotal = offsetof(D, total) / 4, kNx = offsetof(D, nx) / 4, kNy = offsetof(D, ny) / 4,
+                         kNz = offsetof(D, nz) / 4, kPx = offsetof(D, px) / 4, kNq = offsetof(D, nq) / 4,
+                         kDivNq = offsetof(D, div_nq) / 4, kDivNy = offsetof(D, div_ny) / 4,
+                         kRho = offsetof(D, rho) / 4, kNblocks = offsetof(D, nblocks) / 4;
+    static_assert(offsetof(D, nblocks) + 4 <= 128, "the head of an FP32 member fits 128 bytes");
+    static_assert(sizeof(D) % 128 == 0, "member records start on 128-byte boundaries");
 };
 
 template <class S, int V, int MINB, bool SEL>
@@ -107,6 +132,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
                     sa.fault = fault;
                     sa.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
                     sa.stochastic = d.stochastic;
+                    sa.stage_wait_ns = kStageWaitNs;
                 }
             }
             __syncthreads();
@@ -122,23 +148,46 @@ __global__ void __launch_bounds__(kBlock, MINB)
 }
 
 // Staged tiles of an FP32 batch group (2 nodes per thread): the single-grid
-// staged kernel's pipeline over the (member, tile) pairs of every member's
-// staged tiles. The producer lane builds the tile's member arguments for
-// this step into the stage next to the pulses (so the consumers read them
-// from shared memory), or marks the stage empty when the member is past its
-// last step. Energy steps differ between members, so each consumer counts
-// its own uses of every stage's energy barrier (the same sequence in every
-// thread).
+// staged kernel's pipeline over the (member, packed tile entry) pairs of
+// every member's staged tiles. The producer warp holds the entries of the
+// next 32 to 64 tiles and loads the head of the next tile's member (one word
+// per lane) while the current tile's copies are issued; per tile it writes
+// the member's head, the step's output planes and energy partials and the
+// tile's entry into the stage's header, or marks the stage empty when the
+// member is past its last step. Energy steps differ between members, so each
+// consumer counts its own uses of every stage's energy barrier (the same
+// sequence in every thread).
+struct BatchStageHdr
+{
+    unsigned head[32];  // the member's head words (HeadWords)
+    float *out;         // output planes of this tile's step
+    double *epart;      // energy partials of this step (nullptr: not an energy step)
+    int tile;           // -1: an empty stage
+    unsigned flags;
+};
+
+__device__ __forceinline__ unsigned long long headU64(const unsigned *w, int i)
+{
+    return (unsigned long long)w[i] | ((unsigned long long)w[i + 1] << 32);
+}
+__device__ __forceinline__ unsigned long long shflU64(unsigned w, int i)
+{
+    const unsigned lo = __shfl_sync(0xffffffffu, w, i), hi = __shfl_sync(0xffffffffu, w, i + 1);
+    return (unsigned long long)lo | ((unsigned long long)hi << 32);
+}
+
 template <int STAGES = kStages, int MINB = 2>
 __global__ void __launch_bounds__(kStagedThreads, MINB)
-    batchStepKernelStaged(MemberDesc<float> *__restrict__ members, const int2 *__restrict__ tiles,
-                          const int *__restrict__ ntiles, int i, unsigned *fault)
+    batchStepKernelStaged(const MemberDesc<float> *__restrict__ members, const int2 *__restrict__ tiles,
+                          const int *__restrict__ ntiles, int i, unsigned *fault, float negZero)
 {
+    using H = HeadWords;
     constexpr int kData = Stage<float>::kBytes;
-    constexpr int kSlot = kData + (int)((sizeof(StepArgs<float>) + 15) / 16 * 16);
+    constexpr int kDescWords = (int)(sizeof(MemberDesc<float>) / 4);
     extern __shared__ __align__(128) unsigned char stage[];
     __shared__ double red[STAGES][kBlock / 32];
     __shared__ __align__(8) unsigned long long full[STAGES], empty[STAGES], ered[STAGES];
+    __shared__ __align__(16) BatchStageHdr hdr[STAGES];
     const int nt = *ntiles;
     const int mine = nt > (int)blockIdx.x ? (nt - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
     const unsigned st0 = smemAddr(stage), full0 = smemAddr(full), empty0 = smemAddr(empty), ered0 = smemAddr(ered);
@@ -155,13 +204,25 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
     __syncthreads();
     if (threadIdx.x >= kBlock)
     {
-        // producer warp: lane 0 writes the member arguments, then every lane
-        // issues its share of the copies
         const int lane = threadIdx.x - kBlock;
+        const unsigned *words = reinterpret_cast<const unsigned *>(members);
+        EntryWindow<int2> win;
+        win.init(tiles, mine, lane, make_int2(0, 0));
+        // member of the block's tile `it` (it - win.it0 in [0, 64))
+        auto memberAt = [&](int it) {
+            const int d = it - win.it0;
+            const int ma = __shfl_sync(0xffffffffu, win.a.x, d & 31), mb = __shfl_sync(0xffffffffu, win.b.x, d & 31);
+            return d < 32 ? ma : mb;
+        };
+        unsigned wNext = mine > 0 ? words[(size_t)memberAt(0) * kDescWords + lane] : 0u;
         int issued = 0;
         for (int it = 0; it < mine; ++it)
         {
             const int s = it % STAGES;
+            if (it == win.it0 + 32) win.slide(lane);
+            const int e = __shfl_sync(0xffffffffu, win.a.y, it - win.it0);
+            const unsigned w = wNext;
+            if (it + 1 < mine) wNext = words[(size_t)memberAt(it + 1) * kDescWords + lane];
             bool ok = true;
             if (it >= STAGES && lane == 0) ok = mbarWaitBounded(empty0 + 8 * s, (unsigned)(it / STAGES - 1) & 1u);
             if (!__shfl_sync(0xffffffffu, ok, 0))
@@ -169,59 +230,44 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
                 if (lane == 0 && fault) atomicOr(fault, kStageTimeout);
                 break;
             }
-            const int2 tl = tiles[blockIdx.x + it * gridDim.x];
-            const MemberDesc<float> &d = members[tl.x];
-            StepArgs<float> *sa = reinterpret_cast<StepArgs<float> *>(stage + s * kSlot + kData);
-            const long long n = d.base + i;
-            const unsigned bar = full0 + 8 * s;
-            if (n >= d.total)
+            const long long n = (long long)shflU64(w, H::kBase) + i;
+            const bool live = n < (long long)shflU64(w, H::kTotal);
+            float *const buf0 = reinterpret_cast<float *>(shflU64(w, H::kBuf));
+            float *const buf1 = reinterpret_cast<float *>(shflU64(w, H::kBuf + 2));
+            double *const ep = reinterpret_cast<double *>(shflU64(w, H::kEpart));
+            const int nblocks = (int)__shfl_sync(0xffffffffu, w, H::kNblocks);
+            BatchStageHdr &hd = hdr[s];
+            hd.head[lane] = w;
+            if (lane == 0)
             {
-                if (lane == 0)
-                {
-                    sa->nquads = -1;  // the member has finished: an empty stage
-                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(bar) : "memory");
-                }
+                const long long base = n - i;
+                const long long eFirst = (base + 15) / 16 * 16;
+                hd.out = (n & 1) ? buf0 : buf1;
+                hd.epart = (n % 16 == 0) ? ep + ((n - eFirst) / 16) * nblocks : nullptr;
+                hd.tile = live ? entryTile(e) : -1;
+                hd.flags = entryFlags(e);
+            }
+            __syncwarp();
+            const unsigned bar = full0 + 8 * s;
+            if (!live)
+            {
+                if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(bar) : "memory");
             }
             else
             {
-                if (lane == 0)
-                {
-                    StepArgs<float> a;
-                    const long long eFirst = (d.base + 15) / 16 * 16;
-                    a.in = d.buf[n & 1];
-                    a.out = d.buf[(n + 1) & 1];
-                    a.stub = d.stub;
-                    a.mat = d.mat;
-                    a.yhat = d.yhat;
-                    a.ghat = d.ghat;
-                    a.P = d.P;
-                    a.nquads = d.nquads;
-                    a.nx = d.nx;
-                    a.ny = d.ny;
-                    a.nz = d.nz;
-                    a.px = d.px;
-                    a.nq = d.nq;
-                    a.div_nq = d.div_nq;
-                    a.div_ny = d.div_ny;
-                    a.rho = d.rho;
-                    a.scale = d.scale;
-                    a.inv_scale = d.inv_scale;
-                    a.tile_begin = d.tile_begin;
-                    a.spec = d.spec;
-                    a.tile_flags = d.tile_flags;
-                    a.neg_zero = d.neg_zero;
-                    a.sv = d.sv[n];
-                    a.samples = d.samples + (long long)i * d.nsamp * 6;
-                    a.epart = (n % 16 == 0) ? d.epart + ((n - eFirst) / 16) * d.nblocks : nullptr;
-                    a.e_lo = 0;
-                    a.e_hi = LLONG_MAX;
-                    a.fault = fault;
-                    a.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
-                    a.stochastic = d.stochastic;
-                    *sa = a;
-                }
-                __syncwarp();
-                stageTile(*sa, tl.y, st0 + s * kSlot, bar, lane);
+                StageSrc<float> src;
+                src.in = (n & 1) ? buf1 : buf0;
+                src.stub = reinterpret_cast<const float *>(shflU64(w, H::kStub));
+                src.mat = reinterpret_cast<const uint8_t *>(shflU64(w, H::kMat));
+                src.P = (long long)shflU64(w, H::kP);
+                src.px = (int)__shfl_sync(0xffffffffu, w, H::kPx);
+                src.ny = (int)__shfl_sync(0xffffffffu, w, H::kNy);
+                src.nz = (int)__shfl_sync(0xffffffffu, w, H::kNz);
+                src.div_nq.mul = __shfl_sync(0xffffffffu, w, H::kDivNq);
+                src.div_nq.shift = (int)__shfl_sync(0xffffffffu, w, H::kDivNq + 1);
+                src.div_ny.mul = __shfl_sync(0xffffffffu, w, H::kDivNy);
+                src.div_ny.shift = (int)__shfl_sync(0xffffffffu, w, H::kDivNy + 1);
+                stageTile(src, entryTile(e), entryFlags(e), st0 + s * kData, bar, lane);
             }
             issued = it + 1;
         }
@@ -239,14 +285,48 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             if (fault) atomicOr(fault, kStageTimeout);
             return;
         }
-        const StepArgs<float> &a = *reinterpret_cast<const StepArgs<float> *>(stage + s * kSlot + kData);
-        if (a.nquads >= 0)
+        const BatchStageHdr &hd = hdr[s];
+        const int tile = hd.tile;
+        if (tile >= 0)
         {
-            const int tile = tiles[blockIdx.x + it * gridDim.x].y;
+            StepArgs<float> a;
+            a.in = nullptr;  // the staged body reads its inputs from the stage
+            a.out = hd.out;
+            a.stub = reinterpret_cast<float *>(headU64(hd.head, H::kStub));
+            a.mat = nullptr;
+            a.yhat = reinterpret_cast<const float *>(headU64(hd.head, H::kYhat));
+            a.ghat = reinterpret_cast<const float *>(headU64(hd.head, H::kGhat));
+            a.P = (long long)headU64(hd.head, H::kP);
+            a.nquads = 0;
+            a.nx = (int)hd.head[H::kNx];
+            a.ny = (int)hd.head[H::kNy];
+            a.nz = (int)hd.head[H::kNz];
+            a.px = (int)hd.head[H::kPx];
+            a.nq = (int)hd.head[H::kNq];
+            a.div_nq.mul = hd.head[H::kDivNq];
+            a.div_nq.shift = (int)hd.head[H::kDivNq + 1];
+            a.div_ny.mul = hd.head[H::kDivNy];
+            a.div_ny.shift = (int)hd.head[H::kDivNy + 1];
+            a.rho = __uint_as_float(hd.head[H::kRho]);
+            a.scale = 1.0f;
+            a.inv_scale = 1.0f;
+            a.tile_begin = nullptr;
+            a.spec = nullptr;
+            a.sv = 0.0f;
+            a.samples = nullptr;
+            a.epart = hd.epart;
+            a.e_lo = 0;
+            a.e_hi = LLONG_MAX;
+            a.fault = fault;
+            a.round_seed = 0;
+            a.stochastic = 0;
+            a.tile_flags = nullptr;
+            a.neg_zero = negZero;
+            a.stage_wait_ns = kStageWaitNs;
             const unsigned ep = (eBits >> s) & 1u;
             if (a.epart != nullptr) eBits ^= 1u << s;
-            stepTileInterior<float, 2, true>(a, tile, red[s], (a.tile_flags[tile] & kTileDiel) != 0,
-                                             stage + s * kSlot, ered0 + 8 * s, ep);
+            stepTileInterior<float, 2, true>(a, tile, red[s], (hd.flags & kTileDiel) != 0, stage + s * kData,
+                                             ered0 + 8 * s, ep);
         }
         __syncwarp();
         if ((threadIdx.x & 31) == 0)

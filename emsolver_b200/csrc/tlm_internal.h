@@ -244,7 +244,9 @@ struct tlm_solver
     uint8_t *dTileFlags = nullptr;  // per step-kernel tile: tlmk::kTileGeneral / kTileDiel / kTileEdge
     int *dStaged = nullptr, *dListed = nullptr;  // tiles of the staged kernel / of the list kernel
     int nStaged = 0, nListed = 0, stagedGrid = 0;
-    std::vector<int> stagedTiles, listedTiles;  // host copies (a batch builds its tile tables from them)
+    // host copies (a batch builds its tile tables from them); staged and edge
+    // tiles as packed entries (tlmk::packStagedEntry: tile | flags << 24)
+    std::vector<int> stagedTiles, listedTiles;
     std::vector<int> edgeTiles;                 // interior tiles on an outer face (listed alone, staged in a batch)
     cudaStream_t side = nullptr;      // the list kernel's stream (forked from and joined to `stream`)
     cudaEvent_t evFork = nullptr, evJoin = nullptr;

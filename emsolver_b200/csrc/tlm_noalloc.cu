@@ -197,6 +197,7 @@ tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_planes, fl
     a.e_lo = 0;
     a.e_hi = LLONG_MAX;
     a.fault = sc.fault;
+    a.stage_wait_ns = tlmk::kStageWaitNs;
     if (input_is_incident)
         tlmk::stepKernelShaped<float, kNoAllocV, 3, true, false><<<(unsigned)nblocks, tlmk::kBlock, 0, s>>>(a);
     else

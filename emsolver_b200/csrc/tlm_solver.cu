@@ -222,17 +222,25 @@ tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
     h->edgeTiles.clear();
     if (h->storage != TLM_STORE_F32 || h->cfg.no_staging || h->V != 2 || !shapeOf(h->storage, h->variant).select)
         return TLM_OK;
+    // staged lists hold packed entries (tile and flags, tlmk::packStagedEntry)
     std::vector<int> staged, listed, edge;
     for (int t = 0; t < h->nblocks; ++t)
     {
         const uint8_t f = flags[(size_t)t];
-        ((f & tlmk::kTileGeneral) ? listed : (f & tlmk::kTileEdge) ? edge : staged).push_back(t);
+        if (f & tlmk::kTileGeneral)
+            listed.push_back(t);
+        else if (f & tlmk::kTileEdge)
+        {
+            listed.push_back(t);
+            edge.push_back(tlmk::packStagedEntry(t, f));
+        }
+        else
+            staged.push_back(tlmk::packStagedEntry(t, f));
     }
     // interior tiles on an outer face cost the producer more (their segments
     // come in runs); alone on the device they run in the list kernel, which
     // overlaps the staged one, while a batch stages them too (edgeTiles)
     h->edgeTiles = edge;
-    listed.insert(listed.end(), edge.begin(), edge.end());
     std::sort(listed.begin(), listed.end());
     if (staged.empty()) return TLM_OK;
     int sms = 0;
@@ -463,6 +471,9 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
     a.e_lo = h->ghostLo ? planeNodes : 0;
     a.e_hi = h->ghostHi ? (long long)(h->nz - 1) * planeNodes : LLONG_MAX;
     a.fault = h->dFault;
+    a.stage_wait_ns = h->cfg.stage_wait_us > 0   ? (unsigned long long)h->cfg.stage_wait_us * 1000ull
+                      : h->cfg.stage_wait_us < 0 ? 0ull
+                                                 : tlmk::kStageWaitNs;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (h->timing)
     {
@@ -873,6 +884,7 @@ void tlm_config_default(tlm_config *c)
     c->rounding = 0;
     c->general_tiles = 0;
     c->no_staging = 0;
+    c->stage_wait_us = 0;
     c->surface_monitors = 0;
 }
 

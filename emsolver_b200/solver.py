@@ -93,6 +93,7 @@ class TlmConfig:
     generalTiles: bool = False  # True: no interior-tile fast path (cross-checks)
     surfaceMonitors: bool = False  # PEC-surface Js and Huygens-box DFT monitors
     noStaging: bool = False    # True: no shared-memory staging of FP32 interior tiles (cross-checks)
+    stageWaitUs: int = 0       # staged tiles' wait limit in us (0 default ~2 s, < 0 first poll)
 
     def to_c(self):
         c = _lib.ConfigC()
@@ -112,6 +113,7 @@ class TlmConfig:
         c.general_tiles = 1 if self.generalTiles else 0
         c.surface_monitors = 1 if self.surfaceMonitors else 0
         c.no_staging = 1 if self.noStaging else 0
+        c.stage_wait_us = int(self.stageWaitUs)
         return c
 
 

@@ -122,6 +122,13 @@ typedef struct tlm_config {
     int no_staging;      /* 1: FP32 interior tiles load their pulses directly
                             instead of through shared-memory stages filled by
                             bulk copies; results are identical */
+    int stage_wait_us;   /* staged tiles: the consumers give up waiting for a
+                            stage's bulk copies (the producer for a stage to
+                            be released) after this many microseconds and the
+                            step fails with TLM_ECUDA; 0 = default (about 2 s),
+                            < 0 = at the first poll that finds the stage not
+                            ready (exercises the error path). The producer
+                            always lets the copies it issued land */
 } tlm_config;
 
 typedef struct tlm_solver *tlm_handle;

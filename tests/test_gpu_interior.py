@@ -103,3 +103,29 @@ def test_interior_body_equals_general_body(built, storage, rounding):
         assert np.array_equal(sa, sb), (storage, v)
         for k in ra:
             assert np.array_equal(ra[k], rb[k]), (storage, v, k)
+
+
+def test_stage_wait_running_out_fails_the_step(built):
+    """A stage wait that runs out (tlm_config.stage_wait_us < 0: give up at
+    the first poll that finds the stage not ready) sets the kernel's fault
+    flag instead of hanging: the step returns TLM_ECUDA with the wait's
+    message, and the device stays usable -- a fresh handle then steps the
+    same grid bitwise like a handle that loads its pulses directly."""
+    w = workloads.heterogeneous(n=96, steps=24)
+    v = pair_variant(Storage.F32)
+    assert staged_tiles(w) > 0
+    s = build_solver(w, kernel_variant=v, stage_wait_us=-1)
+    with pytest.raises(_lib.TlmError) as err:
+        s.step(1)
+    assert err.value.status == _lib.TLM_ECUDA
+    assert "never arrived" in str(err.value)
+    s.close()
+    out = []
+    for no_staging in (False, True):
+        r = build_solver(w, kernel_variant=v, no_staging=no_staging)
+        r.step(w.steps)
+        out.append((r.pulses(), r.stubs(), records(r, w, f64=True)))
+        r.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for k in out[0][2]:
+        assert np.array_equal(out[0][2][k], out[1][2][k]), k
