@@ -43,7 +43,8 @@ class ConfigC(C.Structure):
                 ("use_gpu", C.c_int), ("record_every", C.c_int), ("storage", C.c_int),
                 ("pulse_scale", C.c_float), ("steps_per_launch", C.c_int),
                 ("kernel_variant", C.c_int), ("rounding", C.c_int), ("general_tiles", C.c_int),
-                ("surface_monitors", C.c_int), ("no_staging", C.c_int), ("stage_wait_us", C.c_int)]
+                ("surface_monitors", C.c_int), ("no_staging", C.c_int), ("stage_wait_us", C.c_int),
+                ("near_field", C.c_int)]
 
 
 class EmsimFaceC(C.Structure):

@@ -149,11 +149,13 @@ template <class R> __global__ void __launch_bounds__(512) windowEpilogue(const E
 }
 
 // Connect applied to a reflected state: the incident pulses the next step
-// would see, in the reference's AoS layout (the reference's V).
+// would see, in the reference's AoS layout (the reference's V). Nodes of the
+// near-field box `nb` (none when nb.lo_in is null) see their sources
+// completed by the residuals, as the step does.
 template <class S, class O>
 __global__ void incidentToAos(const S *__restrict__ refl, const uint8_t *__restrict__ mat, long long P,
                               int nx, int ny, int nz, int px, typename Traits<S>::R rho,
-                              typename Traits<S>::R scale, O *__restrict__ out)
+                              typename Traits<S>::R scale, O *__restrict__ out, NearBox nb)
 {
     using R = typename Traits<S>::R;
     const long long n = (long long)nx * ny * nz;
@@ -173,28 +175,43 @@ __global__ void incidentToAos(const S *__restrict__ refl, const uint8_t *__restr
         const int co[3] = { i, j, k };
         const int dims[3] = { nx, ny, nz };
         const long long st[3] = { 1, px, (long long)px * ny };
+        const bool inBox = nb.lo_in != nullptr && nb.at(i, j, k) >= 0;
         for (int s = 0; s < 12; ++s)
         {
             const int ax = s >> 2, side = (s >> 1) & 1;
             const int qn = co[ax] + (side ? 1 : -1);
-            const R own = loadOne<S>(refl, s * P + node, scale);
+            R own = loadOne<S>(refl, s * P + node, scale);
+            if (inBox) own += nb.lo_in[s * nb.bP + nb.at(i, j, k)];
             R v;
             if (qn < 0 || qn >= dims[ax])
                 v = rho * own;
             else
             {
-                const long long nb = node + (side ? st[ax] : -st[ax]);
-                v = (mat[nb] == kPec) ? -own : loadOne<S>(refl, (s ^ 2) * P + nb, scale);
+                const long long nbr = node + (side ? st[ax] : -st[ax]);
+                if (mat[nbr] == kPec)
+                    v = -own;
+                else
+                {
+                    v = loadOne<S>(refl, (s ^ 2) * P + nbr, scale);
+                    if (inBox)
+                    {
+                        int c2[3] = { i, j, k };
+                        c2[ax] = qn;
+                        const long long b = nb.at(c2[0], c2[1], c2[2]);
+                        if (b >= 0) v += nb.lo_in[(s ^ 2) * nb.bP + b];
+                    }
+                }
             }
             dst[s] = (O)v;
         }
     }
 }
 
-// Incident planes (state written by tlm_set_pulses) -> AoS.
+// Incident planes (state written by tlm_set_pulses) -> AoS; near-field box
+// nodes completed by their residuals.
 template <class S, class O>
 __global__ void planesToAos(const S *__restrict__ planes, long long P, int nx, int ny, int nz, int px,
-                            typename Traits<S>::R scale, O *__restrict__ out)
+                            typename Traits<S>::R scale, O *__restrict__ out, NearBox nb)
 {
     const long long n = (long long)nx * ny * nz;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
@@ -204,17 +221,24 @@ __global__ void planesToAos(const S *__restrict__ planes, long long P, int nx, i
         const int j = (int)((c / nx) % ny);
         const int k = (int)(c / ((long long)nx * ny));
         const long long node = ((long long)k * ny + j) * px + i;
-        for (int s = 0; s < 12; ++s) out[c * 12 + s] = (O)loadOne<S>(planes, s * P + node, scale);
+        const long long b = nb.lo_in != nullptr ? nb.at(i, j, k) : -1;
+        for (int s = 0; s < 12; ++s)
+        {
+            typename Traits<S>::R v = loadOne<S>(planes, s * P + node, scale);
+            if (b >= 0) v += nb.lo_in[s * nb.bP + b];
+            out[c * 12 + s] = (O)v;
+        }
     }
 }
 
 // Incident AoS state -> incident planes (PEC and padding nodes get 0), one
 // aligned group of 4 nodes per thread iteration (the unit of every storage
-// type, block floating point included).
+// type, block floating point included). Near-field box nodes (nb.lo_out
+// non-null) also get the residual of their rounded value.
 template <class S, class I>
 __global__ void aosToIncident(const I *__restrict__ in, const uint8_t *__restrict__ mat, long long P,
                               int nx, int ny, int nz, int px, typename Traits<S>::R inv_scale,
-                              S *__restrict__ planes)
+                              S *__restrict__ planes, NearBox nb)
 {
     using R = typename Traits<S>::R;
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < P / 4;
@@ -235,6 +259,16 @@ __global__ void aosToIncident(const I *__restrict__ in, const uint8_t *__restric
                 v[c] = real ? (R)in[cell * 12 + s] : R(0);
             }
             storeVec<S, 4>(planes, s * P + node0, v, inv_scale, false, 0u, s);
+            if constexpr (Traits<S>::kScaled)
+            {
+                if (nb.lo_out != nullptr)
+                    for (int c = 0; c < 4; ++c)
+                    {
+                        const long long b = nb.at(i0 + c, j, k);
+                        if (b >= 0)
+                            nb.lo_out[s * nb.bP + b] = v[c] - decode(encode<S>(v[c], inv_scale), R(1) / inv_scale);
+                    }
+            }
         }
     }
 }

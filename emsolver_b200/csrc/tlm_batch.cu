@@ -158,6 +158,9 @@ template <class S> MemberDesc<S> makeDesc(tlm_solver *h)
     d.stochastic = h->cfg.rounding == 1 ? 1 : 0;
     d.base = h->curStep;
     d.total = h->cfg.total_steps;
+    d.near = h->nearBox;  // residual planes beside buf[0] (lo_in) and buf[1] (lo_out)
+    d.near.lo_in = h->nearBox.bP > 0 ? h->dLo[0] : nullptr;
+    d.near.lo_out = h->nearBox.bP > 0 ? h->dLo[1] : nullptr;
     tlmk::EpilogueArgs<R> &a = d.epi;
     a.samples = static_cast<const R *>(h->dSamples);
     a.nsamp = h->nsamp;

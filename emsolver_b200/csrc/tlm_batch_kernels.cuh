@@ -53,6 +53,7 @@ template <class S> struct alignas(128) MemberDesc
     R *samples;              // [window][nsamp][6]
     int nsamp;
     int stochastic;
+    NearBox near;            // near-field box (lo_in/lo_out: the residuals beside buf[0] / buf[1])
     EpilogueArgs<R> epi;     // monitor outputs (window fields filled per window)
 };
 
@@ -133,6 +134,12 @@ __global__ void __launch_bounds__(kBlock, MINB)
                     sa.round_seed = mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
                     sa.stochastic = d.stochastic;
                     sa.stage_wait_ns = kStageWaitNs;
+                    sa.near = d.near;
+                    if (n & 1)
+                    {
+                        sa.near.lo_in = d.near.lo_out;
+                        sa.near.lo_out = const_cast<float *>(d.near.lo_in);
+                    }
                 }
             }
             __syncthreads();

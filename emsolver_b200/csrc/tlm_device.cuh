@@ -469,6 +469,28 @@ __device__ __forceinline__ void scatterStub2(const float2 (&in)[12], float2 (&vs
 
 // A source or monitor attached to one node. Entries are sorted by node
 // (stable: per node, the reference's injection order, then the sample).
+// The near-field box of 16-bit storage (tlm_config.near_field): every node
+// inside it keeps, beside its stored 16-bit pulses, their FP32 residuals, so
+// that decode(stored) + residual is exactly the FP32 pulse. Box nodes read
+// their neighbours' pulses completed by the residuals (zero outside the box)
+// and so step as FP32 storage would; nodes outside read the 16-bit values.
+struct NearBox
+{
+    const float *lo_in;  // 12 residual planes of the input state, bP nodes each (nullptr: no box)
+    float *lo_out;       // the same for the output state
+    int x0, y0, z0;      // box origin (node coordinates)
+    int nx, ny, nz;      // box extent
+    long long bP;        // nx * ny * nz
+    // residual index of node (i, j, k), -1 outside the box
+    __device__ __forceinline__ long long at(int i, int j, int k) const
+    {
+        const unsigned bi = (unsigned)(i - x0), bj = (unsigned)(j - y0), bk = (unsigned)(k - z0);
+        return (bi < (unsigned)nx && bj < (unsigned)ny && bk < (unsigned)nz)
+                   ? ((long long)bk * ny + bj) * nx + bi
+                   : -1;
+    }
+};
+
 struct SpecEntry
 {
     long long node;  // padded node index

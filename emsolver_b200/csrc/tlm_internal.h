@@ -236,6 +236,10 @@ struct tlm_solver
 
     // device memory
     void *dPulses[2] = { nullptr, nullptr };
+    // near-field box of 16-bit storage (tlm_config.near_field): its extent
+    // (nearBox.bP == 0: none) and the residual planes beside each pulse buffer
+    tlmk::NearBox nearBox{};
+    float *dLo[2] = { nullptr, nullptr };
     void *dStub = nullptr;
     uint8_t *dMat = nullptr;
     void *dYhat = nullptr, *dGhat = nullptr;

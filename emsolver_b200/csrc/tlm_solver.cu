@@ -31,12 +31,13 @@ thread_local std::string g_threadError;
 
 const char *kVersion = "tlm_b200 0.1.0 (sm_100a)";
 
+// Smallest power of two >= v (a power of two maps to itself).
 float pow2Ceil(float v)
 {
     if (!(v > 0.0f) || !std::isfinite(v)) return 1.0f;
     int e = 0;
-    std::frexp(v, &e);
-    return std::ldexp(1.0f, e);
+    const float m = std::frexp(v, &e);  // v = m * 2^e, m in [0.5, 1)
+    return m == 0.5f ? v : std::ldexp(1.0f, e);
 }
 
 } // namespace
@@ -77,6 +78,9 @@ void freeMonitors(tlm_solver *h)
     devFree(h, h->dEhist);
     devFree(h, h->dWdt);
     devFree(h, h->dDft);
+    devFree(h, h->dLo[0]);
+    devFree(h, h->dLo[1]);
+    h->nearBox = tlmk::NearBox{};
     h->recCap = 0;
     h->prepared = false;
 }
@@ -119,6 +123,51 @@ long long paddedNode(const tlm_solver *h, uint64_t cell)
 // a tile is general when it is the partial last tile, holds a source or
 // monitor entry (tileBegin ranges), or holds a node that is PEC or next to a
 // PEC node.
+// The near-field box (tlm_config.near_field = r > 0, FP16/BF16 storage):
+// the bounding box of the PEC cells and port cells grown by r cells on every
+// side and clipped to the grid; none (bP = 0) without such cells.
+tlmk::NearBox nearBoxOf(const tlm_solver *h)
+{
+    tlmk::NearBox b{};
+    const int r = h->cfg.near_field;
+    if (r <= 0 || (h->storage != TLM_STORE_F16 && h->storage != TLM_STORE_BF16)) return b;
+    int lo[3] = { h->nx, h->ny, h->nz }, hi[3] = { -1, -1, -1 };
+    auto take = [&](long long i, long long j, long long k) {
+        const long long c[3] = { i, j, k };
+        for (int a = 0; a < 3; ++a)
+        {
+            lo[a] = (int)std::min<long long>(lo[a], c[a]);
+            hi[a] = (int)std::max<long long>(hi[a], c[a]);
+        }
+    };
+    for (int k = 0; k < h->nz; ++k)
+        for (int j = 0; j < h->ny; ++j)
+        {
+            const uint8_t *row = h->mat.data() + ((size_t)k * h->ny + j) * h->nx;
+            for (int i = 0; i < h->nx; ++i)
+                if (row[i] == tlmk::kPec) take(i, j, k);
+        }
+    for (const PortInfo &p : h->ports)
+        for (uint64_t c : p.cells)
+            take((long long)(c % (uint64_t)h->nx), (long long)(c / (uint64_t)h->nx % (uint64_t)h->ny),
+                 (long long)(c / ((uint64_t)h->nx * h->ny)));
+    if (hi[0] < 0) return b;
+    const int n[3] = { h->nx, h->ny, h->nz };
+    for (int a = 0; a < 3; ++a)
+    {
+        lo[a] = std::max(lo[a] - r, 0);
+        hi[a] = std::min(hi[a] + r, n[a] - 1);
+    }
+    b.x0 = lo[0];
+    b.y0 = lo[1];
+    b.z0 = lo[2];
+    b.nx = hi[0] - lo[0] + 1;
+    b.ny = hi[1] - lo[1] + 1;
+    b.nz = hi[2] - lo[2] + 1;
+    b.bP = (long long)b.nx * b.ny * b.nz;
+    return b;
+}
+
 std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tileBegin)
 {
     const long long T = (long long)kBlock * h->V;
@@ -143,6 +192,16 @@ std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tile
     }
     for (int b = 0; b < nb; ++b)
         if (tileBegin[b + 1] > tileBegin[b]) f[(size_t)b] |= tlmk::kTileGeneral;
+    // near-field box: the tiles over each of its rows
+    const tlmk::NearBox &nb3 = h->nearBox;
+    if (nb3.bP > 0)
+        for (int k = nb3.z0; k < nb3.z0 + nb3.nz; ++k)
+            for (int j = nb3.y0; j < nb3.y0 + nb3.ny; ++j)
+            {
+                const long long r0 = ((long long)k * h->ny + j) * h->px;
+                for (long long t = (r0 + nb3.x0) / T; t * T < r0 + nb3.x0 + nb3.nx && t < nb; ++t)
+                    f[(size_t)t] |= tlmk::kTileGeneral | tlmk::kTileNear;
+            }
     const long long sy = h->px, sz = (long long)h->px * h->ny;
     const uint8_t *mat = h->mat.data();
     for (int k = 0; k < h->nz; ++k)
@@ -313,6 +372,14 @@ tlm_status prepare(tlm_solver *h)
             tile[b] = (int)e;
         }
     }
+    h->nearBox = nearBoxOf(h);
+    if (h->nearBox.bP > 0)
+        for (int b = 0; b < 2; ++b)
+        {
+            const size_t bytes = (size_t)12 * h->nearBox.bP * sizeof(float);
+            TLM_TRY(devAlloc(h, &h->dLo[b], bytes));
+            TLM_CU(h, cudaMemsetAsync(h->dLo[b], 0, bytes, h->stream));
+        }
     {
         const std::vector<uint8_t> flags = tileFlags(h, tile);
         TLM_TRY(devAlloc(h, &h->dTileFlags, flags.size()));
@@ -425,6 +492,15 @@ tlm_status ensureRecords(tlm_solver *h, long long need)
     return TLM_OK;
 }
 
+// Kernel view of the near-field box for a step that reads pulse buffer `cur`.
+tlmk::NearBox nearArgs(const tlm_solver *h, int cur)
+{
+    tlmk::NearBox b = h->nearBox;
+    b.lo_in = b.bP > 0 ? h->dLo[cur] : nullptr;
+    b.lo_out = b.bP > 0 ? h->dLo[cur ^ 1] : nullptr;
+    return b;
+}
+
 // Launch the step kernel in the tile shape `variant` of the storage type
 // (the shape tables of tlm_internal.h).
 template <class S>
@@ -474,6 +550,7 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
     a.stage_wait_ns = h->cfg.stage_wait_us > 0   ? (unsigned long long)h->cfg.stage_wait_us * 1000ull
                       : h->cfg.stage_wait_us < 0 ? 0ull
                                                  : tlmk::kStageWaitNs;
+    a.near = nearArgs(h, h->curBuf);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (h->timing)
     {
@@ -808,10 +885,11 @@ template <class S, class O> static tlm_status pulsesToHost(tlm_solver *h, O *out
     const S *cur = static_cast<const S *>(h->dPulses[h->curBuf]);
     if (h->stateIncident)  // state written by tlm_set_pulses: already incident
         tlmk::planesToAos<S, O><<<gridBlocksFor(h->ncell), 256, 0, h->stream>>>(
-            cur, h->P, h->nx, h->ny, h->nz, h->px, (R)h->scale, d);
+            cur, h->P, h->nx, h->ny, h->nz, h->px, (R)h->scale, d, nearArgs(h, h->curBuf));
     else
         tlmk::incidentToAos<S, O><<<gridBlocksFor(h->ncell), 256, 0, h->stream>>>(
-            cur, h->dMat, h->P, h->nx, h->ny, h->nz, h->px, (R)h->cfg.boundary_rho, (R)h->scale, d);
+            cur, h->dMat, h->P, h->nx, h->ny, h->nz, h->px, (R)h->cfg.boundary_rho, (R)h->scale, d,
+            nearArgs(h, h->curBuf));
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, need * sizeof(O), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -844,9 +922,12 @@ template <class S> static tlm_status setPulsesT(tlm_solver *h, const float *in)
     cudaError_t e = cudaMemcpyAsync(d, in, need * sizeof(float), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess)
     {
+        // the box's residuals go beside the buffer the next step reads
+        tlmk::NearBox nb = nearArgs(h, h->curBuf);
+        nb.lo_out = const_cast<float *>(nb.lo_in);
         tlmk::aosToIncident<S, float><<<gridBlocksFor(h->P), 256, 0, h->stream>>>(
             d, h->dMat, h->P, h->nx, h->ny, h->nz, h->px, (R)(1.0f / h->scale),
-            static_cast<S *>(h->dPulses[h->curBuf]));
+            static_cast<S *>(h->dPulses[h->curBuf]), nb);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -885,6 +966,7 @@ void tlm_config_default(tlm_config *c)
     c->general_tiles = 0;
     c->no_staging = 0;
     c->stage_wait_us = 0;
+    c->near_field = 0;
     c->surface_monitors = 0;
 }
 
@@ -1028,6 +1110,9 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     if (cfg->general_tiles < 0 || cfg->general_tiles > 1)
         return h->fail(TLM_EINVAL, "general_tiles must be 0 or 1");
     if (cfg->no_staging < 0 || cfg->no_staging > 1) return h->fail(TLM_EINVAL, "no_staging must be 0 or 1");
+    if (cfg->near_field < 0) return h->fail(TLM_EINVAL, "near_field must be >= 0");
+    if (cfg->near_field > 0 && cfg->storage != TLM_STORE_F16 && cfg->storage != TLM_STORE_BF16)
+        return h->fail(TLM_EINVAL, "near_field applies to FP16 and BF16 storage only");
     if (cfg->surface_monitors < 0 || cfg->surface_monitors > 1)
         return h->fail(TLM_EINVAL, "surface_monitors must be 0 or 1");
     if (cfg->record_every < 0 || cfg->huy_offset < 0)
@@ -1378,6 +1463,8 @@ tlm_status tlm_set_slab(tlm_handle h, int ghost_lo, int ghost_hi)
         return h->fail(TLM_EINVAL, "slabs do not run surface monitors, cut planes or frames");
     if ((h->storage == TLM_STORE_F16 || h->storage == TLM_STORE_BF16) && !(h->cfg.pulse_scale > 0.0f))
         return h->fail(TLM_EINVAL, "16-bit slabs need an explicit pulse_scale shared by every slab");
+    if (h->cfg.near_field > 0)
+        return h->fail(TLM_EINVAL, "slabs do not exchange near-field residuals (near_field must be 0)");
     h->ghostLo = ghost_lo;
     h->ghostHi = ghost_hi;
     return TLM_OK;
@@ -1585,6 +1672,10 @@ tlm_status tlm_set_pulses(tlm_handle h, const float *in, size_t n)
         return h->fail(TLM_EINVAL, "pulse array must hold 12 values per cell");
     DeviceGuard dg(h->device);
     TLM_TRY(syncState(h));
+    // the state is stored with the scale the steps will decode it with, and
+    // a near-field box needs its residual planes
+    if (h->curStep == 0 && !h->prepared) TLM_TRY(chooseScale(h));
+    if (h->cfg.near_field > 0) TLM_TRY(prepare(h));
     switch (h->storage)
     {
     case TLM_STORE_F64: return setPulsesT<double>(h, in);

@@ -51,6 +51,7 @@ template <class S> struct StepArgs
     const uint8_t *__restrict__ tile_flags;  // per tile: kTileGeneral / kTileDiel (nullptr: all general)
     float neg_zero;                // -0.0f, supplied at run time (see mul2)
     unsigned long long stage_wait_ns;  // staged tiles: consumers' limit on a stage wait (0: first poll)
+    NearBox near;                  // 16-bit storage: the near-field box (near.lo_in == nullptr: none)
 };
 
 // Per-tile flags, computed on the host from the material map and the source
@@ -60,7 +61,9 @@ template <class S> struct StepArgs
 // nodes.
 // kTileEdge: the tile has a node on an outer y or z face (its stage is
 // assembled from runs, see stageRuns).
-enum : uint8_t { kTileGeneral = 1, kTileDiel = 2, kTileEdge = 4 };
+// kTileNear: the tile has nodes in the near-field box (always with
+// kTileGeneral: only the general body completes pulses with residuals).
+enum : uint8_t { kTileGeneral = 1, kTileDiel = 2, kTileEdge = 4, kTileNear = 8 };
 
 #ifdef TLM_CHECKED
 #define TLM_GUARD(idx, limit, code)                                                         \
@@ -580,6 +583,39 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
     const long long P = a.P;
     const long long sy = a.px, sz = (long long)a.px * a.ny;
 
+    // near-field box (16-bit storage): residuals complete the decoded pulses
+    // of box nodes, exactly (block-uniform: the tile's flag)
+    constexpr bool kNearType = Traits<S>::kScaled;
+    bool near = false;
+    if constexpr (kNearType)
+        near = a.near.lo_in != nullptr && a.tile_flags != nullptr && (a.tile_flags[tile] & kTileNear) != 0;
+    // slot s of the V nodes x0.. of row (jj, kk)
+    auto addLo = [&](R(&v)[V], int s, int jj, int kk) {
+        if constexpr (kNearType)
+        {
+            if (near && live)
+            {
+#pragma unroll
+                for (int c = 0; c < V; ++c)
+                {
+                    const long long b = a.near.at(x0 + c, jj, kk);
+                    if (b >= 0) v[c] += a.near.lo_in[s * a.near.bP + b];
+                }
+            }
+        }
+    };
+    // slot s of node (ii, jj, kk)
+    auto addLo1 = [&](R &v, int s, int ii, int jj, int kk) {
+        if constexpr (kNearType)
+        {
+            if (near && live)
+            {
+                const long long b = a.near.at(ii, jj, kk);
+                if (b >= 0) v += a.near.lo_in[s * a.near.bP + b];
+            }
+        }
+    };
+
     uint8_t m[V];
     if (live && TLM_GUARD(node0, P - V + 1, 1))
         loadMat<V>(a.mat, node0, m);
@@ -607,6 +643,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
 #pragma unroll
                 for (int c = 0; c < V; ++c) inc[s][c] = R(0);
             }
+            addLo(inc[s], s, j, k);
         }
     }
     else
@@ -660,6 +697,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
 #pragma unroll
                 for (int c = 0; c < V; ++c) ox[s][c] = R(0);
             }
+            addLo(ox[s], s, j, k);  // before the lane shuffles below hand them on
         }
         R prevX[2], nextX[2];
 #pragma unroll
@@ -673,14 +711,20 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
 #pragma unroll
             for (int t = 0; t < 2; ++t)
                 if (TLM_GUARD((2 + t) * P + node0 - 1, 12 * P, 6))
+                {
                     prevX[t] = loadOne<S>(a.in, (2 + t) * P + node0 - 1, a.scale);
+                    addLo1(prevX[t], 2 + t, x0 - 1, j, k);
+                }
         }
         if (lane == 31 && needNext)
         {
 #pragma unroll
             for (int t = 0; t < 2; ++t)
                 if (TLM_GUARD(t * P + node0 + V, 12 * P, 6))
+                {
                     nextX[t] = loadOne<S>(a.in, t * P + node0 + V, a.scale);
+                    addLo1(nextX[t], t, x0 + V, j, k);
+                }
         }
 #pragma unroll
         for (int c = 0; c < V; ++c)
@@ -731,6 +775,10 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                         for (int c = 0; c < V; ++c) vLo[c] = R(0);
                     }
                     if (atLo)
+                        addLo(vLo, sLo, j, k);
+                    else
+                        addLo(vLo, sHi, ax == 1 ? j - 1 : j, ax == 2 ? k - 1 : k);
+                    if (atLo)
                     {
 #pragma unroll
                         for (int c = 0; c < V; ++c) vLo[c] = a.rho * vLo[c];
@@ -740,6 +788,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                         R own[V];
                         if (TLM_GUARD(sLo * P + node0, 12 * P - V + 1, 8))
                             loadVec<S, V>(a.in, sLo * P + node0, own, a.scale);
+                        addLo(own, sLo, j, k);
 #pragma unroll
                         for (int c = 0; c < V; ++c)
                             if ((pm >> c) & 1u) vLo[c] = -own[c];
@@ -756,6 +805,10 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                         for (int c = 0; c < V; ++c) vHi[c] = R(0);
                     }
                     if (atHi)
+                        addLo(vHi, sHi, j, k);
+                    else
+                        addLo(vHi, sLo, ax == 1 ? j + 1 : j, ax == 2 ? k + 1 : k);
+                    if (atHi)
                     {
 #pragma unroll
                         for (int c = 0; c < V; ++c) vHi[c] = a.rho * vHi[c];
@@ -765,6 +818,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                         R own[V];
                         if (TLM_GUARD(sHi * P + node0, 12 * P - V + 1, 10))
                             loadVec<S, V>(a.in, sHi * P + node0, own, a.scale);
+                        addLo(own, sHi, j, k);
 #pragma unroll
                         for (int c = 0; c < V; ++c)
                             if ((pp >> c) & 1u) vHi[c] = -own[c];
@@ -929,8 +983,25 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
         {
             if (TLM_GUARD(s * P + node0, 12 * P - V + 1, 12))
             {
-                storeVec<S, V>(a.out, s * P + node0, outv[s], a.inv_scale, a.stochastic != 0,
+                // box nodes round to nearest: their residual completes that value
+                storeVec<S, V>(a.out, s * P + node0, outv[s], a.inv_scale, a.stochastic != 0 && !near,
                                a.round_seed, s);
+            }
+        }
+        if constexpr (kNearType)
+        {
+            if (near)
+            {
+#pragma unroll
+                for (int c = 0; c < V; ++c)
+                {
+                    const long long b = a.near.at(x0 + c, j, k);
+                    if (b < 0) continue;
+#pragma unroll
+                    for (int s = 0; s < 12; ++s)
+                        a.near.lo_out[s * a.near.bP + b] =
+                            outv[s][c] - decode(encode<S>(outv[s][c], a.inv_scale), a.scale);
+                }
             }
         }
         if (anyDiel && dielMask)

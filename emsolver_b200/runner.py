@@ -7,7 +7,7 @@ from .solver import MatProps, TlmConfig, TlmSolver, VoxelGridSpec
 def build_solver(w, device: int = 0, storage: int | None = None, steps_per_launch: int = 0,
                  variant: str | None = None, pulse_scale: float = 0.0, kernel_variant: int = 0,
                  rounding: int = 0, general_tiles: bool = False, no_staging: bool = False,
-                 stage_wait_us: int = 0) -> TlmSolver:
+                 stage_wait_us: int = 0, near_field: int | None = None) -> TlmSolver:
     """Create, set up and populate a solver exactly as the reference would be:
     setup, ports (in order), plane wave, probes at cell centres, port DFT."""
     s = TlmSolver(device, variant)
@@ -18,7 +18,8 @@ def build_solver(w, device: int = 0, storage: int | None = None, steps_per_launc
                     boundaryRho=w.rho, storage=w.storage if storage is None else storage,
                     stepsPerLaunch=steps_per_launch, pulseScale=pulse_scale,
                     kernelVariant=kernel_variant, rounding=rounding, generalTiles=general_tiles,
-                    noStaging=no_staging, stageWaitUs=stage_wait_us)
+                    noStaging=no_staging, stageWaitUs=stage_wait_us,
+                    nearField=w.meta.get("near_field", 0) if near_field is None else near_field)
     s.setup(grid, w.mat, [MatProps(e, g) for e, g in w.table], cfg)
     if w.waveform == 3 and w.sv is not None:
         s.setSourceTable(w.sv)

@@ -94,6 +94,7 @@ class TlmConfig:
     surfaceMonitors: bool = False  # PEC-surface Js and Huygens-box DFT monitors
     noStaging: bool = False    # True: no shared-memory staging of FP32 interior tiles (cross-checks)
     stageWaitUs: int = 0       # staged tiles' wait limit in us (0 default ~2 s, < 0 first poll)
+    nearField: int = 0         # FP16/BF16: radius of the FP32-residual box around PEC and ports (0 none)
 
     def to_c(self):
         c = _lib.ConfigC()
@@ -114,6 +115,7 @@ class TlmConfig:
         c.surface_monitors = 1 if self.surfaceMonitors else 0
         c.no_staging = 1 if self.noStaging else 0
         c.stage_wait_us = int(self.stageWaitUs)
+        c.near_field = int(self.nearField)
         return c
 
 

@@ -129,6 +129,15 @@ typedef struct tlm_config {
                             < 0 = at the first poll that finds the stage not
                             ready (exercises the error path). The producer
                             always lets the copies it issued land */
+    int near_field;      /* FP16/BF16 storage: radius r in cells of the
+                            near-field box, the bounding box of the PEC cells
+                            and port cells grown by r (0 = none). Box cells
+                            keep the FP32 residual of their stored pulses
+                            beside them (4 B more per pulse, read and written
+                            in the box only) and step as FP32 storage would;
+                            the rest of the grid is stored in 16 bits. The box
+                            is fixed when the first step (or tlm_set_pulses)
+                            prepares the grid */
 } tlm_config;
 
 typedef struct tlm_solver *tlm_handle;
