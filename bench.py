@@ -1,7 +1,8 @@
 """Throughput of the B200 SCN TLM step (node-updates/s and % of HBM roofline).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload heterogeneous|plain|precision] [--storage f32|bf16|f16|f64|bfp16]
+                    [--workload heterogeneous|plain|precision|energy|batched|served|fdtd]
+                    [--storage f32|bf16|f16|f64|bfp16] [--near-field R]
 
 A "step" is one TLM time step (inject, monitors, scatter, connect) of the
 whole grid. Default workload: 192^3 heterogeneous grid (16 lossy dielectric
@@ -40,7 +41,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=20)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="heterogeneous",
-                   choices=["heterogeneous", "plain", "precision", "batched", "served", "fdtd"])
+                   choices=["heterogeneous", "plain", "precision", "energy", "batched", "served", "fdtd"])
     p.add_argument("--instances", type=int, default=256, help="batched: number of instances")
     p.add_argument("--requests", type=int, default=200, help="served: number of requests")
     p.add_argument("--rate", type=float, default=200.0, help="served: mean arrivals per second")
@@ -48,7 +49,14 @@ def parse():
                    help="served: largest cubic edge (the full stream goes to 256)")
     p.add_argument("--steps-max", type=int, default=2000,
                    help="served: most steps per request (the full stream goes to 8000)")
-    p.add_argument("--autotune", action="store_true", help="batched: run the autotuner first")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="batched: skip the autotuner (default tuning, windows of --window steps)")
+    p.add_argument("--window", type=int, default=100, help="batched: steps per CUDA-graph window")
+    p.add_argument("--near-field", type=int, default=None,
+                   help="16-bit storage: radius of the FP32-residual box around PEC and ports "
+                        "(default 6 for f16/bf16)")
+    p.add_argument("--precision-steps", type=int, default=8000, help="precision: steps per mode")
+    p.add_argument("--energy-steps", type=int, default=3000, help="energy: steps per mode")
     p.add_argument("--chunk", type=int, default=32, help="batched: instances set up per window")
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64", "bfp16"])
     p.add_argument("--steps-per-launch", type=int, default=0)
@@ -67,6 +75,30 @@ def make_workload(name, steps):
 
 
 STORAGE = {"f32": (0, 4, 4), "bf16": (1, 2, 4), "f16": (2, 2, 4), "f64": (3, 8, 8), "bfp16": (4, 2, 4)}
+
+
+def near_of(args):
+    """The near-field radius for the storage mode (default 6 for FP16/BF16)."""
+    if args.storage not in ("f16", "bf16"):
+        return 0
+    return 6 if args.near_field is None else args.near_field
+
+
+def box_nodes(s):
+    b = s.nearFieldBox()
+    return 0 if b is None else b[1][0] * b[1][1] * b[1][2]
+
+
+def check_world(args):
+    """--gpus N must match the launcher's WORLD_SIZE (torchrun starts the
+    ranks; this script does not)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        sys.stderr.write(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch N ranks with "
+                         f"python -m torch.distributed.run --nproc-per-node {args.gpus} bench.py --gpus "
+                         f"{args.gpus} ...\n")
+        sys.exit(2)
+    return world
 DTYPE = {"f32": "f32", "bf16": "bf16 storage / f32 arithmetic",
          "f16": "f16 storage / f32 arithmetic", "f64": "f64",
          "bfp16": "16-bit block floating point storage / f32 arithmetic"}
@@ -197,7 +229,8 @@ def reference_rate(w, steps_budget, seconds_budget, warm=2):
 
 
 def run_reference_arm(args):
-    d = Dist(args.gpus) if int(os.environ.get("WORLD_SIZE", "1")) > 1 else None
+    world = check_world(args)
+    d = Dist(args.gpus) if world > 1 else None
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -205,7 +238,7 @@ def run_reference_arm(args):
     w = make_workload(args.workload, args.warmup + args.steps)
     rate, cores, kind, done, dt = reference_rate(w, args.steps, 120.0, warm=min(args.warmup, 3))
     line = {
-        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * dt / done, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "impl": "reference",
@@ -220,16 +253,48 @@ def run_reference_arm(args):
         d.close()
 
 
+def accuracy_vs_reference(s, w, steps_done):
+    """Port and probe records of the timed solve against the reference's own
+    CPU step on the same grid (tests/golden/heterogeneous.npz, written by the
+    reference compiled headless): the largest |difference| over the peak of
+    each series, over the steps both runs cover."""
+    path = os.path.join(ROOT, "tests", "golden", "heterogeneous.npz")
+    if w.name != "heterogeneous" or (w.nx, w.ny, w.nz) != (192, 192, 192) or not os.path.exists(path):
+        return None
+    g = np.load(path)
+    n = min(steps_done, g["port0_v"].shape[0])
+    ours = {}
+    p = s.port(0)
+    ours["port0_v"], ours["port0_i"] = p.vRec, p.iRec
+    for q in range(len(w.probes_cell)):
+        r = s.probe(q)
+        ours[f"probe{q}_ex"], ours[f"probe{q}_ey"], ours[f"probe{q}_ez"] = r.ex, r.ey, r.ez
+    worst, exact = 0.0, True
+    for k, a in ours.items():
+        a = np.asarray(a[:n], np.float64)
+        b = g[k][:n].astype(np.float64)
+        d = float(np.abs(a - b).max()) if n else 0.0
+        peak = float(np.abs(b).max()) if n else 0.0
+        exact = exact and d == 0.0
+        if peak > 0:
+            worst = max(worst, d / peak)
+    return {"vs": "the reference's CPU step on the same grid (its records in tests/golden/heterogeneous.npz)",
+            "steps_compared": n, "series": len(ours), "max_abs_diff_over_peak": worst,
+            "bitwise": bool(exact), "tolerance": 1e-5}
+
+
 def run_ours(args):
     from emsolver_b200.runner import build_solver
     import torch
 
+    check_world(args)
     dist = Dist(args.gpus)
     dev = dist.local if dist.world > 1 else 0
     code, sbytes, rbytes = STORAGE[args.storage]
+    nf = near_of(args)
     w = make_workload(args.workload, args.warmup + args.steps)
     w.steps = args.warmup + args.steps
-    s = build_solver(w, device=dev, storage=code, steps_per_launch=args.steps_per_launch)
+    s = build_solver(w, device=dev, storage=code, steps_per_launch=args.steps_per_launch, near_field=nf)
     s.step(args.warmup)
     torch.cuda.set_device(dev)
     ext = torch.cuda.ExternalStream(s.stream(), device=dev)
@@ -253,11 +318,15 @@ def run_ours(args):
     per_step_kernels = s.stepLaunches()
     ms_max = dist.max(ms)
     kern_max = dist.max(kern_ms)
+    accuracy = accuracy_vs_reference(s, w, args.warmup + args.steps) if args.storage == "f32" else None
+    nbox = box_nodes(s)
     s.close()
 
     n = w.ncells
     value = dist.world * n * args.steps / (ms_max / 1000.0)
-    bytes_step = w.bytes_per_step(sbytes, rbytes)
+    # 16-bit storage with a near-field box: its cells also read and write
+    # the 12 FP32 residuals
+    bytes_step = w.bytes_per_step(sbytes, rbytes) + 96 * nbox
     per_launch_ms = kern_max / max(launches, 1)
     achieved = bytes_step / (per_launch_ms / 1000.0) / 1e9
     peak, peak_kind = peaks()
@@ -270,7 +339,7 @@ def run_ours(args):
     if not args.no_e2e:
         dist.barrier()
         t0 = time.perf_counter()
-        s2 = build_solver(w, device=dev, storage=code, steps_per_launch=args.steps_per_launch)
+        s2 = build_solver(w, device=dev, storage=code, steps_per_launch=args.steps_per_launch, near_field=nf)
         s2.step(args.steps)
         recs = [s2.probe(q) for q in range(len(w.probes_cell))]
         ports = [s2.port(p) for p in range(len(w.ports))]
@@ -301,7 +370,8 @@ def run_ours(args):
             "config": {"workload": f"{args.workload} {w.nx}x{w.ny}x{w.nz}, {len(w.table)} lossy "
                                    f"dielectric boxes, {len(w.probes_cell)} probes",
                        "nodes": n, "dielectric_nodes": w.n_diel(),
-                       "storage": args.storage, "steps_per_launch": window,
+                       "storage": args.storage, "near_field": nf, "near_field_cells": nbox,
+                       "steps_per_launch": window,
                        "parallelism": f"replicas x{dist.world}",
                        "l2": f"state {2 * 12 * sbytes * n / 1e6:.0f} MB > L2 (126 MB); no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -310,6 +380,7 @@ def run_ours(args):
                          "kernel_ms_per_step": per_launch_ms, "kernels_per_step": per_step_kernels},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "accuracy": accuracy,
             "gpu_launches": launches * per_step_kernels + epilogues,
             "clocks": clk,
         }
@@ -381,6 +452,106 @@ def run_fdtd(args):
     print(json.dumps(line), flush=True)
 
 
+PRECISION_MODES = [("f64", 3, 0), ("f32", 0, 0), ("f16", 2, 0), ("f16_near6", 2, 6), ("bf16", 1, 0),
+                   ("bf16_near6", 1, 6), ("bfp16", 4, 0)]
+
+
+def timed_solve(w, storage, near):
+    """Set up, step the whole run with CUDA events on the solver's stream,
+    return (solver, ms)."""
+    import torch
+    from emsolver_b200.runner import build_solver
+    s = build_solver(w, storage=storage, near_field=near)
+    s.step(1)
+    ext = torch.cuda.ExternalStream(s.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    s.stepAsync(w.steps - 1)
+    e1.record(ext)
+    s.sync()
+    torch.cuda.synchronize()
+    return s, e0.elapsed_time(e1)
+
+
+def run_precision(args):
+    """The precision configuration: 384x384x256 grid, half-wave dipole of 60
+    PEC cells with a 1-cell feed gap, Gaussian voltage source across the gap,
+    outer reflection 0, port DFT at 64 frequencies over 0.5-1.5 of resonance,
+    --precision-steps steps (8000 by default), in every storage mode. Input
+    impedance and S11 of each mode against the FP64 storage mode (bitwise
+    the FP64 oracle on the grids the tests cover), largest relative error
+    over the 64 frequencies; node-updates/s and the fraction of the measured
+    HBM bandwidth at each mode's algorithmic bytes."""
+    from emsolver_b200 import workloads
+    from emsolver_b200.solver import s11_from_dft
+    w = workloads.precision_dipole(steps=args.precision_steps)
+    peak, kind = peaks()
+    res = {}
+    for name, code, near in PRECISION_MODES:
+        s, ms = timed_solve(w, code, near)
+        v, i = s.portDft(0)
+        z, g = s11_from_dft(v, i)
+        sb, rb = {0: (4, 4), 1: (2, 4), 2: (2, 4), 3: (8, 8), 4: (2, 4)}[code]
+        nbox = box_nodes(s)
+        s.close()
+        per_step = ms / (w.steps - 1)
+        bytes_step = w.bytes_per_step(sb, rb) + 96 * nbox
+        res[name] = {"z": z, "s11": g, "ms_per_step": per_step, "near_field_cells": nbox,
+                     "node_updates_per_s": w.ncells / (per_step / 1e3),
+                     "hbm_frac": bytes_step / (per_step / 1e3) / 1e9 / peak}
+    zr, gr = res["f64"]["z"], res["f64"]["s11"]
+    modes = {}
+    for name, r in res.items():
+        modes[name] = {"s11_rel_err_vs_fp64": float(np.max(np.abs(r["s11"] - gr) / np.abs(gr))),
+                       "zin_rel_err_vs_fp64": float(np.max(np.abs(r["z"] - zr) / np.abs(zr))),
+                       "ms_per_step": r["ms_per_step"], "node_updates_per_s": r["node_updates_per_s"],
+                       "hbm_frac": r["hbm_frac"], "near_field_cells": r["near_field_cells"]}
+    head = modes["f16_near6"]
+    line = {"metric": "S11 relative error vs FP64 storage", "value": head["s11_rel_err_vs_fp64"],
+            "unit": "relative (max over 64 frequencies)", "n_gpus": 1, "steps": w.steps, "warmup": 1,
+            "ms_per_step": head["ms_per_step"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f16 storage + FP32 residuals in the near-field box / f32 arithmetic",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"precision dipole {w.nx}x{w.ny}x{w.nz}, {w.meta['length'] - 1} PEC cells "
+                                   f"+ 1-cell gap, {len(w.dft_freqs)} DFT frequencies, {w.steps} steps",
+                       "headline_mode": "f16_near6", "peak_kind": kind},
+            "zin_rel_err_vs_fp64": head["zin_rel_err_vs_fp64"],
+            "s11_rel_err_vs_fp64": {k: m["s11_rel_err_vs_fp64"] for k, m in modes.items()},
+            "modes": modes}
+    print(json.dumps(line), flush=True)
+
+
+def run_energy(args):
+    """Energy drift of a closed lossless grid: 128^3 cells, outer reflection
+    1, no loss, a PEC dipole of 31 cells fed by a Gaussian pulse that has
+    died out by step 512. The FP64 energy history (every 16 steps, the
+    reference's cadence) from step 512 to the last step stays constant in
+    exact arithmetic; reported per storage mode: the relative change from
+    step 512 to the end and the largest relative excursion."""
+    from emsolver_b200 import workloads
+    w = workloads.dipole(128, 128, 128, 31, None, steps=args.energy_steps, nfreq=8, name="closed_cavity")
+    w.rho = 1.0
+    modes = {}
+    for name, code, near in PRECISION_MODES:
+        s, ms = timed_solve(w, code, near)
+        st, ev = s.getEnergyHistory(f64=True)
+        s.close()
+        st, ev = np.asarray(st), np.asarray(ev, np.float64)
+        k0 = int(np.searchsorted(st, 512))
+        e0 = ev[k0]
+        modes[name] = {"drift": float((ev[-1] - e0) / e0),
+                       "max_excursion": float(np.max(np.abs(ev[k0:] - e0)) / e0),
+                       "from_step": int(st[k0]), "to_step": int(st[-1]), "ms_per_step": ms / (w.steps - 1)}
+    line = {"metric": "relative energy drift, closed lossless grid", "value": modes["f32"]["drift"],
+            "unit": "relative", "n_gpus": 1, "steps": w.steps, "warmup": 1,
+            "ms_per_step": modes["f32"]["ms_per_step"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (per-mode results in `modes`)", "data": "synthetic",
+            "config": {"workload": f"closed cavity {w.nx}x{w.ny}x{w.nz}, rho 1, lossless, 31-cell PEC dipole, "
+                                   f"Gaussian pulse source, {w.steps} steps"},
+            "modes": modes}
+    print(json.dumps(line), flush=True)
+
+
 def sequential_solves(ws):
     """Each instance alone through the plain API, one after the other:
     setup, all steps, port DFT back to the host, free. Returns per-solve
@@ -397,33 +568,76 @@ def sequential_solves(ws):
     return times
 
 
-def run_batched(args):
-    """256 independent dipole instances, edges U{24..96}, 1000 steps each."""
-    import torch
-    from emsolver_b200 import Batch, workloads
+def batch_dfts(ws, storage, near, tuning=None):
+    """Every instance attached to one batch and run to its end; returns the
+    port DFTs (untimed helper for the accuracy check)."""
+    from emsolver_b200 import Batch
     from emsolver_b200.runner import build_solver
+    solvers = [build_solver(w, storage=storage, near_field=near) for w in ws]
+    with Batch() as b:
+        for s in solvers:
+            b.attach(s)
+        if tuning is not None:
+            b.set_tuning(tuning)
+        b.run()
+    out = [s.portDft(0) for s in solvers]
+    for s in solvers:
+        s.close()
+    return out
+
+
+def run_batched(args):
+    """256 independent dipole instances (edges U{24..96} per axis, wire of
+    U[0.3,0.9] of the z extent with a 1-cell gap port, dielectric slab eps_r
+    U[1,6]), 1000 steps each, FP32 storage unless --storage says otherwise;
+    CUDA-graph windows of 100 steps, tile shape and window chosen by the
+    autotuner (--no-autotune: defaults). Against the same instances solved
+    one after the other through the plain API; every instance's S11 against
+    an FP64-storage batch of the same instances."""
+    import torch
+    from emsolver_b200 import Batch, BatchTuning, workloads
+    from emsolver_b200.runner import build_solver
+    from emsolver_b200.solver import s11_from_dft
+    code, sbytes, rbytes = STORAGE[args.storage]
+    nf = near_of(args)
     ws = workloads.batched_instances(count=args.instances, steps=1000)
+    for w in ws:
+        w.storage = code
+        w.meta["near_field"] = nf
     nodes = sum(w.ncells for w in ws)
     work = sum(w.ncells * w.steps for w in ws)
-    bytes_all = sum(w.bytes_per_step() * w.steps for w in ws)
     sequential_solves(ws[:4])                        # warm-up (context, kernels)
     seq = sequential_solves(ws)
     # the solves through Batch.solve: set-up of the next instances overlaps
     # the device's windows, finished members leave at once
     tp = time.perf_counter()
     with Batch() as bp:
+        bp.set_tuning(BatchTuning(steps_per_launch=args.window))
         dfts = bp.solve(ws, build_solver, lambda s, w: s.portDft(0), chunk=args.chunk)
     pipelined_s = time.perf_counter() - tp
     assert len(dfts) == len(ws)
-    # all instances attached at once, the device time of the whole run
+    # the tuning: the autotuner on these instances (untimed; cached by
+    # workload signature), or the defaults
+    if args.no_autotune:
+        tuning = BatchTuning(steps_per_launch=args.window)
+    else:
+        tsolvers = [build_solver(w) for w in ws]
+        with Batch() as bt:
+            for s in tsolvers:
+                bt.attach(s)
+            tuning = bt.autotune(trial_windows=2)
+        for s in tsolvers:
+            s.close()
+    # all instances attached at once: set-up, the device time of the whole
+    # run, read-back
     t0 = time.perf_counter()
     solvers = [build_solver(w) for w in ws]
     tb = time.perf_counter()
     b = Batch()
     for s in solvers:
         b.attach(s)
+    b.set_tuning(tuning)
     ta = time.perf_counter()
-    tuning = b.autotune(trial_windows=2) if args.autotune else b.get_tuning()
     t1 = time.perf_counter()
     ext = torch.cuda.ExternalStream(b.stream())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -432,28 +646,39 @@ def run_batched(args):
     e1.record(ext)
     torch.cuda.synchronize()
     gpu_ms = e0.elapsed_time(e1)
-    for s in solvers:
-        s.portDft(0)
+    got = [s.portDft(0) for s in solvers]
     t2 = time.perf_counter()
     b.close()
+    nbox = sum(box_nodes(s) for s in solvers)
     for s in solvers:
         s.close()
     t3 = time.perf_counter()
     batched_s = t3 - t0
+    # accuracy: S11 of every instance against the FP64 storage mode
+    ref = batch_dfts(ws, 3, 0)
+    errs = []
+    for (v, i), (rv, ri) in zip(got, ref):
+        a, r = s11_from_dft(v, i)[1], s11_from_dft(rv, ri)[1]
+        errs.append(float(np.max(np.abs(a - r) / np.abs(r))))
     peak, kind = peaks()
+    bytes_all = sum(w.bytes_per_step(sbytes, rbytes) * w.steps for w in ws) + 96 * nbox * 1000
     line = {
         "metric": "batched solves/s", "value": len(ws) / batched_s, "unit": "solves/s",
         "n_gpus": 1, "steps": 1000, "warmup": 4, "ms_per_step": gpu_ms / 1000.0,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": DTYPE[args.storage] + (f", near-field box r={nf}" if nf else ""),
         "data": "synthetic (seeded)",
         "config": {"workload": f"batched: {len(ws)} dipole instances, edges U{{24..96}}, 1000 steps",
-                   "nodes": nodes, "tuning": tuning.__dict__,
+                   "nodes": nodes, "storage": args.storage, "near_field": nf,
+                   "tuning": tuning.__dict__, "autotuned": not args.no_autotune,
                    "includes": "setup of every instance, all steps, port DFT read-back, free"},
         "sequential_plain_gpu": {"value": len(ws) / sum(seq), "unit": "solves/s",
                                  "seconds": sum(seq), "p50_s": float(np.percentile(seq, 50)),
                                  "p99_s": float(np.percentile(seq, 99))},
         "speedup_vs_sequential": sum(seq) / batched_s,
         "seconds": batched_s,
+        "s11_rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "instances": len(errs),
+                                "within_1e-3": int(sum(e <= 1e-3 for e in errs))},
         "pipelined": {"value": len(ws) / pipelined_s, "unit": "solves/s", "seconds": pipelined_s,
                       "chunk": args.chunk, "speedup_vs_sequential": sum(seq) / pipelined_s,
                       "api": "Batch.solve: host set-up of the next chunk overlaps each window"},
@@ -557,6 +782,10 @@ def main():
         run_served(args)
     elif args.workload == "fdtd":
         run_fdtd(args)
+    elif args.workload == "precision":
+        run_precision(args)
+    elif args.workload == "energy":
+        run_energy(args)
     else:
         run_ours(args)
 

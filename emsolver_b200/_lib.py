@@ -311,6 +311,7 @@ SIGNATURES = {
     "tlm_set_kernel_timing": (_st, [_h, C.c_int]),
     "tlm_kernel_time": (_st, [_h, _P(C.c_double), _P(C.c_longlong)]),
     "tlm_step_launches": (_st, [_h, _P(C.c_int)]),
+    "tlm_near_field_box": (_st, [_h, _P(C.c_int)]),
 }
 
 

@@ -305,6 +305,57 @@ __global__ void aosToStubs(const R *__restrict__ in, long long P, int nx, int ny
     }
 }
 
+// Material map in the reference's cell order -> the padded layout (row pitch
+// px, padding columns PEC), one padded node per thread.
+static __global__ void padMaterial(const uint8_t *__restrict__ raw, int nx, int px, long long rows,
+                            uint8_t *__restrict__ out)
+{
+    const long long P = rows * px;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < P;
+         n += (long long)gridDim.x * blockDim.x)
+    {
+        const long long r = n / px;
+        const int i = (int)(n - r * px);
+        out[n] = i < nx ? raw[r * nx + i] : (uint8_t)kPec;
+    }
+}
+
+// The material part of the step kernel's tile flags (tiles of T consecutive
+// padded nodes, T a multiple of 32): kTileGeneral when a node of the tile is
+// PEC or has a PEC neighbour inside the grid, kTileDiel when it holds a
+// dielectric node; padding columns count for neither. One padded node per
+// thread; the 32 nodes of a warp lie in one tile, so one lane ORs the
+// warp's flags into that tile's word.
+static __global__ void materialTileFlags(const uint8_t *__restrict__ mat, int nx, int ny, int nz, int px, long long T,
+                                  unsigned *__restrict__ flags)
+{
+    const long long sy = px, sz = (long long)px * ny, P = sz * nz;
+    for (long long base = blockIdx.x * (long long)blockDim.x; base < P; base += (long long)gridDim.x * blockDim.x)
+    {
+        const long long n = base + threadIdx.x;
+        unsigned f = 0;
+        if (n < P)
+        {
+            const long long r = n / px;
+            const int i = (int)(n - r * px);
+            const int j = (int)(r % ny), k = (int)(r / ny);
+            if (i < nx)
+            {
+                const uint8_t m = mat[n];
+                if (m >= kDiel0) f |= kTileDiel;
+                bool g = m == kPec;
+                g = g || (i > 0 && mat[n - 1] == kPec) || (i < nx - 1 && mat[n + 1] == kPec);
+                g = g || (j > 0 && mat[n - sy] == kPec) || (j < ny - 1 && mat[n + sy] == kPec);
+                g = g || (k > 0 && mat[n - sz] == kPec) || (k < nz - 1 && mat[n + sz] == kPec);
+                if (g) f |= kTileGeneral;
+            }
+        }
+        f = __reduce_or_sync(0xffffffffu, f);
+        const long long n0 = base + (threadIdx.x & ~31u);
+        if ((threadIdx.x & 31) == 0 && f != 0 && n0 < P) atomicOr(&flags[n0 / T], f);
+    }
+}
+
 // Unitarity KATs (TlmSolver.cpp:116-169): max |S^T W S - W| with W = 1 on
 // the 12 links and yh on the 3 stubs (stub case).
 static __global__ void unitarityKernel(float epsr, int withStubs, float *err)

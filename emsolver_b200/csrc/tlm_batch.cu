@@ -886,11 +886,12 @@ tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *
         *msPerStep = ms / (t.steps_per_launch * trial_windows);
         return TLM_OK;
     };
-    tlm_batch_tuning best{ 0, 64, 0, 1, 1e30 };
+    // tile shapes at windows of 100 steps, then other window lengths for the best shape
+    tlm_batch_tuning best{ 0, 100, 0, 1, 1e30 };
     tlm_status st = TLM_OK;
     for (int v = 0; v < nvar && st == TLM_OK; ++v)
     {
-        tlm_batch_tuning t{ v, 64, 0, 1, 0.0 };
+        tlm_batch_tuning t{ v, 100, 0, 1, 0.0 };
         double ms = 0.0;
         st = trial(t, &ms);
         if (st == TLM_OK && ms < best.ms_per_step)
@@ -899,7 +900,7 @@ tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *
             best.ms_per_step = ms;
         }
     }
-    for (int w : { 16, 32, 128 })
+    for (int w : { 50, 200 })
     {
         if (st != TLM_OK) break;
         tlm_batch_tuning t = best;

@@ -168,14 +168,14 @@ tlmk::NearBox nearBoxOf(const tlm_solver *h)
     return b;
 }
 
-std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tileBegin)
+std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tileBegin,
+                               const std::vector<unsigned> &matFlags)
 {
     const long long T = (long long)kBlock * h->V;
     const int nb = h->nblocks;
     std::vector<uint8_t> f((size_t)nb, h->cfg.general_tiles ? tlmk::kTileGeneral : 0);
-    auto mark = [&](long long node, uint8_t bit) {
-        if (node >= 0 && node < h->P) f[(size_t)(node / T)] |= bit;
-    };
+    // PEC and dielectric flags from the device pass over the material map
+    for (int b = 0; b < nb; ++b) f[(size_t)b] |= (uint8_t)matFlags[(size_t)b];
     if (h->nquads % kBlock) f[(size_t)nb - 1] |= tlmk::kTileGeneral;
     // outer y and z faces: the first and last plane, the first and last row
     // of every plane
@@ -202,34 +202,28 @@ std::vector<uint8_t> tileFlags(const tlm_solver *h, const std::vector<int> &tile
                 for (long long t = (r0 + nb3.x0) / T; t * T < r0 + nb3.x0 + nb3.nx && t < nb; ++t)
                     f[(size_t)t] |= tlmk::kTileGeneral | tlmk::kTileNear;
             }
-    const long long sy = h->px, sz = (long long)h->px * h->ny;
-    const uint8_t *mat = h->mat.data();
-    for (int k = 0; k < h->nz; ++k)
-        for (int j = 0; j < h->ny; ++j)
-        {
-            const long long r0 = ((long long)k * h->ny + j) * h->px;
-            const uint8_t *row = mat + ((size_t)k * h->ny + j) * h->nx;
-            for (int i = 0; i < h->nx; ++i)
-            {
-                const uint8_t m = row[i];
-                if (m == tlmk::kAir) continue;
-                const long long node = r0 + i;
-                if (m >= tlmk::kDiel0)
-                {
-                    f[(size_t)(node / T)] |= tlmk::kTileDiel;
-                    continue;
-                }
-                // PEC: the node and every node that has it as a neighbour
-                mark(node, tlmk::kTileGeneral);
-                if (i > 0) mark(node - 1, tlmk::kTileGeneral);
-                if (i < h->nx - 1) mark(node + 1, tlmk::kTileGeneral);
-                mark(node - sy, tlmk::kTileGeneral);
-                mark(node + sy, tlmk::kTileGeneral);
-                mark(node - sz, tlmk::kTileGeneral);
-                mark(node + sz, tlmk::kTileGeneral);
-            }
-        }
     return f;
+}
+
+// The material part of the tile flags, computed on the device from the
+// padded material map (tlmk::materialTileFlags) and read back.
+tlm_status materialFlags(tlm_solver *h, std::vector<unsigned> &out)
+{
+    out.assign((size_t)h->nblocks, 0u);
+    unsigned *d = nullptr;
+    TLM_TRY(tmpAlloc(h, &d, out.size() * sizeof(unsigned)));
+    cudaError_t e = cudaMemsetAsync(d, 0, out.size() * sizeof(unsigned), h->stream);
+    if (e == cudaSuccess)
+    {
+        tlmk::materialTileFlags<<<std::max(1, std::min(h->nblocks * h->V, 148 * 16)), 256, 0, h->stream>>>(
+            h->dMat, h->nx, h->ny, h->nz, h->px, (long long)kBlock * h->V, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out.data(), d, out.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFreeAsync(d, h->stream);
+    return h->cuda(e, "tile flags from the material map");
 }
 
 // Build the device tables of sources and monitors once, before the first
@@ -381,7 +375,9 @@ tlm_status prepare(tlm_solver *h)
             TLM_CU(h, cudaMemsetAsync(h->dLo[b], 0, bytes, h->stream));
         }
     {
-        const std::vector<uint8_t> flags = tileFlags(h, tile);
+        std::vector<unsigned> mf;
+        TLM_TRY(materialFlags(h, mf));
+        const std::vector<uint8_t> flags = tileFlags(h, tile, mf);
         TLM_TRY(devAlloc(h, &h->dTileFlags, flags.size()));
         TLM_CU(h, cudaMemcpyAsync(h->dTileFlags, flags.data(), flags.size(), cudaMemcpyHostToDevice,
                                   h->stream));
@@ -1118,17 +1114,16 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
     if (cfg->record_every < 0 || cfg->huy_offset < 0)
         return h->fail(TLM_EINVAL, "record_every and huy_offset must be >= 0");
     if (!std::isfinite(cfg->boundary_rho)) return h->fail(TLM_EINVAL, "boundary_rho not finite");
-    bool anyDiel = false;
-    for (long long c = 0; c < n; ++c)
-    {
-        if (mat[c] >= TLM_MAT_DIEL0)
-        {
-            anyDiel = true;
-            if (mat[c] - TLM_MAT_DIEL0 >= n_table)
+    // the largest id decides (a loop the compiler vectorises); the first
+    // offending cell is looked for only when there is one
+    uint8_t maxId = 0;
+    for (long long c = 0; c < n; ++c) maxId = std::max(maxId, mat[c]);
+    const bool anyDiel = maxId >= TLM_MAT_DIEL0;
+    if (anyDiel && maxId - TLM_MAT_DIEL0 >= n_table)
+        for (long long c = 0; c < n; ++c)
+            if (mat[c] >= TLM_MAT_DIEL0 && mat[c] - TLM_MAT_DIEL0 >= n_table)
                 return h->fail(TLM_EINVAL, "material id " + std::to_string(mat[c]) + " at cell " +
                                                std::to_string(c) + " has no table entry");
-        }
-    }
     DeviceGuard dg(h->device);
     cudaStreamSynchronize(h->stream);
     freeAll(h);
@@ -1206,15 +1201,22 @@ tlm_status tlm_setup(tlm_handle h, const tlm_grid *grid, const uint8_t *mat, siz
         TLM_TRY(devAlloc(h, &h->dStub, 3 * (size_t)h->P * rb));
         TLM_CU(h, cudaMemsetAsync(h->dStub, 0, 3 * (size_t)h->P * rb, h->stream));
     }
-    // padded material map: padding columns are PEC (never updated, zero)
+    // padded material map: padding columns are PEC (never updated, zero);
+    // the caller's map goes up as it is and is padded on the device
     {
-        std::vector<uint8_t> pm((size_t)h->P, (uint8_t)TLM_MAT_PEC);
-        for (long long r = 0; r < (long long)h->ny * h->nz; ++r)
-            std::memcpy(&pm[(size_t)r * h->px], &mat[(size_t)r * h->nx], h->nx);
+        uint8_t *raw = nullptr;
         TLM_TRY(devAlloc(h, &h->dMat, (size_t)h->P));
-        TLM_CU(h, cudaMemcpyAsync(h->dMat, pm.data(), (size_t)h->P, cudaMemcpyHostToDevice,
-                                  h->stream));
-        TLM_CU(h, cudaStreamSynchronize(h->stream));
+        TLM_TRY(tmpAlloc(h, &raw, (size_t)n));
+        cudaError_t e = cudaMemcpyAsync(raw, mat, (size_t)n, cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess)
+        {
+            const long long rows = (long long)h->ny * h->nz;
+            tlmk::padMaterial<<<(int)std::min<long long>((h->P + 255) / 256, 148LL * 32), 256, 0, h->stream>>>(
+                raw, h->nx, h->px, rows, h->dMat);
+            e = cudaGetLastError();
+        }
+        cudaFreeAsync(raw, h->stream);
+        TLM_CU(h, e);
     }
     TLM_TRY(devAlloc(h, &h->dYhat, h->yhat32.size() * rb));
     TLM_TRY(devAlloc(h, &h->dGhat, h->ghat32.size() * rb));
@@ -1826,6 +1828,16 @@ tlm_status tlm_set_kernel_timing(tlm_handle h, int enable)
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->timing = enable != 0;
     h->evUsed = 0;
+    return TLM_OK;
+}
+
+tlm_status tlm_near_field_box(tlm_handle h, int box[6])
+{
+    TLM_TRY(checkHandle(h));
+    if (!box) return h->fail(TLM_EINVAL, "null output");
+    const tlmk::NearBox &b = h->nearBox;
+    const int v[6] = { b.x0, b.y0, b.z0, b.nx, b.ny, b.nz };
+    for (int t = 0; t < 6; ++t) box[t] = b.bP > 0 ? v[t] : 0;
     return TLM_OK;
 }
 

@@ -518,6 +518,12 @@ class TlmSolver:
     def setKernelTiming(self, on: bool):
         self._c(self._L.tlm_set_kernel_timing(self._h, 1 if on else 0))
 
+    def nearFieldBox(self):
+        """((i0, j0, k0), (ni, nj, nk)) of the near-field box, or None."""
+        b = (C.c_int * 6)()
+        self._c(self._L.tlm_near_field_box(self._h, b))
+        return None if b[3] == 0 else ((b[0], b[1], b[2]), (b[3], b[4], b[5]))
+
     def stepLaunches(self) -> int:
         """Kernels launched per step (not counting the window epilogue)."""
         n = C.c_int(0)

@@ -332,9 +332,10 @@ TLM_API tlm_status tlm_batch_launch_window(tlm_batch b, int *n_steps);
 TLM_API tlm_status tlm_batch_sync(tlm_batch b);
 TLM_API tlm_status tlm_batch_set_tuning(tlm_batch b, const tlm_batch_tuning *t);
 TLM_API tlm_status tlm_batch_get_tuning(tlm_batch b, tlm_batch_tuning *t);
-/* Time trial_windows windows of every tile shape (then of steps-per-launch
- * 16/32/64/128 for the best shape) on the batch's own members, keep the
- * fastest, and rewind every member to step 0 (fields zero). Call before the
+/* Time trial_windows windows of 100 steps of every tile shape (then
+ * windows of 50 and 200 steps for the best shape) on the batch's own
+ * members, keep the fastest, and rewind every member to step 0 (fields
+ * zero). Call before the
  * first step. Results are cached per (GPU, storage modes, size class), in
  * the file named by TLM_AUTOTUNE_CACHE when that variable is set. */
 TLM_API tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *out);
@@ -539,6 +540,11 @@ TLM_API tlm_status tlm_step_planes_noalloc(const float *in_planes, float *out_pl
 TLM_API int tlm_kernel_variants(int storage);
 TLM_API tlm_status tlm_kernel_variant_info(int storage, int variant, int *nodes_per_thread,
                                            int *min_blocks_per_sm);
+
+/* The near-field box (tlm_config.near_field) fixed when the grid was
+ * prepared: box[0..2] its first cell (i, j, k), box[3..5] its extent in
+ * cells; all zero when the handle has none (or is not prepared yet). */
+TLM_API tlm_status tlm_near_field_box(tlm_handle h, int box[6]);
 
 /* The handle's CUDA stream (cudaStream_t) for event timing by the caller. */
 TLM_API tlm_status tlm_get_stream(tlm_handle h, void **stream);

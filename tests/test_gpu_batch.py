@@ -109,7 +109,7 @@ def test_autotune_then_run(built):
         for s in solvers:
             b.attach(s)
         t = b.autotune(trial_windows=1)
-        assert t.ms_per_step > 0 and t.steps_per_launch in (16, 32, 64, 128)
+        assert t.ms_per_step > 0 and t.steps_per_launch in (50, 100, 200)
         for s in solvers:
             assert s.currentStep() == 0
         b.run()
