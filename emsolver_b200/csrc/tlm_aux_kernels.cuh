@@ -181,7 +181,7 @@ __global__ void incidentToAos(const S *__restrict__ refl, const uint8_t *__restr
             const int ax = s >> 2, side = (s >> 1) & 1;
             const int qn = co[ax] + (side ? 1 : -1);
             R own = loadOne<S>(refl, s * P + node, scale);
-            if (inBox) own += nb.lo_in[s * nb.bP + nb.at(i, j, k)];
+            if (inBox) own += nb.lo_in[s * nb.bP + nb.at(i, j, k)] * scale;  // residuals: storage units
             R v;
             if (qn < 0 || qn >= dims[ax])
                 v = rho * own;
@@ -198,7 +198,7 @@ __global__ void incidentToAos(const S *__restrict__ refl, const uint8_t *__restr
                         int c2[3] = { i, j, k };
                         c2[ax] = qn;
                         const long long b = nb.at(c2[0], c2[1], c2[2]);
-                        if (b >= 0) v += nb.lo_in[(s ^ 2) * nb.bP + b];
+                        if (b >= 0) v += nb.lo_in[(s ^ 2) * nb.bP + b] * scale;
                     }
                 }
             }
@@ -225,7 +225,7 @@ __global__ void planesToAos(const S *__restrict__ planes, long long P, int nx, i
         for (int s = 0; s < 12; ++s)
         {
             typename Traits<S>::R v = loadOne<S>(planes, s * P + node, scale);
-            if (b >= 0) v += nb.lo_in[s * nb.bP + b];
+            if (b >= 0) v += nb.lo_in[s * nb.bP + b] * scale;  // residuals: storage units
             out[c * 12 + s] = (O)v;
         }
     }
@@ -265,17 +265,21 @@ __global__ void aosToIncident(const I *__restrict__ in, const uint8_t *__restric
                     for (int c = 0; c < 4; ++c)
                     {
                         const long long b = nb.at(i0 + c, j, k);
-                        if (b >= 0)
-                            nb.lo_out[s * nb.bP + b] = v[c] - decode(encode<S>(v[c], inv_scale), R(1) / inv_scale);
+                        if (b >= 0)  // in storage units, like the step kernels' residuals
+                        {
+                            const R u = v[c] * inv_scale;
+                            nb.lo_out[s * nb.bP + b] = u - decodeRaw(encodeRaw<S>(u));
+                        }
                     }
             }
         }
     }
 }
 
+// Stub planes (storage units) -> AoS, times `scale`.
 template <class R, class O>
 __global__ void stubsToAos(const R *__restrict__ stub, long long P, int nx, int ny, int nz, int px,
-                           O *__restrict__ out)
+                           O *__restrict__ out, R scale)
 {
     const long long n = (long long)nx * ny * nz;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
@@ -285,7 +289,7 @@ __global__ void stubsToAos(const R *__restrict__ stub, long long P, int nx, int 
         const int j = (int)((c / nx) % ny);
         const int k = (int)(c / ((long long)nx * ny));
         const long long node = ((long long)k * ny + j) * px + i;
-        for (int s = 0; s < 3; ++s) out[c * 3 + s] = (O)stub[s * P + node];
+        for (int s = 0; s < 3; ++s) out[c * 3 + s] = (O)(stub[s * P + node] * scale);
     }
 }
 

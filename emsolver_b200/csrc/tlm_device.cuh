@@ -211,6 +211,24 @@ __device__ __forceinline__ float decode(__nv_bfloat16 s, float scale)
 {
     return __bfloat162float(s) * scale;
 }
+// Stored value <-> pulse in storage units (no per-grid scale): the step
+// kernels work in storage units, since the scale is a power of two and the
+// step is linear, which only differs from the scaled pulse by that exact
+// factor.
+__device__ __forceinline__ float decodeRaw(float s) { return s; }
+__device__ __forceinline__ double decodeRaw(double s) { return s; }
+__device__ __forceinline__ float decodeRaw(__half s) { return __half2float(s); }
+__device__ __forceinline__ float decodeRaw(__nv_bfloat16 s) { return __bfloat162float(s); }
+template <class S> __device__ __forceinline__ S encodeRaw(float v);
+template <> __device__ __forceinline__ float encodeRaw<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half encodeRaw<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 encodeRaw<__nv_bfloat16>(float v)
+{
+    return __float2bfloat16_rn(v);
+}
+template <class S> __device__ __forceinline__ S encodeRaw(double v);
+template <> __device__ __forceinline__ double encodeRaw<double>(double v) { return v; }
+
 template <class S> __device__ __forceinline__ S encode(float v, float inv);
 template <> __device__ __forceinline__ float encode<float>(float v, float) { return v; }
 template <> __device__ __forceinline__ __half encode<__half>(float v, float inv)

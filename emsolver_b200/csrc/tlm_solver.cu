@@ -264,9 +264,9 @@ template <class S> tlm_status stagedAttributes(tlm_solver *h)
 // FP32 with 2 nodes per thread (the default shape): interior tiles go to the
 // staged kernel, the others (PEC, sources, monitors, the partial last tile)
 // to the list kernel, both launched every step (tlm_config.no_staging = 1: the single
-// step kernel as before). The 16-bit storage types are bound by instruction
-// issue, not by load latency: staged, they measured slower than their own
-// default shape, so they keep the single kernel.
+// step kernel as before). The 16-bit storage types keep the single step
+// kernel: staged, or with their interior tiles in a kernel of their own
+// beside the list kernel, they measured slower.
 tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
 {
     h->nStaged = h->nListed = 0;
@@ -536,7 +536,7 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
     a.spec = h->dSpec;
     a.tile_flags = h->dTileFlags;
     a.neg_zero = -0.0f;
-    a.sv = (R)sourceValue(h, n);
+    a.sv = (R)sourceValue(h, n) * (R)(1.0f / h->scale);  // in storage units
     a.samples = static_cast<R *>(h->dSamples) + (size_t)i * h->nsamp * 6;
     a.epart = (n % 16 == 0) ? h->dEpart + (size_t)((n - eFirst) / 16) * h->nblocks : nullptr;
     const long long planeNodes = (long long)h->ny * h->px;
@@ -744,7 +744,9 @@ tlm_status uploadSourceTable(tlm_solver *h, long long steps)
     else
     {
         std::vector<float> v32(v64.size());
-        for (size_t t = 0; t < v64.size(); ++t) v32[t] = (float)v64[t];
+        // in storage units (the step kernels' sv)
+        const float inv = 1.0f / h->scale;
+        for (size_t t = 0; t < v64.size(); ++t) v32[t] = (float)v64[t] * inv;
         TLM_CU(h, cudaMemcpyAsync(h->dSv, v32.data(), v32.size() * 4, cudaMemcpyHostToDevice, h->stream));
         TLM_CU(h, cudaStreamSynchronize(h->stream));
     }
@@ -1705,10 +1707,10 @@ tlm_status tlm_get_stubs(tlm_handle h, float *out, size_t cap)
     TLM_TRY(tmpAlloc(h, &d, need * sizeof(float)));
     if (h->storage == TLM_STORE_F64)
         tlmk::stubsToAos<double, float><<<gridBlocksFor(h->ncell), 256, 0, h->stream>>>(
-            static_cast<const double *>(h->dStub), h->P, h->nx, h->ny, h->nz, h->px, d);
+            static_cast<const double *>(h->dStub), h->P, h->nx, h->ny, h->nz, h->px, d, 1.0);
     else
         tlmk::stubsToAos<float, float><<<gridBlocksFor(h->ncell), 256, 0, h->stream>>>(
-            static_cast<const float *>(h->dStub), h->P, h->nx, h->ny, h->nz, h->px, d);
+            static_cast<const float *>(h->dStub), h->P, h->nx, h->ny, h->nz, h->px, d, h->scale);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, need * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);

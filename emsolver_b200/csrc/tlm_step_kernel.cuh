@@ -37,7 +37,9 @@ template <class S> struct StepArgs
     int nx, ny, nz, px, nq;        // nq = px / V
     FastDiv div_nq, div_ny;        // division by nq and by ny (nquads < 2^31)
     R rho;
-    R scale, inv_scale;            // pulse = stored * scale (BF16/F16)
+    R scale, inv_scale;            // pulse = stored * scale (BF16/F16); the step works in
+                                   // storage units: sv, stubs and residuals are in those
+                                   // units, samples and energy partials are scaled back
     // sources and monitors
     const int *__restrict__ tile_begin;  // [gridDim.x + 1] ranges into spec
     const SpecEntry *__restrict__ spec;
@@ -75,7 +77,8 @@ enum : uint8_t { kTileGeneral = 1, kTileDiel = 2, kTileEdge = 4, kTileNear = 8 }
 // Plane access by node index, for every storage type. Element storage
 // (float, double, half, bfloat16) is read and written as aligned vectors of
 // V nodes; block floating point (Bfp4) as one word per aligned 4-node group.
-template <class S, int V>
+// kUnit: the value in storage units (decodeRaw), else scaled by `scale`.
+template <class S, int V, bool kUnit = false>
 __device__ __forceinline__ void loadVec(const S *__restrict__ base, long long node,
                                         typename Traits<S>::R (&dst)[V], typename Traits<S>::R scale)
 {
@@ -91,28 +94,37 @@ __device__ __forceinline__ void loadVec(const S *__restrict__ base, long long no
     {
         const Pack<S, V> p = *reinterpret_cast<const Pack<S, V> *>(base + node);
 #pragma unroll
-        for (int c = 0; c < V; ++c) dst[c] = decode(p.v[c], scale);
+        for (int c = 0; c < V; ++c)
+        {
+            if constexpr (kUnit)
+                dst[c] = decodeRaw(p.v[c]);
+            else
+                dst[c] = decode(p.v[c], scale);
+        }
     }
 }
 
-template <class S>
+template <class S, bool kUnit = false>
 __device__ __forceinline__ typename Traits<S>::R loadOne(const S *__restrict__ base, long long node,
                                                          typename Traits<S>::R scale)
 {
     if constexpr (std::is_same<S, Bfp4>::value)
         return bfpDecodeOne(base[node >> 2], (int)(node & 3));
+    else if constexpr (kUnit)
+        return decodeRaw(base[node]);
     else
         return decode(base[node], scale);
 }
 
 // Store V nodes of plane slot `salt`; with stochastic rounding the random
 // bits are a function of (node, slot, step seed).
-template <class S, int V>
+template <class S, int V, bool kUnit = false>
 __device__ __forceinline__ void storeVec(S *__restrict__ base, long long node,
                                          const typename Traits<S>::R (&src)[V],
                                          typename Traits<S>::R inv, bool stochastic, unsigned seed,
                                          int salt)
 {
+    if constexpr (kUnit) inv = typename Traits<S>::R(1);
     if constexpr (std::is_same<S, Bfp4>::value)
     {
         static_assert(V == 4, "block floating point groups hold 4 nodes");
@@ -135,17 +147,23 @@ __device__ __forceinline__ void storeVec(S *__restrict__ base, long long node,
 #pragma unroll
             for (int c = 0; c < V; c += 2)
             {
+                const float lo = kUnit ? src[c] : src[c] * inv, hi = kUnit ? src[c + 1] : src[c + 1] * inv;
                 if constexpr (std::is_same<S, __half>::value)
-                    *reinterpret_cast<__half2 *>(&p.v[c]) = __floats2half2_rn(src[c] * inv, src[c + 1] * inv);
+                    *reinterpret_cast<__half2 *>(&p.v[c]) = __floats2half2_rn(lo, hi);
                 else
-                    *reinterpret_cast<__nv_bfloat162 *>(&p.v[c]) =
-                        __floats2bfloat162_rn(src[c] * inv, src[c + 1] * inv);
+                    *reinterpret_cast<__nv_bfloat162 *>(&p.v[c]) = __floats2bfloat162_rn(lo, hi);
             }
         }
         else
         {
 #pragma unroll
-            for (int c = 0; c < V; ++c) p.v[c] = encode<S>(src[c], inv);
+            for (int c = 0; c < V; ++c)
+            {
+                if constexpr (kUnit)
+                    p.v[c] = encodeRaw<S>(src[c]);
+                else
+                    p.v[c] = encode<S>(src[c], inv);
+            }
         }
         *reinterpret_cast<Pack<S, V> *>(base + node) = p;
     }
@@ -283,30 +301,30 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
         const S *YZ = reinterpret_cast<const S *>(sm + L::kOffYZ);
         const int l = threadIdx.x * V;
 #pragma unroll
-        for (int s = 0; s < 4; ++s) loadVec<S, V>(X + s * L::kSegX + L::kHalo, l, ox[s], a.scale);
+        for (int s = 0; s < 4; ++s) loadVec<S, V, true>(X + s * L::kSegX + L::kHalo, l, ox[s], a.scale);
 #pragma unroll
-        for (int g = 0; g < 8; ++g) loadVec<S, V>(YZ + g * kStageNodes, l, inc[4 + g], a.scale);
+        for (int g = 0; g < 8; ++g) loadVec<S, V, true>(YZ + g * kStageNodes, l, inc[4 + g], a.scale);
 #pragma unroll
         for (int t = 0; t < 2; ++t)
         {
-            prevX[t] = loadOne<S>(X + (2 + t) * L::kSegX + L::kHalo, l - 1, a.scale);
-            nextX[t] = loadOne<S>(X + t * L::kSegX + L::kHalo, l + V, a.scale);
+            prevX[t] = loadOne<S, true>(X + (2 + t) * L::kSegX + L::kHalo, l - 1, a.scale);
+            nextX[t] = loadOne<S, true>(X + t * L::kSegX + L::kHalo, l + V, a.scale);
         }
         (void)lane;
     }
     else
     {
 #pragma unroll
-        for (int s = 0; s < 4; ++s) loadVec<S, V>(a.in, s * P + node0, ox[s], a.scale);
+        for (int s = 0; s < 4; ++s) loadVec<S, V, true>(a.in, s * P + node0, ox[s], a.scale);
 #pragma unroll
         for (int t = 0; t < 2; ++t)
         {
             // -y face: (y,+) of the row below; +y face: (y,-) of the row above;
             // on an outer face the own pulse of the face instead
-            loadVec<S, V>(a.in, atYlo ? (4 + t) * P + node0 : (6 + t) * P + node0 - sy, inc[4 + t], a.scale);
-            loadVec<S, V>(a.in, atYhi ? (6 + t) * P + node0 : (4 + t) * P + node0 + sy, inc[6 + t], a.scale);
-            loadVec<S, V>(a.in, atZlo ? (8 + t) * P + node0 : (10 + t) * P + node0 - sz, inc[8 + t], a.scale);
-            loadVec<S, V>(a.in, atZhi ? (10 + t) * P + node0 : (8 + t) * P + node0 + sz, inc[10 + t], a.scale);
+            loadVec<S, V, true>(a.in, atYlo ? (4 + t) * P + node0 : (6 + t) * P + node0 - sy, inc[4 + t], a.scale);
+            loadVec<S, V, true>(a.in, atYhi ? (6 + t) * P + node0 : (4 + t) * P + node0 + sy, inc[6 + t], a.scale);
+            loadVec<S, V, true>(a.in, atZlo ? (8 + t) * P + node0 : (10 + t) * P + node0 - sz, inc[8 + t], a.scale);
+            loadVec<S, V, true>(a.in, atZhi ? (10 + t) * P + node0 : (8 + t) * P + node0 + sz, inc[10 + t], a.scale);
         }
         // ---- x neighbours: own vector, adjacent lane, or (warp edge) a scalar load ----
 #pragma unroll
@@ -318,12 +336,12 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
         if (lane == 0 && x0 > 0)
         {
 #pragma unroll
-            for (int t = 0; t < 2; ++t) prevX[t] = loadOne<S>(a.in, (2 + t) * P + node0 - 1, a.scale);
+            for (int t = 0; t < 2; ++t) prevX[t] = loadOne<S, true>(a.in, (2 + t) * P + node0 - 1, a.scale);
         }
         if (lane == 31 && x0 + V <= a.nx - 1)
         {
 #pragma unroll
-            for (int t = 0; t < 2; ++t) nextX[t] = loadOne<S>(a.in, t * P + node0 + V, a.scale);
+            for (int t = 0; t < 2; ++t) nextX[t] = loadOne<S, true>(a.in, t * P + node0 + V, a.scale);
         }
     }
 #pragma unroll
@@ -401,7 +419,7 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
                 {
                     double tot = 0.0;
                     for (int w = 0; w < kBlock / 32; ++w) tot += red[w];
-                    a.epart[tile] = tot;
+                    a.epart[tile] = tot * ((double)a.scale * (double)a.scale);
                 }
                 else if (a.fault)
                     atomicOr(a.fault, kStageTimeout);
@@ -410,7 +428,7 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
         else
         {
             const double tot = blockSumDouble(e, red);
-            if (threadIdx.x == 0) a.epart[tile] = tot;
+            if (threadIdx.x == 0) a.epart[tile] = tot * ((double)a.scale * (double)a.scale);
         }
     }
 
@@ -533,7 +551,7 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     }
 #pragma unroll
     for (int s = 0; s < 12; ++s)
-        storeVec<S, V>(a.out, s * P + node0, outv[s], a.inv_scale, a.stochastic != 0, a.round_seed, s);
+        storeVec<S, V, true>(a.out, s * P + node0, outv[s], a.inv_scale, a.stochastic != 0, a.round_seed, s);
     if (dielMask)
     {
 #pragma unroll
@@ -637,7 +655,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
         for (int s = 0; s < 12; ++s)
         {
             if (live && TLM_GUARD(s * P + node0, 12 * P - V + 1, 2))
-                loadVec<S, V>(a.in, s * P + node0, inc[s], a.scale);
+                loadVec<S, V, true>(a.in, s * P + node0, inc[s], a.scale);
             else
             {
 #pragma unroll
@@ -691,7 +709,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
         for (int s = 0; s < 4; ++s)
         {
             if (live && TLM_GUARD(s * P + node0, 12 * P - V + 1, 5))
-                loadVec<S, V>(a.in, s * P + node0, ox[s], a.scale);
+                loadVec<S, V, true>(a.in, s * P + node0, ox[s], a.scale);
             else
             {
 #pragma unroll
@@ -712,7 +730,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
             for (int t = 0; t < 2; ++t)
                 if (TLM_GUARD((2 + t) * P + node0 - 1, 12 * P, 6))
                 {
-                    prevX[t] = loadOne<S>(a.in, (2 + t) * P + node0 - 1, a.scale);
+                    prevX[t] = loadOne<S, true>(a.in, (2 + t) * P + node0 - 1, a.scale);
                     addLo1(prevX[t], 2 + t, x0 - 1, j, k);
                 }
         }
@@ -722,7 +740,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
             for (int t = 0; t < 2; ++t)
                 if (TLM_GUARD(t * P + node0 + V, 12 * P, 6))
                 {
-                    nextX[t] = loadOne<S>(a.in, t * P + node0 + V, a.scale);
+                    nextX[t] = loadOne<S, true>(a.in, t * P + node0 + V, a.scale);
                     addLo1(nextX[t], t, x0 + V, j, k);
                 }
         }
@@ -768,7 +786,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                 {
                     const long long idx = atLo ? sLo * P + node0 : sHi * P + node0 - st;
                     if (live && TLM_GUARD(idx, 12 * P - V + 1, 7))
-                        loadVec<S, V>(a.in, idx, vLo, a.scale);
+                        loadVec<S, V, true>(a.in, idx, vLo, a.scale);
                     else
                     {
 #pragma unroll
@@ -787,7 +805,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                     {
                         R own[V];
                         if (TLM_GUARD(sLo * P + node0, 12 * P - V + 1, 8))
-                            loadVec<S, V>(a.in, sLo * P + node0, own, a.scale);
+                            loadVec<S, V, true>(a.in, sLo * P + node0, own, a.scale);
                         addLo(own, sLo, j, k);
 #pragma unroll
                         for (int c = 0; c < V; ++c)
@@ -798,7 +816,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                 {
                     const long long idx = atHi ? sHi * P + node0 : sLo * P + node0 + st;
                     if (live && TLM_GUARD(idx, 12 * P - V + 1, 9))
-                        loadVec<S, V>(a.in, idx, vHi, a.scale);
+                        loadVec<S, V, true>(a.in, idx, vHi, a.scale);
                     else
                     {
 #pragma unroll
@@ -817,7 +835,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                     {
                         R own[V];
                         if (TLM_GUARD(sHi * P + node0, 12 * P - V + 1, 10))
-                            loadVec<S, V>(a.in, sHi * P + node0, own, a.scale);
+                            loadVec<S, V, true>(a.in, sHi * P + node0, own, a.scale);
                         addLo(own, sHi, j, k);
 #pragma unroll
                         for (int c = 0; c < V; ++c)
@@ -885,9 +903,9 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
                     }
                     R *dst = a.samples + (long long)se.arg * 6;
 #pragma unroll
-                    for (int jj = 0; jj < 3; ++jj) dst[jj] = nodeVoltage(v, jj);
+                    for (int jj = 0; jj < 3; ++jj) dst[jj] = nodeVoltage(v, jj) * a.scale;
 #pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) dst[3 + kk] = circulation(v, kk);
+                    for (int kk = 0; kk < 3; ++kk) dst[3 + kk] = circulation(v, kk) * a.scale;
                 }
             }
         }
@@ -907,7 +925,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
             }
         }
         const double tot = blockSumDouble(e, red);
-        if (threadIdx.x == 0) a.epart[tile] = tot;
+        if (threadIdx.x == 0) a.epart[tile] = tot * ((double)a.scale * (double)a.scale);
     }
 
     // ---- scatter and store ----
@@ -984,7 +1002,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
             if (TLM_GUARD(s * P + node0, 12 * P - V + 1, 12))
             {
                 // box nodes round to nearest: their residual completes that value
-                storeVec<S, V>(a.out, s * P + node0, outv[s], a.inv_scale, a.stochastic != 0 && !near,
+                storeVec<S, V, true>(a.out, s * P + node0, outv[s], a.inv_scale, a.stochastic != 0 && !near,
                                a.round_seed, s);
             }
         }
@@ -1000,7 +1018,7 @@ __device__ __forceinline__ void stepTile(const StepArgs<S> &a, int tile, double 
 #pragma unroll
                     for (int s = 0; s < 12; ++s)
                         a.near.lo_out[s * a.near.bP + b] =
-                            outv[s][c] - decode(encode<S>(outv[s][c], a.inv_scale), a.scale);
+                            outv[s][c] - decodeRaw(encodeRaw<S>(outv[s][c]));
                 }
             }
         }
