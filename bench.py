@@ -56,6 +56,14 @@ def parse():
                    help="16-bit storage: radius of the FP32-residual box around PEC and ports "
                         "(default 6 for f16/bf16)")
     p.add_argument("--precision-steps", type=int, default=8000, help="precision: steps per mode")
+    p.add_argument("--order", default="least-work", choices=["least-work", "arrival"],
+                   help="served: admission order")
+    p.add_argument("--max-running-cells", type=int, default=32 << 20,
+                   help="served: cap on the running requests' padded cells (0: none)")
+    p.add_argument("--solo-cells", type=int, default=4 << 20,
+                   help="served: requests this large run on their own beside the batch (0: never)")
+    p.add_argument("--served-16bit", default="f16nf", choices=["f16nf", "bf16"],
+                   help="served: storage of the stream's 16-bit half")
     p.add_argument("--energy-steps", type=int, default=3000, help="energy: steps per mode")
     p.add_argument("--chunk", type=int, default=32, help="batched: instances set up per window")
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64", "bfp16"])
@@ -695,13 +703,17 @@ def run_batched(args):
 
 
 def run_served(args):
-    """Poisson arrivals of dipole solves (edge log-uniform, steps uniform,
-    FP32 or BF16 storage with probability 0.5), scaled by --edge-max and
-    --steps-max; latency percentiles beside solves/s, against the same
-    stream served one solve at a time by the plain API."""
+    """Poisson arrivals of dipole solves (cubic edge log-uniform, steps
+    uniform, FP32 or 16-bit storage with probability 0.5), scaled by
+    --edge-max and --steps-max; latency percentiles beside solves/s, against
+    the same stream served one solve at a time by the plain API (a FIFO
+    replay of each request's measured plain solve time). The stream's 16-bit
+    half is stored as FP16 with the near-field box (--served-16bit f16nf,
+    the default: BF16 misses the 1e-3 S11 bar even with the box) or as BF16
+    (--served-16bit bf16). Every request's S11 is checked against an FP64
+    storage run of the same solve."""
     import threading
     from emsolver_b200 import Server, workloads
-    from emsolver_b200.runner import build_solver
     from emsolver_b200.solver import s11_from_dft
     stream = workloads.request_stream(count=args.requests, rate=args.rate, edge_hi=args.edge_max,
                                       steps_hi=args.steps_max)
@@ -709,6 +721,11 @@ def run_served(args):
     ws = [w for _, w in stream]
     for w in ws:
         w.dft_freqs = w.dft_freqs[:16]
+        if w.storage == 1:                        # the stream's 16-bit half
+            if args.served_16bit == "f16nf":
+                w.storage, w.meta["near_field"] = 2, 6
+            else:
+                w.meta["near_field"] = 0
     sequential_solves([ws[0]])
     seq = sequential_solves(ws)
     # plain FIFO single-solve server on the same arrival stream
@@ -719,6 +736,8 @@ def run_served(args):
         plain_lat.append(done - a)
     plain_span = done - arrivals[0]
     srv = Server(steps_per_launch=64)
+    srv.set_policy(Server.ARRIVAL if args.order == "arrival" else Server.LEAST_WORK, args.max_running_cells,
+                   args.solo_cells)
     ids = [None] * len(ws)
     t0 = time.perf_counter()
 
@@ -735,33 +754,33 @@ def run_served(args):
     for rid in ids:
         srv.wait(rid, -1.0)
     t1 = time.perf_counter()
-    lat = []
+    lat, got = [], []
     for rid in ids:
-        lat.append(srv.result(rid)[2])
+        v, i, l = srv.result(rid)
+        lat.append(l)
+        got.append((v, i))
     st = srv.stats()
-    # S11 of sampled requests against the FP64 storage mode
-    errs = {}
-    for k in range(min(4, len(ws))):
-        w = ws[k]
-        v, i, _ = srv.result(ids[k])
-        r = build_solver(w, storage=3)
-        r.step(w.steps)
-        rv, ri = r.portDft(0)
-        r.close()
-        s_srv, s_ref = s11_from_dft(v, i)[1], s11_from_dft(rv, ri)[1]
-        errs[f"{w.name}_{'bf16' if w.storage == 1 else 'f32'}"] = float(
-            np.max(np.abs(s_srv - s_ref) / np.abs(s_ref)))
     srv.close()
     span = t1 - t0
+    # every request's S11 against the FP64 storage mode (one FP64 batch)
+    ref = batch_dfts(ws, 3, 0)
+    errs = {"f32": [], "16-bit": []}
+    for w, (v, i), (rv, ri) in zip(ws, got, ref):
+        a, r = s11_from_dft(v, i)[1], s11_from_dft(rv, ri)[1]
+        errs["f32" if w.storage == 0 else "16-bit"].append(float(np.max(np.abs(a - r) / np.abs(r))))
     work = sum(w.ncells * w.steps for w in ws)
     line = {
         "metric": "served solves/s", "value": len(ws) / span, "unit": "solves/s", "n_gpus": 1,
         "steps": len(ws), "warmup": 1, "ms_per_step": 1000.0 * span / len(ws),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 or bf16 storage per request", "data": "synthetic (seeded Poisson stream)",
+        "dtype": "f32 or 16-bit storage per request (" +
+                 ("FP16 + near-field box r=6" if args.served_16bit == "f16nf" else "BF16") + ")",
+        "data": "synthetic (seeded Poisson stream)",
         "config": {"workload": f"served: {len(ws)} requests, Poisson {args.rate}/s, cubic edge "
                                f"log-U[32,{args.edge_max}], steps U[500,{args.steps_max}]",
-                   "node_updates": work},
+                   "node_updates": work, "order": args.order, "max_running_cells": args.max_running_cells,
+                   "solo_cells": args.solo_cells,
+                   "served_16bit": args.served_16bit},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "mean": float(np.mean(lat))},
         "plain_sequential": {"solves_per_s": len(ws) / plain_span,
@@ -770,7 +789,9 @@ def run_served(args):
                              "busy_s": sum(seq)},
         "speedup_vs_plain": plain_span / span,
         "node_updates_per_s": work / span,
-        "s11_rel_err_vs_fp64": errs,
+        "s11_rel_err_vs_fp64": {k: {"max": max(v), "median": float(np.median(v)), "requests": len(v),
+                                    "within_1e-3": int(sum(e <= 1e-3 for e in v))}
+                                for k, v in errs.items() if v},
         "server": st,
     }
     print(json.dumps(line), flush=True)

@@ -124,7 +124,8 @@ class ServerStatsC(C.Structure):
                 ("latency_p50_s", C.c_double), ("latency_p99_s", C.c_double),
                 ("latency_mean_s", C.c_double), ("solves_per_s", C.c_double),
                 ("hbm_used_bytes", C.c_size_t), ("hbm_budget_bytes", C.c_size_t),
-                ("windows", C.c_longlong), ("busy_s", C.c_double)]
+                ("windows", C.c_longlong), ("busy_s", C.c_double), ("gpu_window_s", C.c_double),
+                ("setup_s", C.c_double), ("retire_s", C.c_double), ("mean_running_cells", C.c_double)]
 
 
 _h = C.c_void_p
@@ -252,6 +253,7 @@ SIGNATURES = {
     "tlm_batch_autotune": (_st, [_h, C.c_int, _P(BatchTuningC)]),
     "tlm_batch_get_stream": (_st, [_h, _P(C.c_void_p)]),
     "tlm_server_create": (_st, [_P(_h), C.c_int, C.c_size_t, C.c_int]),
+    "tlm_server_set_policy": (_st, [C.c_void_p, C.c_int, C.c_longlong, C.c_longlong]),
     "tlm_server_destroy": (_st, [_h]),
     "tlm_server_submit": (_st, [_h, _P(RequestC), _P(C.c_uint64)]),
     "tlm_server_poll": (_st, [_h, C.c_uint64, _P(C.c_int)]),

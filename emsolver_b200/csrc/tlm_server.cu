@@ -3,8 +3,10 @@
 //
 // Callers submit complete solve requests (grid, materials, sources, probes,
 // DFT frequencies). A worker thread owns one batch: between launch windows
-// it admits queued requests in arrival order while their HBM footprint fits
-// the budget (state stays resident on the device until the request ends),
+// it admits queued requests -- the least work (cells x steps) first, or in
+// arrival order -- while their HBM footprint fits the budget and the running
+// cells stay within a target that keeps the GPU busy (state stays resident
+// on the device until the request ends),
 // attaches them to the running batch, advances every running request one
 // window, and retires the requests that reached their total_steps: their
 // port DFTs and records are copied out, the handle is freed and waiters are
@@ -50,6 +52,9 @@ struct Request
     std::vector<int> probes;  // i j k per probe
     std::vector<double> freqs;
     size_t footprint = 0;
+    long long nodes = 0;      // padded cells of the grid
+    double work = 0.0;        // nodes x total_steps
+    bool solo = false;        // stepped on its own stream by the single-grid kernels, not in the batch
     // progress
     int state = TLM_REQ_QUEUED;
     std::string error;
@@ -71,6 +76,9 @@ struct tlm_server_s
     size_t used = 0;
     int maxRunning = 1024;
     int window = 64;
+    int order = TLM_SERVE_LEAST_WORK;   // admission order (tlm_server_set_policy)
+    long long maxNodes = 32LL << 20;    // running cells cap (0: none)
+    long long soloNodes = 4LL << 20;    // requests this large run alone beside the batch (0: never)
     tlm_batch batch = nullptr;
     std::mutex m;
     std::condition_variable cvWork, cvDone;
@@ -86,6 +94,8 @@ struct tlm_server_s
     long long completed = 0, failed = 0, cancelledCount = 0;
     long long windows = 0;
     double busySeconds = 0.0;
+    double gpuWindowSeconds = 0.0, setupSeconds = 0.0, retireSeconds = 0.0, cellWindows = 0.0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string fatal;
 };
 
@@ -117,6 +127,33 @@ size_t footprintOf(const tlm_grid &g, const std::vector<uint8_t> &mat, const tlm
     const size_t steps = (size_t)std::max(cfg.total_steps, 1);
     return 2 * 12 * P * sb + (diel ? 3 * P * rb : 0) + P + steps * (nports * 2 + nprobes * 3 + 1) * 8 +
            nports * nfreq * 32 + steps * rb + (1u << 20);
+}
+
+// Cells of the near-field box a request will get (tlm_config.near_field):
+// the bounding box of its PEC cells and port cells grown by the radius.
+size_t nearCellsOf(const tlm_grid &g, const std::vector<uint8_t> &mat, const tlm_config &cfg,
+                   const std::vector<PortSpec> &ports)
+{
+    if (cfg.near_field <= 0 || (cfg.storage != TLM_STORE_F16 && cfg.storage != TLM_STORE_BF16)) return 0;
+    long long lo[3] = { g.nx, g.ny, g.nz }, hi[3] = { -1, -1, -1 };
+    auto take = [&](long long c) {
+        const long long v[3] = { c % g.nx, c / g.nx % g.ny, c / ((long long)g.nx * g.ny) };
+        for (int a = 0; a < 3; ++a)
+        {
+            lo[a] = std::min(lo[a], v[a]);
+            hi[a] = std::max(hi[a], v[a]);
+        }
+    };
+    for (size_t c = 0; c < mat.size(); ++c)
+        if (mat[c] == TLM_MAT_PEC) take((long long)c);
+    for (const PortSpec &p : ports)
+        for (uint64_t c : p.cells) take((long long)c);
+    if (hi[0] < 0) return 0;
+    const long long n[3] = { g.nx, g.ny, g.nz };
+    size_t cells = 1;
+    for (int a = 0; a < 3; ++a)
+        cells *= (size_t)(std::min(hi[a] + cfg.near_field, n[a] - 1) - std::max(lo[a] - cfg.near_field, 0LL) + 1);
+    return cells;
 }
 
 // Create and populate the handle of a request (worker thread; may run while
@@ -161,7 +198,7 @@ tlm_status startRequest(tlm_server_s *s, Request &r)
 // Copy the results out of a finished request's handle and free it.
 void finishRequest(tlm_server_s *s, Request &r)
 {
-    tlm_batch_detach(s->batch, r.h);
+    if (!r.solo) tlm_batch_detach(s->batch, r.h);
     r.steps = tlm_current_step(r.h);
     const int np = tlm_port_count(r.h);
     const int nf = (int)r.freqs.size();
@@ -213,7 +250,7 @@ void retire(tlm_server_s *s, std::unique_lock<std::mutex> &lk)
             finishRequest(s, *r);
         else
         {
-            tlm_batch_detach(s->batch, r->h);
+            if (!r->solo) tlm_batch_detach(s->batch, r->h);
             tlm_destroy(r->h);
             r->h = nullptr;
         }
@@ -242,17 +279,29 @@ void workerMain(tlm_server_s *s)
     {
         std::vector<std::shared_ptr<Request>> picked;
         size_t planned = s->used;
+        long long plannedNodes = 0;
+        for (const auto &r : s->running) plannedNodes += r->nodes;
         while (!s->stop && !s->queue.empty() &&
                (int)(s->running.size() + picked.size()) < s->maxRunning)
         {
-            std::shared_ptr<Request> r = s->queue.front();
+            // the next candidate: the least work, or the oldest request
+            auto it = s->queue.begin();
+            if (s->order == TLM_SERVE_LEAST_WORK)
+                it = std::min_element(s->queue.begin(), s->queue.end(),
+                                      [](const std::shared_ptr<Request> &a, const std::shared_ptr<Request> &b) {
+                                          return a->work < b->work || (a->work == b->work && a->id < b->id);
+                                      });
+            std::shared_ptr<Request> r = *it;
             if (r->state == TLM_REQ_CANCELLED)
             {
-                s->queue.pop_front();
+                s->queue.erase(it);
                 continue;
             }
-            if (planned + r->footprint > s->budget && !(s->running.empty() && picked.empty())) break;
-            s->queue.pop_front();
+            const bool first = s->running.empty() && picked.empty();
+            if (planned + r->footprint > s->budget && !first) break;
+            if (s->maxNodes > 0 && plannedNodes + r->nodes > s->maxNodes && !first) break;
+            s->queue.erase(it);
+            plannedNodes += r->nodes;
             r->state = TLM_REQ_RUNNING;
             r->started = Clock::now();
             planned += r->footprint;
@@ -273,20 +322,56 @@ void workerMain(tlm_server_s *s)
             s->cvWork.wait(lk, [&] { return s->stop || !s->queue.empty(); });
             continue;
         }
-        const bool haveRunning = !s->running.empty();
+        std::vector<tlm_handle> solos;
+        bool haveBatch = false;
+        long long runningCells = 0;
+        for (const auto &r : s->running)
+        {
+            runningCells += r->nodes;
+            if (r->solo)
+                solos.push_back(r->h);
+            else
+                haveBatch = true;
+        }
+        const bool haveRunning = haveBatch;
+        const int soloWindow = s->window;
         lk.unlock();
         const Clock::time_point w0 = Clock::now();
         int launched = 0;
         tlm_status st = TLM_OK;
+        void *bs = nullptr;
+        tlm_batch_get_stream(s->batch, &bs);
+        if (haveRunning && s->ev0) cudaEventRecord(s->ev0, static_cast<cudaStream_t>(bs));
         if (haveRunning) st = tlm_batch_launch_window(s->batch, &launched);
+        if (haveRunning && s->ev1) cudaEventRecord(s->ev1, static_cast<cudaStream_t>(bs));
+        // large requests: one window each on their own stream, beside the batch
+        for (tlm_handle h : solos)
+        {
+            const int left = tlm_total_steps(h) - tlm_current_step(h);
+            if (st == TLM_OK && left > 0) st = tlm_step_async(h, std::min(left, soloWindow));
+            if (left > 0) launched = std::max(launched, 1);
+        }
+        const Clock::time_point p0 = Clock::now();
         std::vector<tlm_status> prep(picked.size(), TLM_OK);
         for (size_t k = 0; k < picked.size(); ++k) prep[k] = startRequest(s, *picked[k]);
-        if (st == TLM_OK && launched) st = tlm_batch_sync(s->batch);
+        const double setupDt = std::chrono::duration<double>(Clock::now() - p0).count();
+        if (st == TLM_OK && haveRunning) st = tlm_batch_sync(s->batch);
+        for (tlm_handle h : solos)
+            if (st == TLM_OK) st = tlm_sync(h);
         const double dt = std::chrono::duration<double>(Clock::now() - w0).count();
+        float gpuMs = 0.0f;
+        if (launched && s->ev0 && cudaEventElapsedTime(&gpuMs, s->ev0, s->ev1) != cudaSuccess)
+        {
+            cudaGetLastError();
+            gpuMs = 0.0f;
+        }
         lk.lock();
+        s->setupSeconds += setupDt;
         if (launched)
         {
             s->busySeconds += dt;
+            s->gpuWindowSeconds += gpuMs * 1e-3;
+            s->cellWindows += (double)runningCells;
             ++s->windows;
         }
         if (st != TLM_OK)
@@ -297,7 +382,7 @@ void workerMain(tlm_server_s *s)
                 r->state = TLM_REQ_FAILED;
                 r->error = s->fatal;
                 r->finished = Clock::now();
-                tlm_batch_detach(s->batch, r->h);
+                if (!r->solo) tlm_batch_detach(s->batch, r->h);
                 tlm_destroy(r->h);
                 r->h = nullptr;
                 ++s->failed;
@@ -306,7 +391,11 @@ void workerMain(tlm_server_s *s)
             s->running.clear();
         }
         else
+        {
+            const Clock::time_point r0 = Clock::now();
             retire(s, lk);
+            s->retireSeconds += std::chrono::duration<double>(Clock::now() - r0).count();
+        }
         // attach the requests set up during this window
         for (size_t k = 0; k < picked.size(); ++k)
         {
@@ -320,7 +409,8 @@ void workerMain(tlm_server_s *s)
                 r.finished = Clock::now();
                 continue;
             }
-            if (ps == TLM_OK && (ps = tlm_batch_attach(s->batch, r.h)) != TLM_OK)
+            r.solo = s->soloNodes > 0 && r.nodes >= s->soloNodes;
+            if (ps == TLM_OK && !r.solo && (ps = tlm_batch_attach(s->batch, r.h)) != TLM_OK)
             {
                 r.error = tlm_last_error(nullptr);
                 tlm_destroy(r.h);
@@ -351,7 +441,7 @@ void workerMain(tlm_server_s *s)
     // shutdown: cancel what is left
     for (auto &r : s->running)
     {
-        tlm_batch_detach(s->batch, r->h);
+        if (!r->solo) tlm_batch_detach(s->batch, r->h);
         tlm_destroy(r->h);
         r->h = nullptr;
         r->state = TLM_REQ_CANCELLED;
@@ -401,10 +491,35 @@ tlm_status tlm_server_create(tlm_server *out, int device, size_t hbm_budget_byte
         hbm_budget_bytes = freeB / 10 * 8;
     }
     s->budget = hbm_budget_bytes;
+    {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess)
+        {
+            cudaGetLastError();
+            s->ev0 = s->ev1 = nullptr;
+        }
+        cudaSetDevice(prev);
+    }
     s->t0 = Clock::now();
     s->lastDone = s->t0;
     s->worker = std::thread(workerMain, s);
     *out = s;
+    return TLM_OK;
+}
+
+tlm_status tlm_server_set_policy(tlm_server s, int order, long long max_running_cells, long long solo_cells)
+{
+    if (!s) return serverFail(TLM_EINVAL, "null server");
+    if (order != TLM_SERVE_ARRIVAL && order != TLM_SERVE_LEAST_WORK)
+        return serverFail(TLM_EINVAL, "order must be TLM_SERVE_ARRIVAL or TLM_SERVE_LEAST_WORK");
+    if (max_running_cells < 0 || solo_cells < 0)
+        return serverFail(TLM_EINVAL, "max_running_cells and solo_cells must be >= 0");
+    std::lock_guard<std::mutex> lk(s->m);
+    s->order = order;
+    s->maxNodes = max_running_cells;
+    s->soloNodes = solo_cells;
     return TLM_OK;
 }
 
@@ -418,6 +533,8 @@ tlm_status tlm_server_destroy(tlm_server s)
     s->cvWork.notify_all();
     if (s->worker.joinable()) s->worker.join();
     tlm_batch_destroy(s->batch);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
     delete s;
     return TLM_OK;
 }
@@ -451,7 +568,10 @@ tlm_status tlm_server_submit(tlm_server s, const tlm_request *q, uint64_t *id)
     if (q->n_probes) r->probes.assign(q->probe_ijk, q->probe_ijk + 3 * (size_t)q->n_probes);
     if (q->n_freq) r->freqs.assign(q->freqs, q->freqs + q->n_freq);
     r->footprint = footprintOf(r->grid, r->mat, r->cfg, r->ports.size(), (size_t)q->n_probes,
-                               r->freqs.size());
+                               r->freqs.size()) +
+                   2 * 12 * sizeof(float) * nearCellsOf(r->grid, r->mat, r->cfg, r->ports);
+    r->nodes = (long long)((r->grid.nx + 7) / 8 * 8) * r->grid.ny * r->grid.nz;
+    r->work = (double)r->nodes * (double)std::max(r->cfg.total_steps, 1);
     std::lock_guard<std::mutex> lk(s->m);
     if (s->stop) return serverFail(TLM_ESTATE, "the server is shutting down");
     if (r->footprint > s->budget)
@@ -592,6 +712,10 @@ tlm_status tlm_server_stats(tlm_server s, tlm_server_stats_t *out)
     out->hbm_budget_bytes = s->budget;
     out->windows = s->windows;
     out->busy_s = s->busySeconds;
+    out->gpu_window_s = s->gpuWindowSeconds;
+    out->setup_s = s->setupSeconds;
+    out->retire_s = s->retireSeconds;
+    out->mean_running_cells = s->windows ? s->cellWindows / (double)s->windows : 0.0;
     return TLM_OK;
 }
 
@@ -599,7 +723,17 @@ tlm_status tlm_request_footprint(const tlm_request *q, size_t *bytes)
 {
     if (!q || !bytes || !q->mat) return serverFail(TLM_EINVAL, "null argument");
     std::vector<uint8_t> m(q->mat, q->mat + q->n_cells);
-    *bytes = footprintOf(q->grid, m, q->cfg, (size_t)q->n_ports, (size_t)q->n_probes, (size_t)q->n_freq);
+    std::vector<PortSpec> ports;
+    size_t off = 0;
+    for (int p = 0; p < q->n_ports; ++p)
+    {
+        PortSpec ps;
+        ps.cells.assign(q->port_cells + off, q->port_cells + off + q->port_ncells[p]);
+        off += q->port_ncells[p];
+        ports.push_back(std::move(ps));
+    }
+    *bytes = footprintOf(q->grid, m, q->cfg, (size_t)q->n_ports, (size_t)q->n_probes, (size_t)q->n_freq) +
+             2 * 12 * sizeof(float) * nearCellsOf(q->grid, m, q->cfg, ports);
     return TLM_OK;
 }
 

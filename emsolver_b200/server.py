@@ -27,14 +27,15 @@ def _p(a, t):
 class _Request:
     """A tlm_request built from a Workload; keeps the arrays alive."""
 
-    def __init__(self, w, storage=None, rounding=0):
+    def __init__(self, w, storage=None, rounding=0, near_field=None):
         self.mat = np.ascontiguousarray(w.mat, dtype=np.uint8).reshape(-1)
         self.tab = (_lib.MatPropsC * max(len(w.table), 1))()
         for t, (e, g) in enumerate(w.table):
             self.tab[t].epsr, self.tab[t].sigma = e, g
         cfg = TlmConfig(f0=w.f0, waveform=w.waveform, totalSteps=w.steps, settleSteps=0,
                         boundaryRho=w.rho, storage=w.storage if storage is None else storage,
-                        rounding=rounding)
+                        rounding=rounding,
+                        nearField=w.meta.get("near_field", 0) if near_field is None else near_field)
         self.sv = np.ascontiguousarray(w.sv if (w.waveform == 3 and w.sv is not None) else [],
                                        dtype=np.float32)
         self.cells = np.ascontiguousarray(
@@ -68,10 +69,10 @@ class _Request:
         self.c = r
 
 
-def footprint(w, storage=None) -> int:
+def footprint(w, storage=None, near_field=None) -> int:
     """Device bytes the solve holds while it runs (what admission counts)."""
     L = _lib.load()
-    r = _Request(w, storage)
+    r = _Request(w, storage, near_field=near_field)
     b = C.c_size_t(0)
     check(L, None, L.tlm_request_footprint(C.byref(r.c), C.byref(b)))
     return b.value
@@ -90,8 +91,16 @@ class Server:
     def _c(self, status):
         return check(self._L, None, status)
 
-    def submit(self, w, storage=None, rounding=0) -> int:
-        r = _Request(w, storage, rounding)
+    ARRIVAL, LEAST_WORK = 0, 1
+
+    def set_policy(self, order: int = 1, max_running_cells: int = 32 << 20, solo_cells: int = 4 << 20):
+        """Admission order (LEAST_WORK first, or ARRIVAL), the cap on the
+        running requests' padded cells (0: none), and the size from which a
+        request runs on its own beside the batch (0: never)."""
+        self._c(self._L.tlm_server_set_policy(self._s, int(order), int(max_running_cells), int(solo_cells)))
+
+    def submit(self, w, storage=None, rounding=0, near_field=None) -> int:
+        r = _Request(w, storage, rounding, near_field)
         rid = C.c_uint64(0)
         self._c(self._L.tlm_server_submit(self._s, C.byref(r.c), C.byref(rid)))
         return rid.value

@@ -345,12 +345,13 @@ TLM_API tlm_status tlm_batch_get_stream(tlm_batch b, void **stream);
 
 /* No counterpart in the reference (a desktop application running one solve
  * at a time). Requests are complete solves; a worker thread admits queued
- * requests in arrival order while their device footprint fits the HBM
- * budget, keeps their state resident on the GPU, advances all running
- * requests together in a batch one window at a time, and retires each at its
- * total_steps. Requests that arrive while others run join the batch at the
- * next window. Each result equals the same solve run alone with
- * tlm_setup/tlm_run. */
+ * requests (by default the least work -- padded cells x steps -- first)
+ * while their device footprint fits the HBM budget and the running cells
+ * stay within a cap that keeps the GPU saturated, keeps their state resident
+ * on the GPU, advances all running requests together in a batch one window
+ * at a time, and retires each at its total_steps. Requests that arrive while
+ * others run join the batch at the next window. Each result equals the same
+ * solve run alone with tlm_setup/tlm_run. */
 typedef struct tlm_server_s *tlm_server;
 
 enum { TLM_REQ_QUEUED = 0, TLM_REQ_RUNNING = 1, TLM_REQ_DONE = 2, TLM_REQ_FAILED = 3,
@@ -383,12 +384,29 @@ typedef struct tlm_server_stats_t {
     size_t hbm_used_bytes, hbm_budget_bytes;
     long long windows;
     double busy_s;                  /* time spent stepping */
+    double gpu_window_s;            /* device time of the windows (events) */
+    double setup_s, retire_s;       /* host set-up of admitted requests (during
+                                       windows) / read-out and release of
+                                       finished ones (between windows) */
+    double mean_running_cells;      /* padded cells running, mean over windows */
 } tlm_server_stats_t;
 
 /* hbm_budget_bytes 0 = 80% of the device's free memory; steps_per_launch 0
  * = 64 (the admission / retirement granularity). */
 TLM_API tlm_status tlm_server_create(tlm_server *out, int device, size_t hbm_budget_bytes,
                                      int steps_per_launch);
+/* Admission order: TLM_SERVE_LEAST_WORK (default: the queued request with
+ * the fewest padded cells x steps first, so short solves are not held up
+ * behind long ones) or TLM_SERVE_ARRIVAL (first come, first served);
+ * max_running_cells caps the padded cells of the running requests (0 = no
+ * cap; default 32 Mi), above which queued requests wait rather than slow
+ * every running one down. The first request always runs. Requests of
+ * solo_cells padded cells or more (0 = none; default 4 Mi) do not join the
+ * batch: large grids fill the GPU alone, so they are stepped window by
+ * window on their own stream by the single-grid kernels, beside the batch. */
+enum { TLM_SERVE_ARRIVAL = 0, TLM_SERVE_LEAST_WORK = 1 };
+TLM_API tlm_status tlm_server_set_policy(tlm_server s, int order, long long max_running_cells,
+                                         long long solo_cells);
 /* Stops the worker; queued and running requests end CANCELLED. */
 TLM_API tlm_status tlm_server_destroy(tlm_server s);
 /* Copies the request and queues it; TLM_ENOMEM if it can never fit. */

@@ -109,3 +109,46 @@ def test_destroy_cancels_pending(built):
     for w in ws:
         srv.submit(w)
     srv.close()                           # must not hang with work queued
+
+
+def test_least_work_first_admission(built):
+    """With a running-cells cap that fits one request at a time, a short
+    request queued behind a long one is admitted first under the least-work
+    order (and finishes first), and after it under the arrival order; both
+    results equal the solves run alone."""
+    rng = np.random.default_rng(12)
+    blocker = workloads.random_dipole(rng, 40, 40, 40, 600, name="blocker")
+    long_w = workloads.random_dipole(rng, 40, 40, 40, 600, name="long")
+    short_w = workloads.random_dipole(rng, 24, 24, 24, 150, name="short")
+    for w in (blocker, long_w, short_w):
+        w.dft_freqs = w.dft_freqs[:8]
+    for order, short_first in ((Server.LEAST_WORK, True), (Server.ARRIVAL, False)):
+        with Server() as srv:
+            srv.set_policy(order, 1, 0)           # one request at a time, all in the batch
+            ids = [srv.submit(w) for w in (blocker, long_w, short_w)]
+            for rid in ids:
+                assert srv.wait(rid, 120.0) == DONE
+            lat = {w.name: srv.result(rid)[2] for rid, w in zip(ids, (blocker, long_w, short_w))}
+            assert (lat["short"] < lat["long"]) == short_first, (order, lat)
+            for rid, w in zip(ids, (blocker, long_w, short_w)):
+                v, i, _ = srv.result(rid)
+                av, ai, _, _ = solve_alone(w)
+                assert np.array_equal(v, av) and np.array_equal(i, ai), (order, w.name)
+
+
+def test_solo_lane_results_equal_alone(built):
+    """Requests at or above the solo size run on their own stream beside the
+    batch (here: every request of at least 30^3 cells); all results, solo
+    and batched, equal the solves run alone."""
+    ws = requests(6, seed=21, lo=20, hi=40)
+    with Server() as srv:
+        srv.set_policy(Server.LEAST_WORK, 0, 30 ** 3)
+        ids = [srv.submit(w) for w in ws]
+        for rid in ids:
+            assert srv.wait(rid, 120.0) == DONE
+        for rid, w in zip(ids, ws):
+            v, i, _ = srv.result(rid)
+            vr, ir = srv.port_records(rid)
+            av, ai, avr, air = solve_alone(w)
+            assert np.array_equal(v, av) and np.array_equal(i, ai), w.name
+            assert np.array_equal(vr, avr) and np.array_equal(ir, air), w.name
