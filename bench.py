@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--no-autotune", action="store_true",
                    help="batched: skip the autotuner (default tuning, windows of --window steps)")
     p.add_argument("--window", type=int, default=100, help="batched: steps per CUDA-graph window")
+    p.add_argument("--profile-steps", type=int, default=0,
+                   help="batched: only attach the instances and step them this many steps without "
+                        "graphs (a small case for ncu); prints no bench line")
     p.add_argument("--near-field", type=int, default=None,
                    help="16-bit storage: radius of the FP32-residual box around PEC and ports "
                         "(default 6 for f16/bf16)")
@@ -616,6 +619,16 @@ def run_batched(args):
     for w in ws:
         w.storage = code
         w.meta["near_field"] = nf
+    if args.profile_steps > 0:
+        solvers = [build_solver(w) for w in ws]
+        with Batch() as b:
+            for s in solvers:
+                b.attach(s)
+            b.set_tuning(BatchTuning(steps_per_launch=16, use_graphs=False))
+            b.step(args.profile_steps)
+        for s in solvers:
+            s.close()
+        return
     nodes = sum(w.ncells for w in ws)
     work = sum(w.ncells * w.steps for w in ws)
     sequential_solves(ws[:4])                        # warm-up (context, kernels)

@@ -157,30 +157,36 @@ __global__ void __launch_bounds__(kBlock, MINB)
 // Staged tiles of an FP32 batch group (2 nodes per thread): the single-grid
 // staged kernel's pipeline over the (member, packed tile entry) pairs of
 // every member's staged tiles. The producer warp holds the entries of the
-// next 32 to 64 tiles and loads the head of the next tile's member (one word
-// per lane) while the current tile's copies are issued; per tile it writes
-// the member's head, the step's output planes and energy partials and the
-// tile's entry into the stage's header, or marks the stage empty when the
-// member is past its last step. Energy steps differ between members, so each
-// consumer counts its own uses of every stage's energy barrier (the same
-// sequence in every thread).
-struct BatchStageHdr
+// next 32 to 64 tiles; per tile its lanes load the member's 128-byte head as
+// eight 16-byte vectors (L1-resident: a few hundred members) before waiting
+// for the stage, take the fields they need from registers (warp shuffles
+// share the pipe with the consumers' shared-memory loads and measured about
+// 280 cycles each under load), and lane 0 writes the head, the step's output
+// planes and energy partials and the tile's entry into the stage's header
+// (or marks the stage empty when the member is past its last step), which
+// the consumers read back as 16-byte vectors. Energy steps differ between
+// members, so each consumer counts its own uses of every stage's energy
+// barrier (the same sequence in every thread).
+struct __align__(16) BatchStageHdr
 {
-    unsigned head[32];  // the member's head words (HeadWords)
+    uint4 head[8];      // the member's head words (HeadWords)
     float *out;         // output planes of this tile's step
     double *epart;      // energy partials of this step (nullptr: not an energy step)
     int tile;           // -1: an empty stage
     unsigned flags;
+    unsigned pad_[2];
 };
 
-__device__ __forceinline__ unsigned long long headU64(const unsigned *w, int i)
+// Word i (a compile-time index) of a head held as eight 16-byte vectors.
+template <int I> __device__ __forceinline__ unsigned headWord(const uint4 (&h)[8])
 {
-    return (unsigned long long)w[i] | ((unsigned long long)w[i + 1] << 32);
+    static_assert(I >= 0 && I < 32, "head word index");
+    const uint4 v = h[I / 4];
+    return (I % 4 == 0) ? v.x : (I % 4 == 1) ? v.y : (I % 4 == 2) ? v.z : v.w;
 }
-__device__ __forceinline__ unsigned long long shflU64(unsigned w, int i)
+template <int I> __device__ __forceinline__ unsigned long long headU64(const uint4 (&h)[8])
 {
-    const unsigned lo = __shfl_sync(0xffffffffu, w, i), hi = __shfl_sync(0xffffffffu, w, i + 1);
-    return (unsigned long long)lo | ((unsigned long long)hi << 32);
+    return (unsigned long long)headWord<I>(h) | ((unsigned long long)headWord<I + 1>(h) << 32);
 }
 
 template <int STAGES = kStages, int MINB = 2>
@@ -190,7 +196,6 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
 {
     using H = HeadWords;
     constexpr int kData = Stage<float>::kBytes;
-    constexpr int kDescWords = (int)(sizeof(MemberDesc<float>) / 4);
     extern __shared__ __align__(128) unsigned char stage[];
     __shared__ double red[STAGES][kBlock / 32];
     __shared__ __align__(8) unsigned long long full[STAGES], empty[STAGES], ered[STAGES];
@@ -212,24 +217,20 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
     if (threadIdx.x >= kBlock)
     {
         const int lane = threadIdx.x - kBlock;
-        const unsigned *words = reinterpret_cast<const unsigned *>(members);
         EntryWindow<int2> win;
         win.init(tiles, mine, lane, make_int2(0, 0));
-        // member of the block's tile `it` (it - win.it0 in [0, 64))
-        auto memberAt = [&](int it) {
-            const int d = it - win.it0;
-            const int ma = __shfl_sync(0xffffffffu, win.a.x, d & 31), mb = __shfl_sync(0xffffffffu, win.b.x, d & 31);
-            return d < 32 ? ma : mb;
-        };
-        unsigned wNext = mine > 0 ? words[(size_t)memberAt(0) * kDescWords + lane] : 0u;
         int issued = 0;
         for (int it = 0; it < mine; ++it)
         {
             const int s = it % STAGES;
             if (it == win.it0 + 32) win.slide(lane);
-            const int e = __shfl_sync(0xffffffffu, win.a.y, it - win.it0);
-            const unsigned w = wNext;
-            if (it + 1 < mine) wNext = words[(size_t)memberAt(it + 1) * kDescWords + lane];
+            const int2 ent = make_int2(__shfl_sync(0xffffffffu, win.a.x, it - win.it0),
+                                       __shfl_sync(0xffffffffu, win.a.y, it - win.it0));
+            const int e = ent.y;
+            uint4 h[8];
+            const uint4 *hp = reinterpret_cast<const uint4 *>(members + ent.x);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) h[q] = __ldg(hp + q);
             bool ok = true;
             if (it >= STAGES && lane == 0) ok = mbarWaitBounded(empty0 + 8 * s, (unsigned)(it / STAGES - 1) & 1u);
             if (!__shfl_sync(0xffffffffu, ok, 0))
@@ -237,43 +238,39 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
                 if (lane == 0 && fault) atomicOr(fault, kStageTimeout);
                 break;
             }
-            const long long n = (long long)shflU64(w, H::kBase) + i;
-            const bool live = n < (long long)shflU64(w, H::kTotal);
-            float *const buf0 = reinterpret_cast<float *>(shflU64(w, H::kBuf));
-            float *const buf1 = reinterpret_cast<float *>(shflU64(w, H::kBuf + 2));
-            double *const ep = reinterpret_cast<double *>(shflU64(w, H::kEpart));
-            const int nblocks = (int)__shfl_sync(0xffffffffu, w, H::kNblocks);
-            BatchStageHdr &hd = hdr[s];
-            hd.head[lane] = w;
+            const long long n = (long long)headU64<H::kBase>(h) + i;
+            const bool live = n < (long long)headU64<H::kTotal>(h);
+            float *const buf0 = reinterpret_cast<float *>(headU64<H::kBuf>(h));
+            float *const buf1 = reinterpret_cast<float *>(headU64<H::kBuf + 2>(h));
+            const unsigned bar = full0 + 8 * s;
             if (lane == 0)
             {
+                BatchStageHdr &hd = hdr[s];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) hd.head[q] = h[q];
                 const long long base = n - i;
                 const long long eFirst = (base + 15) / 16 * 16;
+                double *const ep = reinterpret_cast<double *>(headU64<H::kEpart>(h));
                 hd.out = (n & 1) ? buf0 : buf1;
-                hd.epart = (n % 16 == 0) ? ep + ((n - eFirst) / 16) * nblocks : nullptr;
+                hd.epart = (n % 16 == 0) ? ep + ((n - eFirst) / 16) * (int)headWord<H::kNblocks>(h) : nullptr;
                 hd.tile = live ? entryTile(e) : -1;
                 hd.flags = entryFlags(e);
+                if (!live) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(bar) : "memory");
             }
-            __syncwarp();
-            const unsigned bar = full0 + 8 * s;
-            if (!live)
-            {
-                if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(bar) : "memory");
-            }
-            else
+            if (live)
             {
                 StageSrc<float> src;
                 src.in = (n & 1) ? buf1 : buf0;
-                src.stub = reinterpret_cast<const float *>(shflU64(w, H::kStub));
-                src.mat = reinterpret_cast<const uint8_t *>(shflU64(w, H::kMat));
-                src.P = (long long)shflU64(w, H::kP);
-                src.px = (int)__shfl_sync(0xffffffffu, w, H::kPx);
-                src.ny = (int)__shfl_sync(0xffffffffu, w, H::kNy);
-                src.nz = (int)__shfl_sync(0xffffffffu, w, H::kNz);
-                src.div_nq.mul = __shfl_sync(0xffffffffu, w, H::kDivNq);
-                src.div_nq.shift = (int)__shfl_sync(0xffffffffu, w, H::kDivNq + 1);
-                src.div_ny.mul = __shfl_sync(0xffffffffu, w, H::kDivNy);
-                src.div_ny.shift = (int)__shfl_sync(0xffffffffu, w, H::kDivNy + 1);
+                src.stub = reinterpret_cast<const float *>(headU64<H::kStub>(h));
+                src.mat = reinterpret_cast<const uint8_t *>(headU64<H::kMat>(h));
+                src.P = (long long)headU64<H::kP>(h);
+                src.px = (int)headWord<H::kPx>(h);
+                src.ny = (int)headWord<H::kNy>(h);
+                src.nz = (int)headWord<H::kNz>(h);
+                src.div_nq.mul = headWord<H::kDivNq>(h);
+                src.div_nq.shift = (int)headWord<H::kDivNq + 1>(h);
+                src.div_ny.mul = headWord<H::kDivNy>(h);
+                src.div_ny.shift = (int)headWord<H::kDivNy + 1>(h);
                 stageTile(src, entryTile(e), entryFlags(e), st0 + s * kData, bar, lane);
             }
             issued = it + 1;
@@ -293,35 +290,40 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             return;
         }
         const BatchStageHdr &hd = hdr[s];
-        const int tile = hd.tile;
+        const uint4 tail0 = *reinterpret_cast<const uint4 *>(&hd.out);   // out, epart
+        const uint4 tail1 = *reinterpret_cast<const uint4 *>(&hd.tile);  // tile, flags
+        const int tile = (int)tail1.x;
         if (tile >= 0)
         {
+            uint4 h[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) h[q] = hd.head[q];
             StepArgs<float> a;
             a.in = nullptr;  // the staged body reads its inputs from the stage
-            a.out = hd.out;
-            a.stub = reinterpret_cast<float *>(headU64(hd.head, H::kStub));
+            a.out = reinterpret_cast<float *>((unsigned long long)tail0.x | ((unsigned long long)tail0.y << 32));
+            a.stub = reinterpret_cast<float *>(headU64<H::kStub>(h));
             a.mat = nullptr;
-            a.yhat = reinterpret_cast<const float *>(headU64(hd.head, H::kYhat));
-            a.ghat = reinterpret_cast<const float *>(headU64(hd.head, H::kGhat));
-            a.P = (long long)headU64(hd.head, H::kP);
+            a.yhat = reinterpret_cast<const float *>(headU64<H::kYhat>(h));
+            a.ghat = reinterpret_cast<const float *>(headU64<H::kGhat>(h));
+            a.P = (long long)headU64<H::kP>(h);
             a.nquads = 0;
-            a.nx = (int)hd.head[H::kNx];
-            a.ny = (int)hd.head[H::kNy];
-            a.nz = (int)hd.head[H::kNz];
-            a.px = (int)hd.head[H::kPx];
-            a.nq = (int)hd.head[H::kNq];
-            a.div_nq.mul = hd.head[H::kDivNq];
-            a.div_nq.shift = (int)hd.head[H::kDivNq + 1];
-            a.div_ny.mul = hd.head[H::kDivNy];
-            a.div_ny.shift = (int)hd.head[H::kDivNy + 1];
-            a.rho = __uint_as_float(hd.head[H::kRho]);
+            a.nx = (int)headWord<H::kNx>(h);
+            a.ny = (int)headWord<H::kNy>(h);
+            a.nz = (int)headWord<H::kNz>(h);
+            a.px = (int)headWord<H::kPx>(h);
+            a.nq = (int)headWord<H::kNq>(h);
+            a.div_nq.mul = headWord<H::kDivNq>(h);
+            a.div_nq.shift = (int)headWord<H::kDivNq + 1>(h);
+            a.div_ny.mul = headWord<H::kDivNy>(h);
+            a.div_ny.shift = (int)headWord<H::kDivNy + 1>(h);
+            a.rho = __uint_as_float(headWord<H::kRho>(h));
             a.scale = 1.0f;
             a.inv_scale = 1.0f;
             a.tile_begin = nullptr;
             a.spec = nullptr;
             a.sv = 0.0f;
             a.samples = nullptr;
-            a.epart = hd.epart;
+            a.epart = reinterpret_cast<double *>((unsigned long long)tail0.z | ((unsigned long long)tail0.w << 32));
             a.e_lo = 0;
             a.e_hi = LLONG_MAX;
             a.fault = fault;
@@ -330,9 +332,10 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             a.tile_flags = nullptr;
             a.neg_zero = negZero;
             a.stage_wait_ns = kStageWaitNs;
+            a.near = NearBox{};
             const unsigned ep = (eBits >> s) & 1u;
             if (a.epart != nullptr) eBits ^= 1u << s;
-            stepTileInterior<float, 2, true>(a, tile, red[s], (hd.flags & kTileDiel) != 0, stage + s * kData,
+            stepTileInterior<float, 2, true>(a, tile, red[s], (tail1.y & kTileDiel) != 0, stage + s * kData,
                                              ered0 + 8 * s, ep);
         }
         __syncwarp();
