@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=20)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="heterogeneous",
-                   choices=["heterogeneous", "plain", "precision", "energy", "batched", "served", "fdtd"])
+                   choices=["heterogeneous", "plain", "precision", "energy", "batched", "served", "fdtd", "slab"])
     p.add_argument("--instances", type=int, default=256, help="batched: number of instances")
     p.add_argument("--requests", type=int, default=200, help="served: number of requests")
     p.add_argument("--rate", type=float, default=200.0, help="served: mean arrivals per second")
@@ -59,6 +59,8 @@ def parse():
                    help="16-bit storage: radius of the FP32-residual box around PEC and ports "
                         "(default 6 for f16/bf16)")
     p.add_argument("--precision-steps", type=int, default=8000, help="precision: steps per mode")
+    p.add_argument("--slab-edge", type=int, default=384,
+                   help="slab: edge of the heterogeneous grid split into z-slabs over the ranks")
     p.add_argument("--order", default="least-work", choices=["least-work", "arrival"],
                    help="served: admission order")
     p.add_argument("--max-running-cells", type=int, default=32 << 20,
@@ -567,6 +569,64 @@ def run_energy(args):
     print(json.dumps(line), flush=True)
 
 
+def run_slab(args):
+    """One grid split into z-slabs over the ranks of the launch (torchrun,
+    NCCL between GPUs): the heterogeneous grid of --slab-edge cells per axis
+    (16 lossy dielectric boxes, a source, 8 probes), every rank stepping its
+    own planes with the halo exchange overlapped (tlm_slab_step_begin/_end),
+    device-timed on each rank's stream, max over ranks. Strong scaling: the
+    grid is the same at every rank count; value = the grid's node-updates
+    per second."""
+    import datetime
+    import torch
+    import torch.distributed as tdist
+    from emsolver_b200 import workloads
+    from emsolver_b200.slab import SlabSolver
+    world = check_world(args)
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if not tdist.is_initialized():
+        if world > 1:
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        else:
+            tdist.init_process_group("gloo", init_method="tcp://127.0.0.1:0", rank=0, world_size=1)
+    w = workloads.heterogeneous(n=args.slab_edge, steps=args.warmup + args.steps)
+    s = SlabSolver(w, device=local)
+    s.step(args.warmup)
+    ext = torch.cuda.ExternalStream(s.slab.solver.stream(), device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0.record(ext)
+    s.step(args.steps)
+    e1.record(ext)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+    halo = s.slab.nbytes * ((s.send_lo is not None) + (s.send_hi is not None))
+    s.close()
+    if rank == 0:
+        line = {"metric": "TLM node-updates/s (one grid in z-slabs)", "value": w.ncells * args.steps / (ms / 1e3),
+                "unit": "node-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                "config": {"workload": f"heterogeneous {w.nx}x{w.ny}x{w.nz} split into {world} z-slabs",
+                           "nodes": w.ncells, "slab_planes": [list(r) for r in s.ranges],
+                           "halo_bytes_per_step_rank0": halo, "parallelism": f"z-slabs x{world}"},
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+    tdist.destroy_process_group()
+
+
 def sequential_solves(ws):
     """Each instance alone through the plain API, one after the other:
     setup, all steps, port DFT back to the host, free. Returns per-solve
@@ -824,6 +884,8 @@ def main():
         run_precision(args)
     elif args.workload == "energy":
         run_energy(args)
+    elif args.workload == "slab":
+        run_slab(args)
     else:
         run_ours(args)
 

@@ -312,6 +312,10 @@ SIGNATURES = {
     "tlm_device_bytes": (_st, [_h, _P(C.c_size_t)]),
     "tlm_set_kernel_timing": (_st, [_h, C.c_int]),
     "tlm_kernel_time": (_st, [_h, _P(C.c_double), _P(C.c_longlong)]),
+    "tlm_slab_step_begin": (_st, [_h, C.c_void_p, C.c_void_p]),
+    "tlm_slab_step_end": (_st, [_h, C.c_void_p, C.c_void_p]),
+    "tlm_slab_flush": (_st, [_h]),
+    "tlm_get_halo_stream": (_st, [_h, _P(C.c_void_p)]),
     "tlm_step_launches": (_st, [_h, _P(C.c_int)]),
     "tlm_near_field_box": (_st, [_h, _P(C.c_int)]),
 }

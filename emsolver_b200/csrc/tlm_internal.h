@@ -254,6 +254,19 @@ struct tlm_solver
     std::vector<int> edgeTiles;                 // interior tiles on an outer face (listed alone, staged in a batch)
     cudaStream_t side = nullptr;      // the list kernel's stream (forked from and joined to `stream`)
     cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    // z-slab steps in two phases (tlm_slab_step_begin / _end): tile lists of
+    // the own planes next to a ghost plane (boundary), of the other own
+    // planes (interior: listed, and staged as packed entries), the stream
+    // the halo messages travel on, and the open launch window
+    bool slabLists = false;
+    int *dSlabB = nullptr, *dSlabI = nullptr, *dSlabS = nullptr;
+    int nSlabB = 0, nSlabI = 0, nSlabS = 0, slabStagedGrid = 0;
+    cudaStream_t halo = nullptr;
+    cudaEvent_t evBoundary = nullptr, evHalo = nullptr;
+    bool slabBegun = false, slabOpen = false;
+    int slabPos = 0;
+    long long slabBase = 0, slabEFirst = 0;
+    std::vector<uint8_t> tileFlagsHost;
     void *dSamples = nullptr;
     double *dEpart = nullptr;
     int *dPortOff = nullptr, *dPortSlots = nullptr, *dPortPol = nullptr, *dPortNb = nullptr;

@@ -81,6 +81,11 @@ void freeMonitors(tlm_solver *h)
     devFree(h, h->dLo[0]);
     devFree(h, h->dLo[1]);
     h->nearBox = tlmk::NearBox{};
+    devFree(h, h->dSlabB);
+    devFree(h, h->dSlabI);
+    devFree(h, h->dSlabS);
+    h->nSlabB = h->nSlabI = h->nSlabS = 0;
+    h->slabLists = false;
     h->recCap = 0;
     h->prepared = false;
 }
@@ -378,6 +383,7 @@ tlm_status prepare(tlm_solver *h)
         std::vector<unsigned> mf;
         TLM_TRY(materialFlags(h, mf));
         const std::vector<uint8_t> flags = tileFlags(h, tile, mf);
+        h->tileFlagsHost = flags;
         TLM_TRY(devAlloc(h, &h->dTileFlags, flags.size()));
         TLM_CU(h, cudaMemcpyAsync(h->dTileFlags, flags.data(), flags.size(), cudaMemcpyHostToDevice,
                                   h->stream));
@@ -510,7 +516,9 @@ void launchShaped(const tlmk::StepArgs<S> &a, int variant, bool incident, int nb
     });
 }
 
-template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long eFirst)
+// The step kernels' arguments for step n, the i-th of its launch window
+// (records of the window's first energy step eFirst), reading buffer curBuf.
+template <class S> tlmk::StepArgs<S> stepArgs(const tlm_solver *h, int n, int i, long long eFirst)
 {
     using R = typename tlmk::Traits<S>::R;
     tlmk::StepArgs<S> a;
@@ -547,6 +555,14 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
                       : h->cfg.stage_wait_us < 0 ? 0ull
                                                  : tlmk::kStageWaitNs;
     a.near = nearArgs(h, h->curBuf);
+    a.round_seed = tlmk::mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
+    a.stochastic = h->cfg.rounding == 1 ? 1 : 0;
+    return a;
+}
+
+template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long eFirst)
+{
+    const tlmk::StepArgs<S> a = stepArgs<S>(h, n, i, eFirst);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (h->timing)
     {
@@ -561,8 +577,6 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
         h->evUsed += 2;
         TLM_CU(h, cudaEventRecord(e0, h->stream));
     }
-    a.round_seed = tlmk::mix32((unsigned)n * 0x9E3779B9u + 0x7f4a7c15u);
-    a.stochastic = h->cfg.rounding == 1 ? 1 : 0;
     if (surfaceActive(h)) TLM_TRY(launchSurface(h, n));  // reads the same input buffer, first
     if constexpr (std::is_same<S, float>::value)
     {
@@ -1069,6 +1083,13 @@ tlm_status tlm_destroy(tlm_handle h)
         cudaEventDestroy(h->evJoin);
         cudaStreamDestroy(h->side);
     }
+    if (h->halo)
+    {
+        cudaStreamSynchronize(h->halo);
+        cudaEventDestroy(h->evBoundary);
+        cudaEventDestroy(h->evHalo);
+        cudaStreamDestroy(h->halo);
+    }
     cudaStreamDestroy(h->stream);
     delete h;
     return TLM_OK;
@@ -1385,6 +1406,8 @@ tlm_status tlm_step_async(tlm_handle h, int n_steps)
     TLM_TRY(checkReady(h));
     if (h->batch) return h->fail(TLM_ESTATE, "the handle is attached to a batch: step the batch");
     if (n_steps < 0) return h->fail(TLM_EINVAL, "n_steps must be >= 0");
+    if (h->slabBegun || h->slabOpen)
+        return h->fail(TLM_ESTATE, "slab steps are open: end them and call tlm_slab_flush first");
     DeviceGuard dg(h->device);
     if (h->curStep == 0 && !h->prepared) TLM_TRY(chooseScale(h));
     return enqueueSteps(h, n_steps, false, nullptr);
@@ -1490,15 +1513,13 @@ size_t haloOffset(const tlm_solver *h, int slot, int k)
     return ((size_t)slot * h->P + (size_t)k * h->ny * h->px) * tlmi::storageBytes(h->storage);
 }
 
-tlm_status haloCopy(tlm_solver *h, bool pack, void *lo, void *hi)
+// Copy the halo between the messages and pulse buffer `buf` on `stream`.
+tlm_status haloCopyOn(tlm_solver *h, bool pack, void *lo, void *hi, cudaStream_t stream, int buf)
 {
-    TLM_TRY(checkReady(h));
     if ((lo != nullptr) != (h->ghostLo != 0) || (hi != nullptr) != (h->ghostHi != 0))
         return h->fail(TLM_EINVAL, "pass a buffer exactly for each side that has a ghost plane");
     if (!lo && !hi) return TLM_OK;  // a slab without neighbours
-    if (h->stateIncident) return h->fail(TLM_ESTATE, "the state is incident pulses (tlm_set_pulses): step first");
-    DeviceGuard dg(h->device);
-    char *state = static_cast<char *>(h->dPulses[h->curBuf]);
+    char *state = static_cast<char *>(h->dPulses[buf]);
     const size_t half = (size_t)h->ny * h->px * tlmi::storageBytes(h->storage);
     const int first = h->ghostLo, last = h->nz - 1 - h->ghostHi;
     // slot = axis * 4 + side * 2 + pol: 8, 9 leave a node through its -z
@@ -1515,9 +1536,139 @@ tlm_status haloCopy(tlm_solver *h, bool pack, void *lo, void *hi)
         {
             char *dev = state + haloOffset(h, sd.slot + t, sd.plane);
             char *msg = sd.buf + t * half;
-            TLM_CU(h, cudaMemcpyAsync(pack ? msg : dev, pack ? dev : msg, half, cudaMemcpyDeviceToDevice, h->stream));
+            TLM_CU(h, cudaMemcpyAsync(pack ? msg : dev, pack ? dev : msg, half, cudaMemcpyDeviceToDevice, stream));
         }
     }
+    return TLM_OK;
+}
+
+tlm_status haloCopy(tlm_solver *h, bool pack, void *lo, void *hi)
+{
+    TLM_TRY(checkReady(h));
+    if (h->stateIncident) return h->fail(TLM_ESTATE, "the state is incident pulses (tlm_set_pulses): step first");
+    DeviceGuard dg(h->device);
+    return haloCopyOn(h, pack, lo, hi, h->stream, h->curBuf);
+}
+
+// Tile lists of the two-phase slab step: tiles that hold a node of an own
+// plane next to a ghost plane (boundary), the other tiles with an own node
+// (interior; FP32's staged tiles among them as packed entries), none of the
+// tiles that lie in ghost planes alone (ghost planes are not stepped: the
+// own planes read only the halo slots that tlm_slab_step_end writes).
+tlm_status buildSlabLists(tlm_solver *h)
+{
+    if (h->slabLists) return TLM_OK;
+    const long long T = (long long)kBlock * h->V, planeN = (long long)h->ny * h->px;
+    const int lowB = h->ghostLo ? 1 : -1, highB = h->ghostHi ? h->nz - 2 : -1;
+    auto ghost = [&](long long k) { return (h->ghostLo && k == 0) || (h->ghostHi && k == h->nz - 1); };
+    const bool staged = h->storage == TLM_STORE_F32 && !h->cfg.no_staging && h->V == 2 &&
+                        shapeOf(h->storage, h->variant).select;
+    std::vector<int> B, I, St;
+    for (int t = 0; t < h->nblocks; ++t)
+    {
+        const long long n0 = (long long)t * T, n1 = std::min(n0 + T, h->P) - 1;
+        bool allGhost = true, boundary = false;
+        for (long long k = n0 / planeN; k <= n1 / planeN; ++k)
+        {
+            allGhost = allGhost && ghost(k);
+            boundary = boundary || k == lowB || k == highB;
+        }
+        if (allGhost) continue;
+        const uint8_t f = h->tileFlagsHost[(size_t)t];
+        if (boundary)
+            B.push_back(t);
+        else if (staged && !(f & (tlmk::kTileGeneral | tlmk::kTileEdge)))
+            St.push_back(tlmk::packStagedEntry(t, f));
+        else
+            I.push_back(t);
+    }
+    auto upload = [&](int **d, const std::vector<int> &v) -> tlm_status {
+        if (v.empty()) return TLM_OK;
+        TLM_TRY(devAlloc(h, d, v.size() * sizeof(int)));
+        return h->cuda(cudaMemcpyAsync(*d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream),
+                       "slab tile lists");
+    };
+    TLM_TRY(upload(&h->dSlabB, B));
+    TLM_TRY(upload(&h->dSlabI, I));
+    TLM_TRY(upload(&h->dSlabS, St));
+    h->nSlabB = (int)B.size();
+    h->nSlabI = (int)I.size();
+    h->nSlabS = (int)St.size();
+    if (h->nSlabS > 0)
+    {
+        int sms = 0;
+        TLM_CU(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+        TLM_TRY(stagedAttributes<float>(h));
+        h->slabStagedGrid = std::min(h->nSlabS, 2 * sms);
+    }
+    // tiles of ghost planes alone never write their energy partials: zero
+    TLM_CU(h, cudaMemsetAsync(h->dEpart, 0, (size_t)(h->window / 16 + 1) * h->nblocks * sizeof(double), h->stream));
+    if (!h->halo)
+    {
+        TLM_CU(h, cudaStreamCreateWithFlags(&h->halo, cudaStreamNonBlocking));
+        TLM_CU(h, cudaEventCreateWithFlags(&h->evBoundary, cudaEventDisableTiming));
+        TLM_CU(h, cudaEventCreateWithFlags(&h->evHalo, cudaEventDisableTiming));
+    }
+    h->slabLists = true;
+    return TLM_OK;
+}
+
+// One phase of a slab step: 0 the boundary tiles, 1 the interior tiles.
+// (C++ linkage: this part of the file lies inside the C ABI's extern "C".)
+extern "C++" {
+template <class S> tlm_status slabLaunch(tlm_solver *h, int phase)
+{
+    const tlmk::StepArgs<S> a = stepArgs<S>(h, (int)(h->slabBase + h->slabPos), h->slabPos, h->slabEFirst);
+    withShape<S>(h->variant, [&](auto V, auto MINB, auto SEL) {
+        if (phase == 0)
+        {
+            if (h->nSlabB > 0)
+                tlmk::stepKernelList<S, V(), MINB(), SEL()><<<h->nSlabB, kBlock, 0, h->stream>>>(a, h->dSlabB);
+            return;
+        }
+        if constexpr (std::is_same<S, float>::value && V() == 2 && SEL())
+        {
+            if (h->nSlabS > 0)
+                tlmk::stepKernelStaged<S, 2><<<h->slabStagedGrid, tlmk::kStagedThreads,
+                                               tlmk::kStages * tlmk::Stage<S>::kBytes, h->stream>>>(a, h->dSlabS,
+                                                                                                    h->nSlabS);
+        }
+        if (h->nSlabI > 0)
+            tlmk::stepKernelList<S, V(), MINB(), SEL()><<<h->nSlabI, kBlock, 0, h->stream>>>(a, h->dSlabI);
+    });
+    return h->cuda(cudaGetLastError(), "slab step launch");
+}
+} // extern "C++"
+
+tlm_status slabPhase(tlm_solver *h, int phase)
+{
+    switch (h->storage)
+    {
+    case TLM_STORE_F64: return slabLaunch<double>(h, phase);
+    case TLM_STORE_BF16: return slabLaunch<__nv_bfloat16>(h, phase);
+    case TLM_STORE_F16: return slabLaunch<__half>(h, phase);
+    case TLM_STORE_BFP16: return slabLaunch<tlmk::Bfp4>(h, phase);
+    default: return slabLaunch<float>(h, phase);
+    }
+}
+
+// Close the open launch window: records, DFT and energy of its steps.
+tlm_status slabCloseWindow(tlm_solver *h)
+{
+    if (!h->slabOpen) return TLM_OK;
+    const long long base = h->slabBase, eFirst = h->slabEFirst;
+    const int w = h->slabPos;
+    const int nE = eFirst < base + w ? (int)((base + w - 1 - eFirst) / 16 + 1) : 0;
+    if (w > 0)
+    {
+        if (h->storage == TLM_STORE_F64)
+            TLM_TRY(launchEpilogue<double>(h, base, w, eFirst, nE));
+        else
+            TLM_TRY(launchEpilogue<float>(h, base, w, eFirst, nE));
+    }
+    h->curStep += w;
+    h->slabOpen = false;
+    h->slabPos = 0;
     return TLM_OK;
 }
 } // namespace
@@ -1527,6 +1678,77 @@ tlm_status tlm_halo_pack(tlm_handle h, void *send_lo, void *send_hi) { return ha
 tlm_status tlm_halo_unpack(tlm_handle h, const void *recv_lo, const void *recv_hi)
 {
     return haloCopy(h, false, const_cast<void *>(recv_lo), const_cast<void *>(recv_hi));
+}
+
+tlm_status tlm_slab_step_begin(tlm_handle h, void *send_lo, void *send_hi)
+{
+    TLM_TRY(checkReady(h));
+    if (h->batch) return h->fail(TLM_ESTATE, "the handle is attached to a batch");
+    if (h->slabBegun) return h->fail(TLM_ESTATE, "end the begun slab step first (tlm_slab_step_end)");
+    if (h->stateIncident) return h->fail(TLM_ESTATE, "the state is incident pulses (tlm_set_pulses): step first");
+    if (surfaceActive(h)) return h->fail(TLM_EINVAL, "slab steps do not run surface monitors");
+    if ((send_lo != nullptr) != (h->ghostLo != 0) || (send_hi != nullptr) != (h->ghostHi != 0))
+        return h->fail(TLM_EINVAL, "pass a buffer exactly for each side that has a ghost plane");
+    DeviceGuard dg(h->device);
+    if (h->curStep == 0 && !h->prepared) TLM_TRY(chooseScale(h));
+    TLM_TRY(prepare(h));
+    TLM_TRY(buildSlabLists(h));
+    if (!h->slabOpen)
+    {
+        h->slabBase = h->curStep;
+        h->slabEFirst = (h->slabBase + 15) / 16 * 16;
+        h->slabPos = 0;
+        TLM_TRY(ensureRecords(h, h->slabBase + h->window));
+        h->slabOpen = true;
+    }
+    // the boundary tiles, then their outgoing halo on the halo stream
+    TLM_TRY(slabPhase(h, 0));
+    TLM_CU(h, cudaEventRecord(h->evBoundary, h->stream));
+    TLM_CU(h, cudaStreamWaitEvent(h->halo, h->evBoundary, 0));
+    TLM_TRY(haloCopyOn(h, true, send_lo, send_hi, h->halo, h->curBuf ^ 1));
+    h->slabBegun = true;
+    return TLM_OK;
+}
+
+tlm_status tlm_slab_step_end(tlm_handle h, const void *recv_lo, const void *recv_hi)
+{
+    TLM_TRY(checkReady(h));
+    if (!h->slabBegun) return h->fail(TLM_ESTATE, "no slab step has begun (tlm_slab_step_begin)");
+    if ((recv_lo != nullptr) != (h->ghostLo != 0) || (recv_hi != nullptr) != (h->ghostHi != 0))
+        return h->fail(TLM_EINVAL, "pass a buffer exactly for each side that has a ghost plane");
+    DeviceGuard dg(h->device);
+    // the received halo into the ghost planes, beside the interior tiles
+    TLM_TRY(haloCopyOn(h, false, const_cast<void *>(recv_lo), const_cast<void *>(recv_hi), h->halo, h->curBuf ^ 1));
+    TLM_CU(h, cudaEventRecord(h->evHalo, h->halo));
+    TLM_TRY(slabPhase(h, 1));
+    TLM_CU(h, cudaStreamWaitEvent(h->stream, h->evHalo, 0));  // the next step reads the ghost planes
+    h->curBuf ^= 1;
+    h->slabBegun = false;
+    if (++h->slabPos == h->window) TLM_TRY(slabCloseWindow(h));
+    return TLM_OK;
+}
+
+tlm_status tlm_slab_flush(tlm_handle h)
+{
+    TLM_TRY(checkReady(h));
+    if (h->slabBegun) return h->fail(TLM_ESTATE, "end the begun slab step first (tlm_slab_step_end)");
+    DeviceGuard dg(h->device);
+    return slabCloseWindow(h);
+}
+
+tlm_status tlm_get_halo_stream(tlm_handle h, void **stream)
+{
+    TLM_TRY(checkReady(h));
+    if (!stream) return h->fail(TLM_EINVAL, "null output");
+    DeviceGuard dg(h->device);
+    if (!h->halo)
+    {
+        TLM_CU(h, cudaStreamCreateWithFlags(&h->halo, cudaStreamNonBlocking));
+        TLM_CU(h, cudaEventCreateWithFlags(&h->evBoundary, cudaEventDisableTiming));
+        TLM_CU(h, cudaEventCreateWithFlags(&h->evHalo, cudaEventDisableTiming));
+    }
+    *stream = (void *)h->halo;
+    return TLM_OK;
 }
 
 int tlm_probe_count(tlm_handle h) { return h ? (int)h->probeCells.size() : 0; }

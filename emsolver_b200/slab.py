@@ -5,11 +5,14 @@ z-slabs over worker threads (TlmSolver.cpp:174-240, 516-613). For a grid too
 large for one GPU's HBM, or to bring several GPUs to one grid, each rank here
 owns a contiguous range of z-planes as its own solver: the planes plus one
 ghost plane on each side that has a neighbour (the neighbour's boundary plane
-with its true material). After every step the ranks trade the z-directed
-pulses that cross each shared face (tlm_halo_pack / tlm_halo_unpack: two
-pulse slots of one plane per face and direction, nx*ny*8 bytes in FP32) with
-point-to-point sends over the group (NCCL between GPUs). Nothing else
-crosses ranks on the data path; records are gathered once at the end.
+with its true material). Every step the ranks trade the z-directed pulses
+that cross each shared face (two pulse slots of one plane per face and
+direction, nx*ny*8 bytes in FP32) with point-to-point sends over the group
+(NCCL between GPUs), overlapped with the step: the planes next to a ghost
+plane step first and their halo leaves on a stream of its own while the
+other planes step (tlm_slab_step_begin / tlm_slab_step_end), and the next
+step waits only for the received halo. Nothing else crosses ranks on the
+data path; records are gathered once at the end.
 
 Results are bitwise those of the undivided grid for every pulse, probe and
 port record (each node's update reads the same values in the same order);
@@ -131,6 +134,15 @@ class DeviceSlab:
     def step1(self):
         self.solver.stepAsync(1)
 
+    def begin(self, send_lo, send_hi):
+        self.solver.slabStepBegin(self._addr(send_lo), self._addr(send_hi))
+
+    def end(self, recv_lo, recv_hi):
+        self.solver.slabStepEnd(self._addr(recv_lo), self._addr(recv_hi))
+
+    def flush(self):
+        self.solver.slabFlush()
+
     def pack(self, send_lo, send_hi):
         self.solver.haloPack(self._addr(send_lo), self._addr(send_hi))
 
@@ -138,8 +150,12 @@ class DeviceSlab:
         self.solver.haloUnpack(self._addr(recv_lo), self._addr(recv_hi))
 
     def exchange_context(self):
+        """The stream the halo messages travel on (the slab steps' halo
+        stream), so that the exchange overlaps the interior planes."""
         import torch
-        return torch.cuda.stream(self.stream)
+        if not hasattr(self, "_halo"):
+            self._halo = torch.cuda.ExternalStream(self.solver.haloStream(), device=self.device)
+        return torch.cuda.stream(self._halo)
 
     def finish(self):
         self.solver.sync()
@@ -202,11 +218,15 @@ class SlabSolver:
                     work.wait()
 
     def step(self, n=1):
+        """n steps in lockstep with the neighbours: per step the slab's
+        boundary planes and their outgoing halo (``begin``), the exchange,
+        then the received halo and the other planes (``end``), the exchange
+        overlapping the other planes' update on the device."""
         for _ in range(n):
-            self.slab.step1()
-            self.slab.pack(self.send_lo, self.send_hi)
+            self.slab.begin(self.send_lo, self.send_hi)
             self._exchange()
-            self.slab.unpack(self.recv_lo, self.recv_hi)
+            self.slab.end(self.recv_lo, self.recv_hi)
+        self.slab.flush()
         self.slab.finish()
 
     def records(self):

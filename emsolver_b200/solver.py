@@ -510,6 +510,26 @@ class TlmSolver:
     def haloUnpack(self, recv_lo: int | None, recv_hi: int | None):
         self._c(self._L.tlm_halo_unpack(self._h, recv_lo, recv_hi))
 
+    def slabStepBegin(self, send_lo: int | None, send_hi: int | None):
+        """Step the own planes next to a ghost plane and pack their outgoing
+        halo on the halo stream (the first half of an overlapped slab step)."""
+        self._c(self._L.tlm_slab_step_begin(self._h, send_lo, send_hi))
+
+    def slabStepEnd(self, recv_lo: int | None, recv_hi: int | None):
+        """Unpack the received halo on the halo stream while the other own
+        planes step (the second half)."""
+        self._c(self._L.tlm_slab_step_end(self._h, recv_lo, recv_hi))
+
+    def slabFlush(self):
+        """Close the open launch window of slab steps (records, DFT, energy)."""
+        self._c(self._L.tlm_slab_flush(self._h))
+
+    def haloStream(self) -> int:
+        """The cudaStream_t the halo messages of slab steps travel on."""
+        s = C.c_void_p()
+        self._c(self._L.tlm_get_halo_stream(self._h, C.byref(s)))
+        return s.value
+
     def deviceBytes(self):
         b = C.c_size_t(0)
         self._c(self._L.tlm_device_bytes(self._h, C.byref(b)))

@@ -503,6 +503,23 @@ TLM_API tlm_status tlm_set_slab(tlm_handle h, int ghost_lo, int ghost_hi);
 TLM_API tlm_status tlm_halo_bytes(tlm_handle h, size_t *bytes);
 TLM_API tlm_status tlm_halo_pack(tlm_handle h, void *send_lo, void *send_hi);
 TLM_API tlm_status tlm_halo_unpack(tlm_handle h, const void *recv_lo, const void *recv_hi);
+/* The same exchange overlapped with the step, in two calls per step:
+ *   tlm_slab_step_begin(h, send_lo, send_hi)   steps the tiles of the own
+ *       planes next to a ghost plane, then packs their outgoing halo on the
+ *       halo stream (tlm_get_halo_stream);
+ *   the caller trades the messages on the halo stream (NCCL send/recv);
+ *   tlm_slab_step_end(h, recv_lo, recv_hi)     unpacks the received halo on
+ *       the halo stream while the other own planes step on the handle's
+ *       stream; the next step waits for the unpack.
+ * Ghost planes are not stepped. Steps are grouped into the handle's launch
+ * windows (records, DFT and energy once per window); tlm_slab_flush closes
+ * a partial window and must precede any other stepping of the handle or
+ * reading its records. Results are bitwise those of tlm_step with
+ * tlm_halo_pack/unpack, and of the undivided grid. */
+TLM_API tlm_status tlm_slab_step_begin(tlm_handle h, void *send_lo, void *send_hi);
+TLM_API tlm_status tlm_slab_step_end(tlm_handle h, const void *recv_lo, const void *recv_hi);
+TLM_API tlm_status tlm_slab_flush(tlm_handle h);
+TLM_API tlm_status tlm_get_halo_stream(tlm_handle h, void **stream);
 
 /* ---- one step over caller-owned device memory, no allocation -------- */
 

@@ -1,5 +1,9 @@
 """A grid split into z-slabs, every slab a B200 solver with ghost planes,
-the halo messages traded between steps (tlm_halo_pack / tlm_halo_unpack).
+the halo messages traded between steps: either after whole steps
+(tlm_halo_pack / tlm_halo_unpack) or overlapped with the step, which then
+runs in two launches (tlm_slab_step_begin: the planes next to a ghost plane
+and their outgoing halo; tlm_slab_step_end: the received halo and the other
+planes).
 
 One GPU here holds every slab: the slabs step one after the other and the
 messages are copied between their buffers with the device idle in between
@@ -19,7 +23,7 @@ from emsolver_b200.solver import Storage
 pytestmark = pytest.mark.gpu
 
 
-def run_split(w, parts, steps, **kw):
+def run_split(w, parts, steps, overlapped=False, **kw):
     ranges = split_planes(w.nz, parts, monitor_intervals(w))
     slabs, bufs = [], []
     for k0, k1 in ranges:
@@ -28,29 +32,42 @@ def run_split(w, parts, steps, **kw):
         slabs.append((s, v, glo, ghi, lo, k0, k1))
         bufs.append({key: (s.buffer() if (glo if key.endswith("lo") else ghi) else None)
                      for key in ("send_lo", "recv_lo", "send_hi", "recv_hi")})
-    for _ in range(steps):
-        for s, *_ in slabs:
-            s.step1()
-        for (s, *_), b in zip(slabs, bufs):
-            s.pack(b["send_lo"], b["send_hi"])
+
+    def trade():
         torch.cuda.synchronize()
         for r in range(len(slabs) - 1):
             bufs[r + 1]["recv_lo"].copy_(bufs[r]["send_hi"])
             bufs[r]["recv_hi"].copy_(bufs[r + 1]["send_lo"])
         torch.cuda.synchronize()
+
+    for _ in range(steps):
+        if overlapped:
+            for (s, *_), b in zip(slabs, bufs):
+                s.begin(b["send_lo"], b["send_hi"])
+            trade()
+            for (s, *_), b in zip(slabs, bufs):
+                s.end(b["recv_lo"], b["recv_hi"])
+            continue
+        for s, *_ in slabs:
+            s.step1()
+        for (s, *_), b in zip(slabs, bufs):
+            s.pack(b["send_lo"], b["send_hi"])
+        trade()
         for (s, *_), b in zip(slabs, bufs):
             s.unpack(b["recv_lo"], b["recv_hi"])
     for s, *_ in slabs:
+        if overlapped:
+            s.flush()
         s.finish()
     return slabs
 
 
-def check_split(w, parts, steps, f64=False, **kw):
+def check_split(w, parts, steps, f64=False, overlapped=False, **kw):
     whole = build_solver(w, **kw)
     whole.step(steps)
     ref = records(whole, w, f64=True)
     ref_p = whole.pulses(f64=f64).reshape(w.nz, w.ny * w.nx, 12)
-    slabs = run_split(w, parts, steps, **kw)
+    slabs = run_split(w, parts, steps, overlapped, **kw)
     energy = np.zeros_like(ref["energy"])
     for s, v, glo, ghi, lo, k0, k1 in slabs:
         p = s.solver.pulses(f64=f64).reshape(v.nz, v.ny * v.nx, 12)
@@ -78,17 +95,26 @@ def dipole_workload(seed, nx=26, ny=24, nz=41, steps=120):
     return w
 
 
+@pytest.mark.parametrize("overlapped", [False, True])
 @pytest.mark.parametrize("parts", [2, 3, 5])
-def test_split_f32_bitwise(built, parts):
-    check_split(dipole_workload(parts), parts, 120)
+def test_split_f32_bitwise(built, parts, overlapped):
+    check_split(dipole_workload(parts), parts, 120, overlapped=overlapped)
 
 
+def test_split_overlapped_staged_tiles_and_partial_window(built):
+    """A slab grid large enough that its interior planes hold staged tiles,
+    stepped a number of steps that leaves a partial launch window."""
+    w = dipole_workload(8, 70, 64, 36, 150)
+    check_split(w, 3, 150, overlapped=True)
+
+
+@pytest.mark.parametrize("overlapped", [False, True])
 @pytest.mark.parametrize("storage,kw", [(Storage.F64, {}), (Storage.BFP16, {}),
                                         (Storage.F16, {"pulse_scale": 2.0 ** -10})])
-def test_split_storage_modes_bitwise(built, storage, kw):
+def test_split_storage_modes_bitwise(built, storage, kw, overlapped):
     w = dipole_workload(11, 18, 17, 29, 80)
     w.storage = int(storage)
-    check_split(w, 3, 80, f64=storage == Storage.F64, **kw)
+    check_split(w, 3, 80, f64=storage == Storage.F64, overlapped=overlapped, **kw)
 
 
 @pytest.mark.parametrize("prop", [0, 2])

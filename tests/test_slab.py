@@ -63,6 +63,18 @@ class OracleSlab:
             v[own, ok, slots] = msg[ok]
         self.S.set_pulses(v.reshape(-1))
 
+    def begin(self, send_lo, send_hi):
+        """The first half of an overlapped slab step: the step, then the
+        outgoing halo."""
+        self.step1()
+        self.pack(send_lo, send_hi)
+
+    def end(self, recv_lo, recv_hi):
+        self.unpack(recv_lo, recv_hi)
+
+    def flush(self):
+        pass
+
     def finish(self):
         pass
 
