@@ -73,6 +73,8 @@ def parse():
     p.add_argument("--chunk", type=int, default=32, help="batched: instances set up per window")
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64", "bfp16"])
     p.add_argument("--steps-per-launch", type=int, default=0)
+    p.add_argument("--kernel-variant", type=int, default=0,
+                   help="tile shape of the step kernel (tlm_kernel_variants lists them)")
     p.add_argument("--no-staging", action="store_true",
                    help="one step kernel for all tiles (no staged FP32 / interior-only 16-bit kernel)")
     p.add_argument("--no-e2e", action="store_true")
@@ -310,7 +312,7 @@ def run_ours(args):
     w = make_workload(args.workload, args.warmup + args.steps)
     w.steps = args.warmup + args.steps
     s = build_solver(w, device=dev, storage=code, steps_per_launch=args.steps_per_launch, near_field=nf,
-                     no_staging=args.no_staging)
+                     no_staging=args.no_staging, kernel_variant=args.kernel_variant)
     s.step(args.warmup)
     torch.cuda.set_device(dev)
     ext = torch.cuda.ExternalStream(s.stream(), device=dev)
@@ -356,7 +358,7 @@ def run_ours(args):
         dist.barrier()
         t0 = time.perf_counter()
         s2 = build_solver(w, device=dev, storage=code, steps_per_launch=args.steps_per_launch, near_field=nf,
-                          no_staging=args.no_staging)
+                          no_staging=args.no_staging, kernel_variant=args.kernel_variant)
         s2.step(args.steps)
         recs = [s2.probe(q) for q in range(len(w.probes_cell))]
         ports = [s2.port(p) for p in range(len(w.ports))]

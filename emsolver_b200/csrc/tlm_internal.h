@@ -65,7 +65,7 @@ struct Shape
 };
 constexpr Shape kShapesF32[] = { { 2, 4, 1 }, { 4, 3, 1 }, { 4, 3, 0 }, { 4, 2, 0 } };
 constexpr Shape kShapesF64[] = { { 1, 4, 1 }, { 1, 4, 0 }, { 2, 3, 0 } };
-constexpr Shape kShapesHalf[] = { { 4, 3, 1 }, { 4, 3, 0 }, { 2, 4, 1 }, { 8, 2, 0 } };
+constexpr Shape kShapesHalf[] = { { 4, 3, 1 }, { 4, 3, 0 }, { 2, 4, 1 }, { 8, 2, 0 }, { 4, 2, 1 } };
 // block floating point: a thread owns whole 4-node groups
 constexpr Shape kShapesBfp[] = { { 4, 3, 1 }, { 4, 3, 0 }, { 4, 2, 0 } };
 

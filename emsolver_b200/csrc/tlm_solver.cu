@@ -259,10 +259,31 @@ tlm_status checkSlabMonitors(tlm_solver *h)
     return TLM_OK;
 }
 
+// The staged kernel's shape per storage type: FP32 stages tiles of 2 nodes
+// per thread in 3 stages, FP16/BF16 tiles of 4 nodes per thread (the same 2
+// KB per plane segment) in 2 stages (3 would not leave room for 2 blocks per
+// SM); both run 2 blocks per SM.
+template <class S> struct StagedShape
+{
+    static constexpr int V = 2, kStages = tlmk::kStages;
+};
+template <> struct StagedShape<__half>
+{
+    static constexpr int V = 4, kStages = 2;
+};
+template <> struct StagedShape<__nv_bfloat16>
+{
+    static constexpr int V = 4, kStages = 2;
+};
+template <class S> constexpr int stagedSmem()
+{
+    return StagedShape<S>::kStages * tlmk::Stage<S, StagedShape<S>::V>::kBytes;
+}
+
 template <class S> tlm_status stagedAttributes(tlm_solver *h)
 {
-    return h->cuda(cudaFuncSetAttribute(tlmk::stepKernelStaged<S, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        tlmk::kStages * tlmk::Stage<S>::kBytes),
+    return h->cuda(cudaFuncSetAttribute(tlmk::stepKernelStaged<S, StagedShape<S>::V, StagedShape<S>::kStages>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, stagedSmem<S>()),
                    "cudaFuncSetAttribute(stepKernelStaged)");
 }
 
@@ -278,8 +299,9 @@ tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
     h->stagedTiles.clear();
     h->listedTiles.clear();
     h->edgeTiles.clear();
-    if (h->storage != TLM_STORE_F32 || h->cfg.no_staging || h->V != 2 || !shapeOf(h->storage, h->variant).select)
-        return TLM_OK;
+    const bool f32 = h->storage == TLM_STORE_F32 && h->V == 2;
+    const bool half = (h->storage == TLM_STORE_F16 || h->storage == TLM_STORE_BF16) && h->V == 4;
+    if (!(f32 || half) || h->cfg.no_staging || !shapeOf(h->storage, h->variant).select) return TLM_OK;
     // staged lists hold packed entries (tile and flags, tlmk::packStagedEntry)
     std::vector<int> staged, listed, edge;
     for (int t = 0; t < h->nblocks; ++t)
@@ -301,9 +323,28 @@ tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
     h->edgeTiles = edge;
     std::sort(listed.begin(), listed.end());
     if (staged.empty()) return TLM_OK;
+    if (half)
+    {
+        // 16-bit tiles with stub-loaded nodes stage 12 KB of FP32 stubs
+        // beside 26 KB of pulses: with more than a quarter of them, the
+        // single kernel measured faster (192^3 heterogeneous: 0.1142 ms staged
+        // against 0.1056; the 384x384x256 dipole: 0.3436 against 0.359)
+        size_t diel = 0;
+        for (int e : staged) diel += (tlmk::entryFlags(e) & tlmk::kTileDiel) != 0;
+        if (4 * diel > staged.size())
+        {
+            h->edgeTiles.clear();
+            return TLM_OK;
+        }
+    }
     int sms = 0;
     TLM_CU(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-    TLM_TRY(stagedAttributes<float>(h));
+    if (h->storage == TLM_STORE_F16)
+        TLM_TRY(stagedAttributes<__half>(h));
+    else if (h->storage == TLM_STORE_BF16)
+        TLM_TRY(stagedAttributes<__nv_bfloat16>(h));
+    else
+        TLM_TRY(stagedAttributes<float>(h));
     if (!h->side)
     {
         TLM_CU(h, cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
@@ -593,6 +634,25 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
             }
             tlmk::stepKernelStaged<S, 2><<<h->stagedGrid, tlmk::kStagedThreads, tlmk::kStages * tlmk::Stage<S>::kBytes,
                                            h->stream>>>(a, h->dStaged, h->nStaged);
+            if (h->nListed > 0) TLM_CU(h, cudaStreamWaitEvent(h->stream, h->evJoin, 0));
+        }
+        else
+            launchShaped<S>(a, h->variant, h->stateIncident, h->nblocks, h->stream);
+    }
+    else if constexpr (std::is_same<S, __half>::value || std::is_same<S, __nv_bfloat16>::value)
+    {
+        if (h->nStaged > 0 && !h->stateIncident)
+        {
+            // as FP32: the listed tiles beside the staged ones
+            if (h->nListed > 0)
+            {
+                TLM_CU(h, cudaEventRecord(h->evFork, h->stream));
+                TLM_CU(h, cudaStreamWaitEvent(h->side, h->evFork, 0));
+                tlmk::stepKernelList<S, 4, 3, true><<<h->nListed, kBlock, 0, h->side>>>(a, h->dListed);
+                TLM_CU(h, cudaEventRecord(h->evJoin, h->side));
+            }
+            tlmk::stepKernelStaged<S, 4, StagedShape<S>::kStages>
+                <<<h->stagedGrid, tlmk::kStagedThreads, stagedSmem<S>(), h->stream>>>(a, h->dStaged, h->nStaged);
             if (h->nListed > 0) TLM_CU(h, cudaStreamWaitEvent(h->stream, h->evJoin, 0));
         }
         else

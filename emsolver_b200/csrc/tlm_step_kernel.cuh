@@ -185,23 +185,24 @@ template <int V> __device__ __forceinline__ unsigned pecMask(const uint8_t (&m)[
     return r;
 }
 
-// Shared-memory stage of one tile of kBlock node pairs (storage S: FP32,
-// FP16 or BF16), filled by bulk copies (stepKernelStaged): slots 0..3 at the
-// tile's own nodes with 16 bytes of halo on each side (the x neighbours),
-// then the eight y/z neighbour segments in the order of inc[4..11] (slot 6+t
-// one row below, 4+t one row above, 10+t one plane below, 8+t one plane
-// above), the three FP32 stub planes, and the material bytes. Offsets in
-// bytes; every segment starts and ends on a 16-byte boundary.
-constexpr int kStageNodes = kBlock * 2;
-template <class S> struct Stage
+// Shared-memory stage of one tile of kBlock x V nodes (storage S: FP32 with
+// V = 2, FP16 or BF16 with V = 4), filled by bulk copies
+// (stepKernelStaged): slots 0..3 at the tile's own nodes with 16 bytes of
+// halo on each side (the x neighbours), then the eight y/z neighbour
+// segments in the order of inc[4..11] (slot 6+t one row below, 4+t one row
+// above, 10+t one plane below, 8+t one plane above), the three FP32 stub
+// planes, and the material bytes. Offsets in bytes; every segment starts and
+// ends on a 16-byte boundary.
+template <class S, int V = 2> struct Stage
 {
+    static constexpr int kNodes = kBlock * V;
     static constexpr int kElem = (int)sizeof(S);
     static constexpr int kHalo = 16 / kElem;                // nodes of x halo on each side
-    static constexpr int kSegX = kStageNodes + 2 * kHalo;   // elements of an x segment
+    static constexpr int kSegX = kNodes + 2 * kHalo;        // elements of an x segment
     static constexpr int kOffYZ = 4 * kSegX * kElem;
-    static constexpr int kOffStub = kOffYZ + 8 * kStageNodes * kElem;
-    static constexpr int kOffMat = kOffStub + 3 * kStageNodes * 4;
-    static constexpr int kBytes = kOffMat + kStageNodes;
+    static constexpr int kOffStub = kOffYZ + 8 * kNodes * kElem;
+    static constexpr int kOffMat = kOffStub + 3 * kNodes * 4;
+    static constexpr int kBytes = kOffMat + kNodes;
     static_assert(kBytes % 16 == 0 && (kSegX * kElem) % 16 == 0 && kOffYZ % 16 == 0 && kOffStub % 16 == 0,
                   "bulk copies need 16-byte multiples");
 };
@@ -293,17 +294,17 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     R prevX[2], nextX[2];
     if constexpr (kStaged)
     {
-        static_assert(V == 2 && (std::is_same<S, float>::value || std::is_same<S, __half>::value ||
-                                 std::is_same<S, __nv_bfloat16>::value),
-                      "staged tiles hold node pairs of FP32, FP16 or BF16");
-        using L = Stage<S>;
+        static_assert((V == 2 || V == 4) && (std::is_same<S, float>::value || std::is_same<S, __half>::value ||
+                                             std::is_same<S, __nv_bfloat16>::value),
+                      "staged tiles hold 2 or 4 nodes per thread of FP32, FP16 or BF16");
+        using L = Stage<S, V>;
         const S *X = reinterpret_cast<const S *>(sm);
         const S *YZ = reinterpret_cast<const S *>(sm + L::kOffYZ);
         const int l = threadIdx.x * V;
 #pragma unroll
         for (int s = 0; s < 4; ++s) loadVec<S, V, true>(X + s * L::kSegX + L::kHalo, l, ox[s], a.scale);
 #pragma unroll
-        for (int g = 0; g < 8; ++g) loadVec<S, V, true>(YZ + g * kStageNodes, l, inc[4 + g], a.scale);
+        for (int g = 0; g < 8; ++g) loadVec<S, V, true>(YZ + g * L::kNodes, l, inc[4 + g], a.scale);
 #pragma unroll
         for (int t = 0; t < 2; ++t)
         {
@@ -440,7 +441,7 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
         if constexpr (kStaged)
         {
 #pragma unroll
-            for (int c = 0; c < V; ++c) m[c] = sm[Stage<S>::kOffMat + threadIdx.x * V + c];
+            for (int c = 0; c < V; ++c) m[c] = sm[Stage<S, V>::kOffMat + threadIdx.x * V + c];
         }
         else
             loadMat<V>(a.mat, node0, m);
@@ -462,8 +463,8 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
         {
             Pack<R, V> p;
             if constexpr (kStaged)
-                p = *reinterpret_cast<const Pack<R, V> *>(reinterpret_cast<const float *>(sm + Stage<S>::kOffStub) +
-                                                          jj * kStageNodes + threadIdx.x * V);
+                p = *reinterpret_cast<const Pack<R, V> *>(reinterpret_cast<const float *>(sm + Stage<S, V>::kOffStub) +
+                                                          jj * Stage<S, V>::kNodes + threadIdx.x * V);
             else
                 p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
 #pragma unroll
@@ -1113,8 +1114,8 @@ __host__ __device__ __forceinline__ int packStagedEntry(int tile, unsigned flags
 {
     return (int)((unsigned)tile | (flags << kEntryTileBits));
 }
-__device__ __forceinline__ int entryTile(int e) { return e & ((1 << kEntryTileBits) - 1); }
-__device__ __forceinline__ unsigned entryFlags(int e) { return (unsigned)e >> kEntryTileBits; }
+__host__ __device__ __forceinline__ int entryTile(int e) { return e & ((1 << kEntryTileBits) - 1); }
+__host__ __device__ __forceinline__ unsigned entryFlags(int e) { return (unsigned)e >> kEntryTileBits; }
 
 // The pieces of stage segment g (inc[4 + g]) for the tile at node0, as
 // (tile offset, nodes, source element) runs: a node on the segment's outer
@@ -1123,7 +1124,7 @@ __device__ __forceinline__ unsigned entryFlags(int e) { return (unsigned)e >> kE
 // in both places are merged, so a tile away from the outer faces has one run
 // per segment. Rows (y) and planes (z) hold multiples of 8 nodes, so every
 // run starts and ends on a 16-byte boundary.
-template <class S, class F>
+template <class S, int V, class F>
 __device__ __forceinline__ void stageRuns(const StageSrc<S> &a, long long node0, int g, F &&emit)
 {
     const bool zAxis = g >= 4, hi = ((g >> 1) & 1) != 0;
@@ -1132,10 +1133,10 @@ __device__ __forceinline__ void stageRuns(const StageSrc<S> &a, long long node0,
     const int faceSlot = (zAxis ? 8 : 4) + (hi ? 2 : 0) + t;
     const int nbSlot = (zAxis ? 8 : 4) + (hi ? 0 : 2) + t;
     const long long shift = zAxis ? (hi ? sz : -sz) : (hi ? sy : -sy);
-    const long long end = node0 + kStageNodes;
+    const long long end = node0 + Stage<S, V>::kNodes;
     // row and plane of the first node (two multiply-high divisions), then
     // rows (y) or planes (z) one after the other
-    const unsigned row0 = fastDiv((unsigned)(node0 >> 1), a.div_nq);
+    const unsigned row0 = fastDiv((unsigned)(node0 / V), a.div_nq);
     const unsigned k0 = fastDiv(row0, a.div_ny);
     long long row = row0;
     int j = (int)(row0 - k0 * (unsigned)a.ny), k = (int)k0;
@@ -1179,23 +1180,24 @@ __device__ __forceinline__ void stageRuns(const StageSrc<S> &a, long long node0,
 // outer-face nodes lanes 0-3 copy the x segments, lanes 4-11 assemble one y/z
 // segment each from its runs, lanes 12-14 copy the stubs and lane 15 the
 // material.
-template <class S>
+template <int V = 2, class S>
 __device__ __forceinline__ void stageTile(const StageSrc<S> &a, int tile, unsigned flags, unsigned st, unsigned bar,
                                           int lane)
 {
-    using L = Stage<S>;
+    using L = Stage<S, V>;
     constexpr unsigned E = L::kElem;
-    const long long node0 = (long long)tile * kStageNodes;
+    constexpr int kNodes = L::kNodes;
+    const long long node0 = (long long)tile * kNodes;
     const long long P = a.P;
     const bool diel = (flags & kTileDiel) != 0 && a.stub != nullptr;
     // x segments: the tile and L::kHalo nodes on each side, clipped to the planes
-    const long long x0 = max(node0 - L::kHalo, 0LL), x1 = min(node0 + kStageNodes + L::kHalo, P);
+    const long long x0 = max(node0 - L::kHalo, 0LL), x1 = min(node0 + kNodes + L::kHalo, P);
     const unsigned segX = L::kSegX * E, xOff = (unsigned)(x0 - (node0 - L::kHalo)) * E;
-    const unsigned xBytes = (unsigned)(x1 - x0) * E, seg = kStageNodes * E, stubSeg = kStageNodes * 4;
+    const unsigned xBytes = (unsigned)(x1 - x0) * E, seg = kNodes * E, stubSeg = kNodes * 4;
     const bool edge = (flags & kTileEdge) != 0;
     if (lane == 0)
     {
-        const unsigned bytes = 4 * xBytes + 8 * seg + (diel ? 3 * stubSeg : 0) + kStageNodes;
+        const unsigned bytes = 4 * xBytes + 8 * seg + (diel ? 3 * stubSeg : 0) + kNodes;
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" : : "r"(bar), "r"(bytes) : "memory");
         if (!edge)
         {
@@ -1217,7 +1219,7 @@ __device__ __forceinline__ void stageTile(const StageSrc<S> &a, int tile, unsign
                 for (int jj = 0; jj < 3; ++jj)
                     bulkCopy(st + L::kOffStub + jj * stubSeg, a.stub + jj * P + node0, stubSeg, bar);
             }
-            bulkCopy(st + L::kOffMat, a.mat + node0, kStageNodes, bar);
+            bulkCopy(st + L::kOffMat, a.mat + node0, kNodes, bar);
         }
     }
     if (!edge) return;
@@ -1228,7 +1230,7 @@ __device__ __forceinline__ void stageTile(const StageSrc<S> &a, int tile, unsign
     {
         const int g = lane - 4;
         const unsigned dst = st + L::kOffYZ + g * seg;
-        stageRuns(a, node0, g, [&](int off, int len, long long src) {
+        stageRuns<S, V>(a, node0, g, [&](int off, int len, long long src) {
             bulkCopy(dst + (unsigned)off * E, a.in + src, (unsigned)len * E, bar);
         });
     }
@@ -1237,7 +1239,7 @@ __device__ __forceinline__ void stageTile(const StageSrc<S> &a, int tile, unsign
         if (diel) bulkCopy(st + L::kOffStub + (lane - 12) * stubSeg, a.stub + (lane - 12) * P + node0, stubSeg, bar);
     }
     else if (lane == 15)
-        bulkCopy(st + L::kOffMat, a.mat + node0, kStageNodes, bar);
+        bulkCopy(st + L::kOffMat, a.mat + node0, kNodes, bar);
 }
 
 // The producer's view of a staged tile list: lane l holds entries it0 + l
@@ -1277,8 +1279,8 @@ template <class S, int V, int STAGES = kStages, int MINB = 2>
 __global__ void __launch_bounds__(kStagedThreads, MINB)
     stepKernelStaged(const StepArgs<S> a, const int *__restrict__ tiles, int ntiles)
 {
-    constexpr int kBytes = Stage<S>::kBytes;
-    static_assert(V == 2, "a stage holds kBlock node pairs");
+    constexpr int kBytes = Stage<S, V>::kBytes;
+    static_assert(V == 2 || V == 4, "a stage holds kBlock x 2 or kBlock x 4 nodes");
     extern __shared__ __align__(128) unsigned char stage[];
     __shared__ double red[STAGES][kBlock / 32];
     __shared__ __align__(8) unsigned long long full[STAGES], empty[STAGES], ered[STAGES];
@@ -1317,7 +1319,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
                 if (lane == 0 && a.fault) atomicOr(a.fault, kStageTimeout);
                 break;
             }
-            stageTile(src, entryTile(e), entryFlags(e), st0 + s * kBytes, full0 + 8 * s, lane);
+            stageTile<V>(src, entryTile(e), entryFlags(e), st0 + s * kBytes, full0 + 8 * s, lane);
             issued = i + 1;
         }
         // the copies of the last STAGES tiles may still be landing: stay

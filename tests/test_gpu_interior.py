@@ -40,11 +40,13 @@ def pair_variant(storage):
     raise AssertionError("no 2-node shape")
 
 
-@pytest.mark.parametrize("storage", [Storage.F32])
+@pytest.mark.parametrize("storage,rounding", [(Storage.F32, 0), (Storage.F16, 0), (Storage.BF16, 0),
+                                              (Storage.F16, 1)])
 @pytest.mark.parametrize("case", ["heterogeneous", "mid", "air_odd"])
-def test_staged_tiles_equal_direct_loads(built, case, storage):
-    """Staged interior tiles against the same tiles loading directly: pulses,
-    stubs and every record (energy included) bitwise."""
+def test_staged_tiles_equal_direct_loads(built, case, storage, rounding):
+    """Staged interior tiles (FP32: 2 nodes per thread; FP16/BF16: 4) against
+    the same tiles loading directly: pulses, stubs and every record (energy
+    included) bitwise, with round-to-nearest and stochastic 16-bit stores."""
     if case == "heterogeneous":
         w = workloads.heterogeneous(n=96, steps=48)
     elif case == "mid":
@@ -53,9 +55,10 @@ def test_staged_tiles_equal_direct_loads(built, case, storage):
         w = workloads.dipole(61, 70, 33, 20, slab=(3, 12, 4.0), steps=40, name="odd")
     assert staged_tiles(w) > 0
     out = []
-    v = pair_variant(storage)
+    v = pair_variant(storage) if storage == Storage.F32 else 0   # the staged shapes
     for no_staging in (True, False):
-        s = build_solver(w, storage=storage, kernel_variant=v, no_staging=no_staging)
+        s = build_solver(w, storage=storage, kernel_variant=v, no_staging=no_staging, rounding=rounding,
+                         pulse_scale=2.0 ** -10 if storage != Storage.F32 else 0.0)
         s.step(w.steps)
         out.append((s.pulses(), s.stubs() if w.table else None, records(s, w, f64=True)))
         s.close()
