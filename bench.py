@@ -71,6 +71,8 @@ def parse():
                    help="served: storage of the stream's 16-bit half")
     p.add_argument("--energy-steps", type=int, default=3000, help="energy: steps per mode")
     p.add_argument("--chunk", type=int, default=32, help="batched: instances set up per window")
+    p.add_argument("--host-threads", type=int, default=8,
+                   help="batched: host threads that set up, read back and free the instances")
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "f64", "bfp16"])
     p.add_argument("--steps-per-launch", type=int, default=0)
     p.add_argument("--kernel-variant", type=int, default=0,
@@ -716,9 +718,12 @@ def run_batched(args):
         for s in tsolvers:
             s.close()
     # all instances attached at once: set-up, the device time of the whole
-    # run, read-back
+    # run, read-back; handles are independent (a stream each, a thread-safe
+    # device pool), so the host work is spread over --host-threads threads
+    from concurrent.futures import ThreadPoolExecutor
+    pool = ThreadPoolExecutor(max_workers=max(1, args.host_threads))
     t0 = time.perf_counter()
-    solvers = [build_solver(w) for w in ws]
+    solvers = list(pool.map(build_solver, ws))
     tb = time.perf_counter()
     b = Batch()
     for s in solvers:
@@ -733,13 +738,13 @@ def run_batched(args):
     e1.record(ext)
     torch.cuda.synchronize()
     gpu_ms = e0.elapsed_time(e1)
-    got = [s.portDft(0) for s in solvers]
+    got = list(pool.map(lambda s: s.portDft(0), solvers))
     t2 = time.perf_counter()
     b.close()
     nbox = sum(box_nodes(s) for s in solvers)
-    for s in solvers:
-        s.close()
+    list(pool.map(lambda s: s.close(), solvers))
     t3 = time.perf_counter()
+    pool.shutdown()
     batched_s = t3 - t0
     # accuracy: S11 of every instance against the FP64 storage mode
     ref = batch_dfts(ws, 3, 0)
@@ -758,6 +763,7 @@ def run_batched(args):
         "config": {"workload": f"batched: {len(ws)} dipole instances, edges U{{24..96}}, 1000 steps",
                    "nodes": nodes, "storage": args.storage, "near_field": nf,
                    "tuning": tuning.__dict__, "autotuned": not args.no_autotune,
+                   "host_threads": args.host_threads,
                    "includes": "setup of every instance, all steps, port DFT read-back, free"},
         "sequential_plain_gpu": {"value": len(ws) / sum(seq), "unit": "solves/s",
                                  "seconds": sum(seq), "p50_s": float(np.percentile(seq, 50)),
