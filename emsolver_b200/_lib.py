@@ -104,7 +104,8 @@ class EmsimCaptureC(C.Structure):
 
 class BatchTuningC(C.Structure):
     _fields_ = [("kernel_variant", C.c_int), ("steps_per_launch", C.c_int),
-                ("blocks_per_sm", C.c_int), ("use_graphs", C.c_int), ("ms_per_step", C.c_double)]
+                ("blocks_per_sm", C.c_int), ("use_graphs", C.c_int), ("overlap", C.c_int),
+                ("ms_per_step", C.c_double)]
 
 
 class RequestC(C.Structure):

@@ -21,17 +21,18 @@ class BatchTuning:
     steps_per_launch: int = 64
     blocks_per_sm: int = 0
     use_graphs: bool = True
+    overlap: bool = False
     ms_per_step: float = 0.0
 
     def to_c(self):
         return _lib.BatchTuningC(int(self.kernel_variant), int(self.steps_per_launch),
                                  int(self.blocks_per_sm), 1 if self.use_graphs else 0,
-                                 float(self.ms_per_step))
+                                 1 if self.overlap else 0, float(self.ms_per_step))
 
     @classmethod
     def from_c(cls, c):
         return cls(c.kernel_variant, c.steps_per_launch, c.blocks_per_sm, bool(c.use_graphs),
-                   c.ms_per_step)
+                   bool(c.overlap), c.ms_per_step)
 
 
 class Batch:

@@ -70,6 +70,9 @@ struct tlm_batch_s
     int window = 64;
     bool useGraph = true;
     int blocksPerSm = 0;         // 0: as many as resident
+    bool overlap = false;        // general tiles beside the staged ones (FP32 staged groups)
+    cudaStream_t side = nullptr; // the general tiles' stream when they overlap
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     bool stagedAttr = false;     // shared-memory size of the staged kernel set on this device
     std::map<int, Group> groups;
     unsigned *dFault = nullptr;
@@ -318,8 +321,27 @@ tlm_status launchGroupStep(tlm_batch_s *b, Group &g, int i, bool doLaunch)
         }
     }
     if (!doLaunch) return TLM_OK;
-    // the other tiles first, at full occupancy (beside the staged kernel, with
-    // the one block per SM that fits next to it, they measured 1.6x slower)
+    if constexpr (kStagedShape)
+    {
+        if (staged && b->overlap)
+        {
+            // the staged tiles on the batch stream (two blocks per SM), the
+            // other tiles beside them on the side stream, one block per SM
+            // (what fits next to two staged blocks: 2 x 9 warps x 80
+            // registers + 8 warps x 64), between a fork and a join; both
+            // read the step's input planes and write disjoint tiles
+            TLM_BCU(b, cudaEventRecord(b->evFork, b->stream));
+            TLM_BCU(b, cudaStreamWaitEvent(b->side, b->evFork, 0));
+            tlmk::batchStepKernelStaged<><<<2 * b->smCount, tlmk::kStagedThreads, kSmem, b->stream>>>(
+                static_cast<const MemberDesc<float> *>(g.dMembers), g.dStaged, g.dNStaged, i, b->dFault, -0.0f);
+            tlmk::batchStepKernel<S, V, MINB, SEL><<<b->smCount, kBlock, 0, b->side>>>(
+                static_cast<MemberDesc<S> *>(g.dMembers), g.dTiles, g.dNTiles, i, b->dFault);
+            TLM_BCU(b, cudaEventRecord(b->evJoin, b->side));
+            TLM_BCU(b, cudaStreamWaitEvent(b->stream, b->evJoin, 0));
+            return b->cuda(cudaGetLastError(), "batchStepKernel launch");
+        }
+    }
+    // the other tiles first, at full occupancy, then the staged ones
     tlmk::batchStepKernel<S, V, MINB, SEL><<<g.gridBlocks, kBlock, 0, b->stream>>>(
         static_cast<MemberDesc<S> *>(g.dMembers), g.dTiles, g.dNTiles, i, b->dFault);
     if constexpr (kStagedShape)
@@ -428,6 +450,7 @@ void advanceMembers(tlm_batch_s *b, int w)
         {
             const int next = std::min(h->curStep + w, std::max(h->cfg.total_steps, h->curStep));
             h->curStep = next;
+            ++h->recVersion;
             h->curBuf = next & 1;
             h->doneStep.store(next);
         }
@@ -558,7 +581,7 @@ void loadCacheFile()
     std::string key;
     tlm_batch_tuning t;
     while (f >> std::quoted(key) >> t.kernel_variant >> t.steps_per_launch >> t.blocks_per_sm >>
-           t.use_graphs >> t.ms_per_step)
+           t.use_graphs >> t.overlap >> t.ms_per_step)
         g_tuneCache[key] = t;
 }
 
@@ -569,7 +592,8 @@ void saveCacheFile()
     std::ofstream f(path);
     for (auto &kv : g_tuneCache)
         f << std::quoted(kv.first) << ' ' << kv.second.kernel_variant << ' ' << kv.second.steps_per_launch
-          << ' ' << kv.second.blocks_per_sm << ' ' << kv.second.use_graphs << ' ' << kv.second.ms_per_step
+          << ' ' << kv.second.blocks_per_sm << ' ' << kv.second.use_graphs << ' ' << kv.second.overlap << ' '
+          << kv.second.ms_per_step
           << '\n';
 }
 
@@ -578,6 +602,7 @@ tlm_status applyTuning(tlm_batch_s *b, const tlm_batch_tuning &t)
     b->window = t.steps_per_launch;
     b->useGraph = t.use_graphs != 0;
     b->blocksPerSm = t.blocks_per_sm;
+    b->overlap = t.overlap != 0;
     std::map<int, Group> regrouped;
     for (auto &kv : b->groups)
         for (tlm_solver *h : kv.second.members)
@@ -632,12 +657,18 @@ tlm_status tlm_batch_create(tlm_batch *out, int device)
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
         b->smCount = sms;
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evFork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evJoin, cudaEventDisableTiming);
     // error flags: bounds checks (checked build), staged-tile waits (every build)
     if (e == cudaSuccess) e = cudaMalloc(&b->dFault, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(b->dFault, 0, sizeof(unsigned));
     if (e != cudaSuccess)
     {
         setThreadError(std::string("batch creation: ") + cudaGetErrorString(e));
+        if (b->evJoin) cudaEventDestroy(b->evJoin);
+        if (b->evFork) cudaEventDestroy(b->evFork);
+        if (b->side) cudaStreamDestroy(b->side);
         if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
         return TLM_ECUDA;
@@ -664,6 +695,10 @@ tlm_status tlm_batch_destroy(tlm_batch b)
     }
     if (b->graph) cudaGraphExecDestroy(b->graph);
     if (b->dFault) cudaFree(b->dFault);
+    cudaStreamSynchronize(b->side);
+    cudaEventDestroy(b->evJoin);
+    cudaEventDestroy(b->evFork);
+    cudaStreamDestroy(b->side);
     cudaStreamDestroy(b->stream);
     delete b;
     return TLM_OK;
@@ -838,6 +873,7 @@ tlm_status tlm_batch_get_tuning(tlm_batch b, tlm_batch_tuning *t)
     t->steps_per_launch = b->window;
     t->blocks_per_sm = b->blocksPerSm;
     t->use_graphs = b->useGraph ? 1 : 0;
+    t->overlap = b->overlap ? 1 : 0;
     t->ms_per_step = 0.0;
     return TLM_OK;
 }
@@ -886,12 +922,26 @@ tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *
         *msPerStep = ms / (t.steps_per_launch * trial_windows);
         return TLM_OK;
     };
-    // tile shapes at windows of 100 steps, then other window lengths for the best shape
-    tlm_batch_tuning best{ 0, 100, 0, 1, 1e30 };
+    // tile shapes at windows of 100 steps, then the general tiles beside the
+    // staged ones instead of before them, then other window lengths
+    tlm_batch_tuning best{ 0, 100, 0, 1, 0, 1e30 };
     tlm_status st = TLM_OK;
     for (int v = 0; v < nvar && st == TLM_OK; ++v)
     {
-        tlm_batch_tuning t{ v, 100, 0, 1, 0.0 };
+        tlm_batch_tuning t{ v, 100, 0, 1, 0, 0.0 };
+        double ms = 0.0;
+        st = trial(t, &ms);
+        if (st == TLM_OK && ms < best.ms_per_step)
+        {
+            best = t;
+            best.ms_per_step = ms;
+        }
+    }
+    // the general tiles beside the staged ones instead of before them
+    if (st == TLM_OK)
+    {
+        tlm_batch_tuning t = best;
+        t.overlap = 1;
         double ms = 0.0;
         st = trial(t, &ms);
         if (st == TLM_OK && ms < best.ms_per_step)

@@ -190,7 +190,7 @@ template <int I> __device__ __forceinline__ unsigned long long headU64(const uin
 }
 
 template <int STAGES = kStages, int MINB = 2>
-__global__ void __launch_bounds__(kStagedThreads, MINB)
+__global__ void __maxnreg__(80)
     batchStepKernelStaged(const MemberDesc<float> *__restrict__ members, const int2 *__restrict__ tiles,
                           const int *__restrict__ ntiles, int i, unsigned *fault, float negZero)
 {

@@ -125,3 +125,31 @@ void cell_of(const float origin[3], float dl, float x, float y, float z, int *i,
 }
 
 } // namespace tlmh
+
+namespace tlmh {
+// Copy n material ids and return the largest: one pass over the caller's map
+// instead of a scan and a copy. Sixteen running maxima side by side, so that
+// the compiler keeps them in one vector register (a byte-wise max per 16
+// bytes) instead of one dependent max per byte.
+__attribute__((optimize("tree-vectorize"))) uint8_t copy_max_u8(const uint8_t *__restrict src,
+                                                                 uint8_t *__restrict dst, size_t n)
+{
+    uint8_t m[16] = {};
+    size_t i = 0;
+    for (; i + 16 <= n; i += 16)
+        for (int l = 0; l < 16; ++l)
+        {
+            const uint8_t v = src[i + l];
+            dst[i + l] = v;
+            m[l] = m[l] > v ? m[l] : v;
+        }
+    uint8_t r = 0;
+    for (int l = 0; l < 16; ++l) r = r > m[l] ? r : m[l];
+    for (; i < n; ++i)
+    {
+        dst[i] = src[i];
+        r = r > src[i] ? r : src[i];
+    }
+    return r;
+}
+} // namespace tlmh

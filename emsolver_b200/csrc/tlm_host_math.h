@@ -1,6 +1,9 @@
 // tlm_host_math.h -- host scalar math that must match the reference bit for bit.
 #pragma once
 
+#include <cstddef>
+#include <cstdint>
+
 namespace tlmh {
 float eta0_f32();
 float timestep_f32(float dl);
@@ -21,4 +24,6 @@ void dft_phase_f32(float f0, float dt, int n, float *c, float *s);
 void dft_phase_f64(float f0, double dt, int n, double *c, double *s);
 double probe_scale_f64(float dl);
 void cell_of(const float origin[3], float dl, float x, float y, float z, int *i, int *j, int *k);
+// copy n bytes and return the largest
+uint8_t copy_max_u8(const uint8_t *src, uint8_t *dst, size_t n);
 } // namespace tlmh

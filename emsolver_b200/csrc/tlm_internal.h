@@ -227,6 +227,12 @@ struct tlm_solver
 
     // time-loop state
     int curStep = 0;       // steps enqueued
+    // host copies of the probe and port records, read back once after steps
+    // and served to every getter until more steps are enqueued or the state
+    // is rewound (recVersion moves then)
+    unsigned long long recVersion = 1, recHostVersion = 0;
+    int recHostSteps = 0;
+    std::vector<double> precHost, vrecHost, irecHost;
     int curBuf = 0;        // pulse buffer holding the current state
     bool stateIncident = false;
 
@@ -391,9 +397,11 @@ void freeSurface(tlm_solver *h);
 tlm_status rewindSurface(tlm_solver *h);
 bool surfaceActive(const tlm_solver *h);
 tlm_status launchSurface(tlm_solver *h, int n);
-// The library's memory pool on a device (created on first use) and the
-// bytes it could hand out: free device memory plus blocks it keeps for reuse.
+// The library's memory pool on a device (created on first use), the bytes it
+// could hand out (free device memory plus blocks it keeps for reuse), and
+// whether the blocks it keeps alone hold `bytes`.
 cudaMemPool_t devicePool(int device);
 size_t poolAvailable(int device);
+bool poolCovers(int device, size_t bytes);
 
 } // namespace tlmi

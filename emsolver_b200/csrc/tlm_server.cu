@@ -478,7 +478,7 @@ tlm_status tlm_server_create(tlm_server *out, int device, size_t hbm_budget_byte
         delete s;
         return st;
     }
-    tlm_batch_tuning t{ 0, s->window, 0, 1, 0.0 };
+    tlm_batch_tuning t{ 0, s->window, 0, 1, 0, 0.0 };
     tlm_batch_set_tuning(s->batch, &t);
     if (hbm_budget_bytes == 0)
     {

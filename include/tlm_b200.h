@@ -308,6 +308,12 @@ typedef struct tlm_batch_tuning {
     int steps_per_launch;  /* steps per window (graph) */
     int blocks_per_sm;     /* resident step-kernel blocks per SM, 0 = all that fit */
     int use_graphs;        /* 1: replay windows as CUDA graphs */
+    int overlap;           /* 1: an FP32 group's general tiles (wire, port, probes,
+                              partial tiles) step on a second stream, one block
+                              per SM, beside its staged tiles (faster when they
+                              are few: one 192^3 grid 0.156 -> 0.144 ms per
+                              step; slower for the batched dipoles, whose wire
+                              tiles are 11 %: 1.29 -> 1.58 ms); 0: before them */
     double ms_per_step;    /* autotuner: measured time per step of the batch */
 } tlm_batch_tuning;
 
@@ -332,10 +338,10 @@ TLM_API tlm_status tlm_batch_launch_window(tlm_batch b, int *n_steps);
 TLM_API tlm_status tlm_batch_sync(tlm_batch b);
 TLM_API tlm_status tlm_batch_set_tuning(tlm_batch b, const tlm_batch_tuning *t);
 TLM_API tlm_status tlm_batch_get_tuning(tlm_batch b, tlm_batch_tuning *t);
-/* Time trial_windows windows of 100 steps of every tile shape (then
- * windows of 50 and 200 steps for the best shape) on the batch's own
- * members, keep the fastest, and rewind every member to step 0 (fields
- * zero). Call before the
+/* Time trial_windows windows of 100 steps of every tile shape (then, for
+ * the best shape, the general tiles beside the staged ones instead of before
+ * them, and windows of 50 and 200 steps) on the batch's own members, keep
+ * the fastest, and rewind every member to step 0 (fields zero). Call before the
  * first step. Results are cached per (GPU, storage modes, size class), in
  * the file named by TLM_AUTOTUNE_CACHE when that variable is set. */
 TLM_API tlm_status tlm_batch_autotune(tlm_batch b, int trial_windows, tlm_batch_tuning *out);

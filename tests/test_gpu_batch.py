@@ -47,13 +47,16 @@ def assert_same(s, w, ref, energy_rtol=0.0):
     return v, i
 
 
-@pytest.mark.parametrize("graphs,window", [(True, 64), (False, 64), (True, 16), (True, 100)])
-def test_batch_members_equal_alone(built, graphs, window):
+@pytest.mark.parametrize("graphs,window,overlap", [(True, 64, False), (False, 64, False), (True, 16, False),
+                                                    (True, 100, False), (True, 64, True), (False, 64, True)])
+def test_batch_members_equal_alone(built, graphs, window, overlap):
+    """overlap: the general tiles on a second stream beside the staged ones."""
     ws = instances(7, seed=1)
     refs = [alone(w) for w in ws]
     solvers = [build_solver(w) for w in ws]
     with Batch() as b:
-        b.set_tuning(BatchTuning(0, window, 0, graphs))
+        b.set_tuning(BatchTuning(0, window, 0, graphs, overlap))
+        assert b.get_tuning().overlap == overlap
         for s in solvers:
             b.attach(s)
         assert b.size() == 7 and b.active() == 7
