@@ -327,9 +327,10 @@ static __global__ void padMaterial(const uint8_t *__restrict__ raw, int nx, int 
 // The material part of the step kernel's tile flags (tiles of T consecutive
 // padded nodes, T a multiple of 32): kTileGeneral when a node of the tile is
 // PEC or has a PEC neighbour inside the grid, kTileDiel when it holds a
-// dielectric node; padding columns count for neither. One padded node per
-// thread; the 32 nodes of a warp lie in one tile, so one lane ORs the
-// warp's flags into that tile's word.
+// dielectric node; padding columns count for neither. Bits 8 and up of a
+// tile's word count its dielectric nodes. One padded node per thread; the
+// 32 nodes of a warp lie in one tile, so one lane ORs the warp's flags into
+// that tile's word and adds its count.
 static __global__ void materialTileFlags(const uint8_t *__restrict__ mat, int nx, int ny, int nz, int px, long long T,
                                   unsigned *__restrict__ flags)
 {
@@ -354,9 +355,12 @@ static __global__ void materialTileFlags(const uint8_t *__restrict__ mat, int nx
                 if (g) f |= kTileGeneral;
             }
         }
+        const unsigned nd = __popc(__ballot_sync(0xffffffffu, (f & kTileDiel) != 0));
         f = __reduce_or_sync(0xffffffffu, f);
         const long long n0 = base + (threadIdx.x & ~31u);
         if ((threadIdx.x & 31) == 0 && f != 0 && n0 < P) atomicOr(&flags[n0 / T], f);
+        // stub-loaded nodes of the tile, counted above the flag byte
+        if ((threadIdx.x & 31) == 0 && nd != 0 && n0 < P) atomicAdd(&flags[n0 / T], nd << 8);
     }
 }
 

@@ -189,6 +189,9 @@ template <int I> __device__ __forceinline__ unsigned long long headU64(const uin
     return (unsigned long long)headWord<I>(h) | ((unsigned long long)headWord<I + 1>(h) << 32);
 }
 
+// At most 80 registers: two blocks of it and one 256-thread block of the
+// general-tile kernel (64 registers) then fit one SM's register file, which
+// the overlapped schedule (tlm_batch_tuning.overlap) needs.
 template <int STAGES = kStages, int MINB = 2>
 __global__ void __maxnreg__(80)
     batchStepKernelStaged(const MemberDesc<float> *__restrict__ members, const int2 *__restrict__ tiles,
@@ -336,7 +339,7 @@ __global__ void __maxnreg__(80)
             const unsigned ep = (eBits >> s) & 1u;
             if (a.epart != nullptr) eBits ^= 1u << s;
             stepTileInterior<float, 2, true>(a, tile, red[s], (tail1.y & kTileDiel) != 0, stage + s * kData,
-                                             ered0 + 8 * s, ep);
+                                             ered0 + 8 * s, ep, (tail1.y & kTileStubSparse) == 0);
         }
         __syncwarp();
         if ((threadIdx.x & 31) == 0)

@@ -65,7 +65,12 @@ template <class S> struct StepArgs
 // assembled from runs, see stageRuns).
 // kTileNear: the tile has nodes in the near-field box (always with
 // kTileGeneral: only the general body completes pulses with residuals).
-enum : uint8_t { kTileGeneral = 1, kTileDiel = 2, kTileEdge = 4, kTileNear = 8 };
+// kTileStubSparse: at most a quarter of the tile's nodes are stub-loaded
+// (with kTileDiel): a staged tile then leaves the three stub segments out of
+// its stage and those nodes read their stubs from the stub planes.
+enum : uint8_t { kTileGeneral = 1, kTileDiel = 2, kTileEdge = 4, kTileNear = 8, kTileStubSparse = 16 };
+// the quarter of kTileStubSparse: stub-loaded nodes x this <= nodes of a tile
+constexpr int kStubSparseDiv = 4;
 
 #ifdef TLM_CHECKED
 #define TLM_GUARD(idx, limit, code)                                                         \
@@ -269,10 +274,12 @@ __device__ __forceinline__ void bulkCopy(unsigned dst, const void *src, unsigned
 // general tile body below. kStaged: the tile's inputs are already in the
 // shared-memory stage `sm` (see Stage and stageRuns; V = 2), outer y/z faces
 // included; the arithmetic is the same.
+// stubStaged (kStaged only): the stage holds the tile's stubs; false for
+// a kTileStubSparse tile, whose stub-loaded nodes load theirs from a.stub.
 template <class S, int V, bool kStaged = false>
 __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel,
                                                  const unsigned char *sm = nullptr, unsigned eBar = 0,
-                                                 unsigned eParity = 0)
+                                                 unsigned eParity = 0, bool stubStaged = true)
 {
     using R = float;
     static_assert(V % 2 == 0, "interior tiles scatter node pairs");
@@ -287,6 +294,40 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     const long long P = a.P;
     const long long sy = a.px, sz = (long long)a.px * a.ny;
     const bool atYlo = j == 0, atYhi = j == a.ny - 1, atZlo = k == 0, atZhi = k == a.nz - 1;
+
+    // ---- stub-loaded nodes of a sparse staged tile: their stubs come from
+    // the stub planes, loaded first so that the loads overlap the rest ----
+    uint8_t m[V];
+    unsigned dielMask = 0;
+    R vs[3][V];
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj)
+    {
+#pragma unroll
+        for (int c = 0; c < V; ++c) vs[jj][c] = R(0);
+    }
+    bool stubsIn = false;  // m, dielMask and vs are set
+    if constexpr (kStaged)
+    {
+        if (diel && !stubStaged)
+        {
+#pragma unroll
+            for (int c = 0; c < V; ++c) m[c] = sm[Stage<S, V>::kOffMat + threadIdx.x * V + c];
+#pragma unroll
+            for (int c = 0; c < V; ++c) dielMask |= ((m[c] >= kDiel0) ? 1u : 0u) << c;
+            if (dielMask)
+            {
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj)
+                {
+                    const Pack<R, V> p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
+#pragma unroll
+                    for (int c = 0; c < V; ++c) vs[jj][c] = p.v[c];
+                }
+            }
+            stubsIn = true;
+        }
+    }
 
     // ---- loads: own x-slots, then the y and z neighbours' opposite faces ----
     R ox[4][V];
@@ -434,9 +475,7 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     }
 
     // ---- scatter (pairs of nodes) and store ----
-    uint8_t m[V];
-    unsigned dielMask = 0;
-    if (diel)
+    if (diel && !stubsIn)
     {
         if constexpr (kStaged)
         {
@@ -447,16 +486,9 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
             loadMat<V>(a.mat, node0, m);
 #pragma unroll
         for (int c = 0; c < V; ++c) dielMask |= ((m[c] >= kDiel0) ? 1u : 0u) << c;
-        dielMask &= liveMask;
     }
-    R vs[3][V];
-#pragma unroll
-    for (int jj = 0; jj < 3; ++jj)
-    {
-#pragma unroll
-        for (int c = 0; c < V; ++c) vs[jj][c] = R(0);
-    }
-    if (dielMask)
+    dielMask &= liveMask;
+    if (dielMask && !stubsIn)
     {
 #pragma unroll
         for (int jj = 0; jj < 3; ++jj)
@@ -1189,7 +1221,8 @@ __device__ __forceinline__ void stageTile(const StageSrc<S> &a, int tile, unsign
     constexpr int kNodes = L::kNodes;
     const long long node0 = (long long)tile * kNodes;
     const long long P = a.P;
-    const bool diel = (flags & kTileDiel) != 0 && a.stub != nullptr;
+    // stubs staged for stub-loaded tiles, unless only a few of their nodes are
+    const bool diel = (flags & kTileDiel) != 0 && (flags & kTileStubSparse) == 0 && a.stub != nullptr;
     // x segments: the tile and L::kHalo nodes on each side, clipped to the planes
     const long long x0 = max(node0 - L::kHalo, 0LL), x1 = min(node0 + kNodes + L::kHalo, P);
     const unsigned segX = L::kSegX * E, xOff = (unsigned)(x0 - (node0 - L::kHalo)) * E;
@@ -1344,8 +1377,9 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         // from a copy the producer left in shared memory.
         const int e = tiles[blockIdx.x + i * gridDim.x];
         const int tile = entryTile(e);
-        stepTileInterior<S, V, true>(a, tile, red[s], (a.tile_flags[tile] & kTileDiel) != 0, stage + s * kBytes,
-                                      ered0 + 8 * s, (unsigned)(i / STAGES) & 1u);
+        const uint8_t tf = a.tile_flags[tile];
+        stepTileInterior<S, V, true>(a, tile, red[s], (tf & kTileDiel) != 0, stage + s * kBytes,
+                                      ered0 + 8 * s, (unsigned)(i / STAGES) & 1u, (tf & kTileStubSparse) == 0);
         __syncwarp();
         if ((threadIdx.x & 31) == 0)
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(empty0 + 8 * s) : "memory");

@@ -113,6 +113,25 @@ def staged_tiles(w, block=256):
     return int((~_general_mask(w, 2, block)).sum())
 
 
+def stub_tile_counts(w, block=256):
+    """(sparse, dense): FP32 staged tiles (2 nodes per thread) with
+    stub-loaded nodes, split by the kernel's rule: sparse when at most a
+    quarter of the tile's nodes are stub-loaded (their stubs are loaded
+    directly instead of staged)."""
+    nx, ny, nz = w.nx, w.ny, w.nz
+    px = (nx + 7) // 8 * 8
+    T = block * 2
+    mat = np.full((nz, ny, px), 1, np.uint8)
+    mat[:, :, :nx] = np.asarray(w.mat).reshape(nz, ny, nx)
+    diel = (mat >= 2).reshape(-1)
+    nb = (diel.size // 2 + block - 1) // block
+    cnt = np.bincount(np.arange(diel.size) // T, weights=diel, minlength=nb)[:nb]
+    staged = ~_general_mask(w, 2, block)
+    sparse = staged & (cnt > 0) & (cnt * 4 <= T)
+    dense = staged & (cnt * 4 > T)
+    return int(sparse.sum()), int(dense.sum())
+
+
 def _general_mask(w, V, block):
     """Per tile of `block` threads x V nodes: True when the tile is general."""
     nx, ny, nz = w.nx, w.ny, w.nz

@@ -15,7 +15,7 @@ from emsolver_b200.runner import build_solver, records
 from emsolver_b200.solver import Storage
 from oracle import Oracle, drive
 from emsolver_b200 import workloads
-from tests.golden.cases import interior_tiles, mid_cases, staged_tiles
+from tests.golden.cases import interior_tiles, mid_cases, staged_tiles, stub_tile_counts
 
 pytestmark = pytest.mark.gpu
 
@@ -52,7 +52,7 @@ def test_staged_tiles_equal_direct_loads(built, case, storage, rounding):
     elif case == "mid":
         w = MID[0]
     else:
-        w = workloads.dipole(61, 70, 33, 20, slab=(3, 12, 4.0), steps=40, name="odd")
+        w = slab_dipole()
     assert staged_tiles(w) > 0
     out = []
     v = pair_variant(storage) if storage == Storage.F32 else 0   # the staged shapes
@@ -68,6 +68,38 @@ def test_staged_tiles_equal_direct_loads(built, case, storage, rounding):
         assert np.array_equal(sa, sb)
     for k in ra:
         assert np.array_equal(ra[k], rb[k]), k
+
+
+def slab_dipole():
+    """A dipole beside a thin dielectric slab (9 of 61 nodes of every row):
+    staged tiles whose few stub-loaded nodes load their stubs directly."""
+    return workloads.dipole(61, 70, 33, 20, slab=(3, 12, 4.0), steps=40, name="odd")
+
+
+def test_cases_hold_sparse_and_dense_stub_tiles():
+    sparse, dense = stub_tile_counts(slab_dipole())
+    assert sparse > 0
+    sparse, dense = stub_tile_counts(workloads.heterogeneous(n=96, steps=48))
+    assert sparse > 0 and dense > 0
+
+
+def test_sparse_stub_tiles_bitwise_vs_oracle(built):
+    """Staged tiles with stubs loaded directly (kTileStubSparse) and staged
+    (the dense ones), FP32: pulses, stubs and records bitwise the oracle."""
+    for w in (slab_dipole(), workloads.heterogeneous(n=64, steps=30)):
+        assert stub_tile_counts(w)[0] > 0
+        s = build_solver(w, kernel_variant=pair_variant(Storage.F32))
+        s.step(w.steps)
+        O = Oracle(False)
+        drive.setup(O, w)
+        drive.advance(O, w, w.steps)
+        assert np.array_equal(s.pulses(), O.pulses()), w.name
+        assert np.array_equal(s.stubs(), O.stubs()), w.name
+        ra, ro = records(s, w), drive.records(O, w)
+        for k in ra:
+            if not k.startswith("energy"):
+                assert np.array_equal(ra[k], ro[k]), (w.name, k)
+        s.close()
 
 
 @pytest.mark.parametrize("w", MID, ids=[w.name for w in MID])
