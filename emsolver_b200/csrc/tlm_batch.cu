@@ -326,10 +326,9 @@ tlm_status launchGroupStep(tlm_batch_s *b, Group &g, int i, bool doLaunch)
         if (staged && b->overlap)
         {
             // the staged tiles on the batch stream (two blocks per SM), the
-            // other tiles beside them on the side stream, one block per SM
-            // (what fits next to two staged blocks: 2 x 9 warps x 80
-            // registers + 8 warps x 64), between a fork and a join; both
-            // read the step's input planes and write disjoint tiles
+            // other tiles beside them on the side stream, one block per SM,
+            // between a fork and a join; both read the step's input planes
+            // and write disjoint tiles
             TLM_BCU(b, cudaEventRecord(b->evFork, b->stream));
             TLM_BCU(b, cudaStreamWaitEvent(b->side, b->evFork, 0));
             tlmk::batchStepKernelStaged<><<<2 * b->smCount, tlmk::kStagedThreads, kSmem, b->stream>>>(

@@ -189,11 +189,8 @@ template <int I> __device__ __forceinline__ unsigned long long headU64(const uin
     return (unsigned long long)headWord<I>(h) | ((unsigned long long)headWord<I + 1>(h) << 32);
 }
 
-// At most 80 registers: two blocks of it and one 256-thread block of the
-// general-tile kernel (64 registers) then fit one SM's register file, which
-// the overlapped schedule (tlm_batch_tuning.overlap) needs.
 template <int STAGES = kStages, int MINB = 2>
-__global__ void __maxnreg__(80)
+__global__ void __launch_bounds__(kStagedThreads, MINB)
     batchStepKernelStaged(const MemberDesc<float> *__restrict__ members, const int2 *__restrict__ tiles,
                           const int *__restrict__ ntiles, int i, unsigned *fault, float negZero)
 {

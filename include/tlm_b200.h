@@ -310,10 +310,11 @@ typedef struct tlm_batch_tuning {
     int use_graphs;        /* 1: replay windows as CUDA graphs */
     int overlap;           /* 1: an FP32 group's general tiles (wire, port, probes,
                               partial tiles) step on a second stream, one block
-                              per SM, beside its staged tiles (faster when they
-                              are few: one 192^3 grid 0.156 -> 0.144 ms per
-                              step; slower for the batched dipoles, whose wire
-                              tiles are 11 %: 1.29 -> 1.58 ms); 0: before them */
+                              per SM, beside its staged tiles; 0: before them.
+                              Measured on B200: equal or up to 8 % faster for a
+                              batch of one 192^3 grid, whose general tiles are
+                              few; 1.24 -> 1.63 ms per step for the batched
+                              dipoles, whose wire tiles are 11 % */
     double ms_per_step;    /* autotuner: measured time per step of the batch */
 } tlm_batch_tuning;
 
