@@ -136,3 +136,42 @@ def test_energy_drift_of_a_closed_lossless_grid(built):
         k0 = int(np.searchsorted(st, 512))
         assert ev[k0] > 0
         assert np.max(np.abs(ev[k0:] - ev[k0])) <= bound * ev[k0], storage
+
+
+def test_records_read_between_steps_follow_the_state(built):
+    """Probe and port records are read back once per step count and served
+    from the host until more steps run: reads between steps, and reads after
+    the same handle is set up again and stepped to the same step count, give
+    the records of the state at that moment."""
+    w = small_dipole(200)
+    ref = build_solver(w)
+    ref.step(200)
+    full = records(ref, w)
+    s = build_solver(w)
+    for n in (37, 63, 100):
+        s.step(n)
+        got = records(s, w)
+        for k in got:
+            if not k.startswith("energy"):
+                assert np.array_equal(got[k], full[k][:s.currentStep()]), (k, s.currentStep())
+    # the same handle set up again with another source amplitude, stepped to
+    # a step count its records were last read at
+    w2 = small_dipole(200)
+    w2.ports[0] = (w2.ports[0][0], w2.ports[0][1], 0.5)
+    ref2 = build_solver(w2)
+    ref2.step(100)
+    s.step(0)
+    before = records(s, w)
+    grid = VoxelGridSpec(w2.nx, w2.ny, w2.nz, tuple(w2.origin), w2.dl)
+    cfg = TlmConfig(f0=w2.f0, waveform=w2.waveform, totalSteps=w2.steps, boundaryRho=w2.rho)
+    s.setup(grid, w2.mat, [MatProps(e, g) for e, g in w2.table], cfg)
+    for cells, pol, amp in w2.ports:
+        s.addPort(cells, pol, amp)
+    for (i, j, k) in w2.probes_cell:
+        s.addProbe(w2.cell_center(i, j, k))
+    s.step(100)
+    got, want = records(s, w2), records(ref2, w2)
+    for k in got:
+        if not k.startswith("energy"):
+            assert np.array_equal(got[k], want[k]), k
+            assert not np.array_equal(got[k], before[k][:100]) or not np.any(want[k]), k
