@@ -232,7 +232,8 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
 #pragma unroll
             for (int q = 0; q < 8; ++q) h[q] = __ldg(hp + q);
             bool ok = true;
-            if (it >= STAGES && lane == 0) ok = mbarWaitBounded(empty0 + 8 * s, (unsigned)(it / STAGES - 1) & 1u);
+            if (it >= STAGES && lane == 0)
+                ok = mbarWaitPaused<0>(empty0 + 8 * s, (unsigned)(it / STAGES - 1) & 1u);
             if (!__shfl_sync(0xffffffffu, ok, 0))
             {
                 if (lane == 0 && fault) atomicOr(fault, kStageTimeout);
@@ -335,8 +336,11 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             a.near = NearBox{};
             const unsigned ep = (eBits >> s) & 1u;
             if (a.epart != nullptr) eBits ^= 1u << s;
-            stepTileInterior<float, 2, true>(a, tile, red[s], (tail1.y & kTileDiel) != 0, stage + s * kData,
-                                             ered0 + 8 * s, ep, (tail1.y & kTileStubSparse) == 0);
+            if (tail1.y & kTileStubSparse)
+                stepTileInterior<float, 2, true, true>(a, tile, red[s], true, stage + s * kData, ered0 + 8 * s, ep);
+            else
+                stepTileInterior<float, 2, true>(a, tile, red[s], (tail1.y & kTileDiel) != 0, stage + s * kData,
+                                                 ered0 + 8 * s, ep);
         }
         __syncwarp();
         if ((threadIdx.x & 31) == 0)

@@ -257,6 +257,35 @@ __device__ __forceinline__ bool mbarWaitBounded(unsigned bar, unsigned parity,
     }
 }
 
+// Sparse-stub tiles (kTileStubSparse) skip staging their stubs in FP32 only:
+// in the 16-bit staged kernel (4 nodes per thread, 96 registers) the second
+// instantiation of the tile body spilled and the 384x384x256 dipole with the
+// near-field box stepped in 0.392 ms against 0.347, so there every
+// stub-loaded tile stages its stubs.
+template <class S> constexpr bool kSparseStubs = std::is_same<S, float>::value;
+
+// The producer's wait for a free stage: the same bounded wait, with a pause
+// of about PAUSE_NS between polls, so that a producer waiting on its
+// consumers does not take their issue slots with a tight polling loop.
+template <unsigned PAUSE_NS>
+__device__ __forceinline__ bool mbarWaitPaused(unsigned bar, unsigned parity,
+                                               unsigned long long limitNs = kStageWaitNs)
+{
+    if (mbarTestWait(bar, parity)) return true;
+    if (limitNs == 0) return false;
+    const unsigned long long t0 = globalTimerNs();
+    for (unsigned it = 1;; ++it)
+    {
+        if (PAUSE_NS > 0) __nanosleep(PAUSE_NS);
+        if (mbarTestWait(bar, parity)) return true;
+        if ((it & 15u) == 0 && globalTimerNs() - t0 > limitNs) return false;
+    }
+}
+// FP32 single grid: 512 ns (192^3 heterogeneous 127.9 -> 126.7 us per step,
+// the 384x384x256 dipole 567 -> 571 us); the 16-bit and batch producers poll
+// without a pause (with 512 ns the dipole in FP16 stepped 5 % slower).
+constexpr unsigned kProducerPauseNs = 512;
+
 __device__ __forceinline__ void bulkCopy(unsigned dst, const void *src, unsigned bytes, unsigned bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
@@ -274,12 +303,13 @@ __device__ __forceinline__ void bulkCopy(unsigned dst, const void *src, unsigned
 // general tile body below. kStaged: the tile's inputs are already in the
 // shared-memory stage `sm` (see Stage and stageRuns; V = 2), outer y/z faces
 // included; the arithmetic is the same.
-// stubStaged (kStaged only): the stage holds the tile's stubs; false for
-// a kTileStubSparse tile, whose stub-loaded nodes load theirs from a.stub.
-template <class S, int V, bool kStaged = false>
+// kSparse (kStaged only): a kTileStubSparse tile, whose stage holds no
+// stubs; its stub-loaded nodes load theirs from a.stub first thing (a
+// separate instantiation, so the other tiles keep the code they had).
+template <class S, int V, bool kStaged = false, bool kSparse = false>
 __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel,
                                                  const unsigned char *sm = nullptr, unsigned eBar = 0,
-                                                 unsigned eParity = 0, bool stubStaged = true)
+                                                 unsigned eParity = 0)
 {
     using R = float;
     static_assert(V % 2 == 0, "interior tiles scatter node pairs");
@@ -297,35 +327,31 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
 
     // ---- stub-loaded nodes of a sparse staged tile: their stubs come from
     // the stub planes, loaded first so that the loads overlap the rest ----
-    uint8_t m[V];
-    unsigned dielMask = 0;
-    R vs[3][V];
-#pragma unroll
-    for (int jj = 0; jj < 3; ++jj)
+    static_assert(kStaged || !kSparse, "sparse-stub tiles are staged tiles");
+    uint8_t mS[V];
+    unsigned dielS = 0;
+    R vsS[3][V];
+    if constexpr (kSparse)
     {
 #pragma unroll
-        for (int c = 0; c < V; ++c) vs[jj][c] = R(0);
-    }
-    bool stubsIn = false;  // m, dielMask and vs are set
-    if constexpr (kStaged)
-    {
-        if (diel && !stubStaged)
+        for (int c = 0; c < V; ++c) mS[c] = sm[Stage<S, V>::kOffMat + threadIdx.x * V + c];
+#pragma unroll
+        for (int c = 0; c < V; ++c) dielS |= ((mS[c] >= kDiel0) ? 1u : 0u) << c;
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj)
         {
 #pragma unroll
-            for (int c = 0; c < V; ++c) m[c] = sm[Stage<S, V>::kOffMat + threadIdx.x * V + c];
+            for (int c = 0; c < V; ++c) vsS[jj][c] = R(0);
+        }
+        if (dielS)
+        {
 #pragma unroll
-            for (int c = 0; c < V; ++c) dielMask |= ((m[c] >= kDiel0) ? 1u : 0u) << c;
-            if (dielMask)
+            for (int jj = 0; jj < 3; ++jj)
             {
+                const Pack<R, V> p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
 #pragma unroll
-                for (int jj = 0; jj < 3; ++jj)
-                {
-                    const Pack<R, V> p = *reinterpret_cast<const Pack<R, V> *>(a.stub + jj * P + node0);
-#pragma unroll
-                    for (int c = 0; c < V; ++c) vs[jj][c] = p.v[c];
-                }
+                for (int c = 0; c < V; ++c) vsS[jj][c] = p.v[c];
             }
-            stubsIn = true;
         }
     }
 
@@ -475,7 +501,15 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
     }
 
     // ---- scatter (pairs of nodes) and store ----
-    if (diel && !stubsIn)
+    uint8_t m[V];
+    unsigned dielMask = 0;
+    if constexpr (kSparse)
+    {
+#pragma unroll
+        for (int c = 0; c < V; ++c) m[c] = mS[c];
+        dielMask = dielS & liveMask;
+    }
+    else if (diel)
     {
         if constexpr (kStaged)
         {
@@ -486,9 +520,16 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
             loadMat<V>(a.mat, node0, m);
 #pragma unroll
         for (int c = 0; c < V; ++c) dielMask |= ((m[c] >= kDiel0) ? 1u : 0u) << c;
+        dielMask &= liveMask;
     }
-    dielMask &= liveMask;
-    if (dielMask && !stubsIn)
+    R vs[3][V];
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj)
+    {
+#pragma unroll
+        for (int c = 0; c < V; ++c) vs[jj][c] = kSparse ? vsS[jj][c] : R(0);
+    }
+    if (!kSparse && dielMask)
     {
 #pragma unroll
         for (int jj = 0; jj < 3; ++jj)
@@ -1222,7 +1263,8 @@ __device__ __forceinline__ void stageTile(const StageSrc<S> &a, int tile, unsign
     const long long node0 = (long long)tile * kNodes;
     const long long P = a.P;
     // stubs staged for stub-loaded tiles, unless only a few of their nodes are
-    const bool diel = (flags & kTileDiel) != 0 && (flags & kTileStubSparse) == 0 && a.stub != nullptr;
+    const bool diel = (flags & kTileDiel) != 0 && !(kSparseStubs<S> && (flags & kTileStubSparse) != 0) &&
+                      a.stub != nullptr;
     // x segments: the tile and L::kHalo nodes on each side, clipped to the planes
     const long long x0 = max(node0 - L::kHalo, 0LL), x1 = min(node0 + kNodes + L::kHalo, P);
     const unsigned segX = L::kSegX * E, xOff = (unsigned)(x0 - (node0 - L::kHalo)) * E;
@@ -1346,7 +1388,8 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             const int e = __shfl_sync(0xffffffffu, win.a, i - win.it0);
             bool ok = true;
             if (i >= STAGES && lane == 0)
-                ok = mbarWaitBounded(empty0 + 8 * s, (unsigned)(i / STAGES - 1) & 1u, a.stage_wait_ns);
+                ok = mbarWaitPaused<std::is_same<S, float>::value ? kProducerPauseNs : 0>(
+                    empty0 + 8 * s, (unsigned)(i / STAGES - 1) & 1u, a.stage_wait_ns);
             if (!__shfl_sync(0xffffffffu, ok, 0))
             {
                 if (lane == 0 && a.fault) atomicOr(a.fault, kStageTimeout);
@@ -1378,8 +1421,19 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         const int e = tiles[blockIdx.x + i * gridDim.x];
         const int tile = entryTile(e);
         const uint8_t tf = a.tile_flags[tile];
-        stepTileInterior<S, V, true>(a, tile, red[s], (tf & kTileDiel) != 0, stage + s * kBytes,
-                                      ered0 + 8 * s, (unsigned)(i / STAGES) & 1u, (tf & kTileStubSparse) == 0);
+        bool done = false;
+        if constexpr (kSparseStubs<S>)
+        {
+            if (tf & kTileStubSparse)
+            {
+                stepTileInterior<S, V, true, true>(a, tile, red[s], true, stage + s * kBytes, ered0 + 8 * s,
+                                                   (unsigned)(i / STAGES) & 1u);
+                done = true;
+            }
+        }
+        if (!done)
+            stepTileInterior<S, V, true>(a, tile, red[s], (tf & kTileDiel) != 0, stage + s * kBytes,
+                                          ered0 + 8 * s, (unsigned)(i / STAGES) & 1u);
         __syncwarp();
         if ((threadIdx.x & 31) == 0)
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(empty0 + 8 * s) : "memory");
