@@ -254,6 +254,7 @@ struct tlm_solver
     uint8_t *dTileFlags = nullptr;  // per step-kernel tile: tlmk::kTileGeneral / kTileDiel / kTileEdge
     int *dStaged = nullptr, *dListed = nullptr;  // tiles of the staged kernel / of the list kernel
     int nStaged = 0, nListed = 0, stagedGrid = 0;
+    bool sparseStaged = false;  // a staged tile is a sparse-stub tile (FP32)
     // host copies (a batch builds its tile tables from them); staged and edge
     // tiles as packed entries (tlmk::packStagedEntry: tile | flags << 24)
     std::vector<int> stagedTiles, listedTiles;

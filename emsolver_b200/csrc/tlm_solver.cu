@@ -289,9 +289,15 @@ template <class S> constexpr int stagedSmem()
 
 template <class S> tlm_status stagedAttributes(tlm_solver *h)
 {
-    return h->cuda(cudaFuncSetAttribute(tlmk::stepKernelStaged<S, StagedShape<S>::V, StagedShape<S>::kStages>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, stagedSmem<S>()),
-                   "cudaFuncSetAttribute(stepKernelStaged)");
+    TLM_TRY(h->cuda(cudaFuncSetAttribute(tlmk::stepKernelStaged<S, StagedShape<S>::V, StagedShape<S>::kStages>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, stagedSmem<S>()),
+                    "cudaFuncSetAttribute(stepKernelStaged)"));
+    if constexpr (tlmk::kSparseStubs<S>)
+        TLM_TRY(h->cuda(cudaFuncSetAttribute(
+                            tlmk::stepKernelStaged<S, StagedShape<S>::V, StagedShape<S>::kStages, 2, true>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, stagedSmem<S>()),
+                        "cudaFuncSetAttribute(stepKernelStaged)"));
+    return TLM_OK;
 }
 
 // FP32 with 2 nodes per thread (the default shape): interior tiles go to the
@@ -303,6 +309,7 @@ template <class S> tlm_status stagedAttributes(tlm_solver *h)
 tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
 {
     h->nStaged = h->nListed = 0;
+    h->sparseStaged = false;
     h->stagedTiles.clear();
     h->listedTiles.clear();
     h->edgeTiles.clear();
@@ -371,6 +378,7 @@ tlm_status prepareStaging(tlm_solver *h, const std::vector<uint8_t> &flags)
                                   h->stream));
     }
     h->nStaged = (int)staged.size();
+    for (int e : staged) h->sparseStaged |= (tlmk::entryFlags(e) & tlmk::kTileStubSparse) != 0;
     h->nListed = (int)listed.size();
     h->stagedTiles = std::move(staged);
     h->listedTiles = std::move(listed);
@@ -642,8 +650,14 @@ template <class S> tlm_status launchStep(tlm_solver *h, int n, int i, long long 
                 tlmk::stepKernelList<S, 2, 4, true><<<h->nListed, kBlock, 0, h->side>>>(a, h->dListed);
                 TLM_CU(h, cudaEventRecord(h->evJoin, h->side));
             }
-            tlmk::stepKernelStaged<S, 2><<<h->stagedGrid, tlmk::kStagedThreads, tlmk::kStages * tlmk::Stage<S>::kBytes,
-                                           h->stream>>>(a, h->dStaged, h->nStaged);
+            if (h->sparseStaged)
+                tlmk::stepKernelStaged<S, 2, tlmk::kStages, 2, true>
+                    <<<h->stagedGrid, tlmk::kStagedThreads, tlmk::kStages * tlmk::Stage<S>::kBytes, h->stream>>>(
+                        a, h->dStaged, h->nStaged);
+            else
+                tlmk::stepKernelStaged<S, 2><<<h->stagedGrid, tlmk::kStagedThreads,
+                                               tlmk::kStages * tlmk::Stage<S>::kBytes, h->stream>>>(a, h->dStaged,
+                                                                                                     h->nStaged);
             if (h->nListed > 0) TLM_CU(h, cudaStreamWaitEvent(h->stream, h->evJoin, 0));
         }
         else
@@ -1716,7 +1730,11 @@ template <class S> tlm_status slabLaunch(tlm_solver *h, int phase)
         }
         if constexpr (std::is_same<S, float>::value && V() == 2 && SEL())
         {
-            if (h->nSlabS > 0)
+            if (h->nSlabS > 0 && h->sparseStaged)
+                tlmk::stepKernelStaged<S, 2, tlmk::kStages, 2, true>
+                    <<<h->slabStagedGrid, tlmk::kStagedThreads, tlmk::kStages * tlmk::Stage<S>::kBytes, h->stream>>>(
+                        a, h->dSlabS, h->nSlabS);
+            else if (h->nSlabS > 0)
                 tlmk::stepKernelStaged<S, 2><<<h->slabStagedGrid, tlmk::kStagedThreads,
                                                tlmk::kStages * tlmk::Stage<S>::kBytes, h->stream>>>(a, h->dSlabS,
                                                                                                     h->nSlabS);

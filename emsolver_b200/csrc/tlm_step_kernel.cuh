@@ -281,9 +281,10 @@ __device__ __forceinline__ bool mbarWaitPaused(unsigned bar, unsigned parity,
         if ((it & 15u) == 0 && globalTimerNs() - t0 > limitNs) return false;
     }
 }
-// FP32 single grid: 512 ns (192^3 heterogeneous 127.9 -> 126.7 us per step,
-// the 384x384x256 dipole 567 -> 571 us); the 16-bit and batch producers poll
-// without a pause (with 512 ns the dipole in FP16 stepped 5 % slower).
+// FP32 single grid: 512 ns (192^3 heterogeneous 127.9 -> 126.7 us per step;
+// 32 polls before the first pause measured 128.0 us); the 16-bit and batch
+// producers poll without a pause (with 512 ns the 384x384x256 dipole in
+// FP16 stepped 5 % slower).
 constexpr unsigned kProducerPauseNs = 512;
 
 __device__ __forceinline__ void bulkCopy(unsigned dst, const void *src, unsigned bytes, unsigned bar)
@@ -1252,8 +1253,9 @@ __device__ __forceinline__ void stageRuns(const StageSrc<S> &a, long long node0,
 // itself (measured faster than spreading them), while on a tile with
 // outer-face nodes lanes 0-3 copy the x segments, lanes 4-11 assemble one y/z
 // segment each from its runs, lanes 12-14 copy the stubs and lane 15 the
-// material.
-template <int V = 2, class S>
+// material. SPARSE: the consumers run sparse-stub tiles (kTileStubSparse)
+// without staged stubs.
+template <int V = 2, bool SPARSE = true, class S>
 __device__ __forceinline__ void stageTile(const StageSrc<S> &a, int tile, unsigned flags, unsigned st, unsigned bar,
                                           int lane)
 {
@@ -1263,7 +1265,7 @@ __device__ __forceinline__ void stageTile(const StageSrc<S> &a, int tile, unsign
     const long long node0 = (long long)tile * kNodes;
     const long long P = a.P;
     // stubs staged for stub-loaded tiles, unless only a few of their nodes are
-    const bool diel = (flags & kTileDiel) != 0 && !(kSparseStubs<S> && (flags & kTileStubSparse) != 0) &&
+    const bool diel = (flags & kTileDiel) != 0 && !(kSparseStubs<S> && SPARSE && (flags & kTileStubSparse) != 0) &&
                       a.stub != nullptr;
     // x segments: the tile and L::kHalo nodes on each side, clipped to the planes
     const long long x0 = max(node0 - L::kHalo, 0LL), x1 = min(node0 + kNodes + L::kHalo, P);
@@ -1350,7 +1352,10 @@ template <class T> struct EntryWindow
     }
 };
 
-template <class S, int V, int STAGES = kStages, int MINB = 2>
+// SPARSE: the grid has sparse-stub tiles (FP32): their instantiation of the
+// tile body is compiled in only then, so that other grids keep the kernel
+// they had (with it, a grid without dielectrics stepped 1 % slower).
+template <class S, int V, int STAGES = kStages, int MINB = 2, bool SPARSE = false>
 __global__ void __launch_bounds__(kStagedThreads, MINB)
     stepKernelStaged(const StepArgs<S> a, const int *__restrict__ tiles, int ntiles)
 {
@@ -1395,7 +1400,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
                 if (lane == 0 && a.fault) atomicOr(a.fault, kStageTimeout);
                 break;
             }
-            stageTile<V>(src, entryTile(e), entryFlags(e), st0 + s * kBytes, full0 + 8 * s, lane);
+            stageTile<V, SPARSE>(src, entryTile(e), entryFlags(e), st0 + s * kBytes, full0 + 8 * s, lane);
             issued = i + 1;
         }
         // the copies of the last STAGES tiles may still be landing: stay
@@ -1422,7 +1427,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         const int tile = entryTile(e);
         const uint8_t tf = a.tile_flags[tile];
         bool done = false;
-        if constexpr (kSparseStubs<S>)
+        if constexpr (kSparseStubs<S> && SPARSE)
         {
             if (tf & kTileStubSparse)
             {
