@@ -63,9 +63,9 @@ def parse():
                    help="slab: edge of the heterogeneous grid split into z-slabs over the ranks")
     p.add_argument("--order", default="least-work", choices=["least-work", "arrival"],
                    help="served: admission order")
-    p.add_argument("--max-running-cells", type=int, default=32 << 20,
+    p.add_argument("--max-running-cells", type=int, default=8 << 20,
                    help="served: cap on the running requests' padded cells (0: none)")
-    p.add_argument("--solo-cells", type=int, default=4 << 20,
+    p.add_argument("--solo-cells", type=int, default=1 << 20,
                    help="served: requests this large run on their own beside the batch (0: never)")
     p.add_argument("--served-16bit", default="f16nf", choices=["f16nf", "bf16"],
                    help="served: storage of the stream's 16-bit half")

@@ -93,7 +93,7 @@ class Server:
 
     ARRIVAL, LEAST_WORK = 0, 1
 
-    def set_policy(self, order: int = 1, max_running_cells: int = 32 << 20, solo_cells: int = 4 << 20):
+    def set_policy(self, order: int = 1, max_running_cells: int = 8 << 20, solo_cells: int = 1 << 20):
         """Admission order (LEAST_WORK first, or ARRIVAL), the cap on the
         running requests' padded cells (0: none), and the size from which a
         request runs on its own beside the batch (0: never)."""

@@ -406,9 +406,9 @@ TLM_API tlm_status tlm_server_create(tlm_server *out, int device, size_t hbm_bud
  * the fewest padded cells x steps first, so short solves are not held up
  * behind long ones) or TLM_SERVE_ARRIVAL (first come, first served);
  * max_running_cells caps the padded cells of the running requests (0 = no
- * cap; default 32 Mi), above which queued requests wait rather than slow
+ * cap; default 8 Mi), above which queued requests wait rather than slow
  * every running one down. The first request always runs. Requests of
- * solo_cells padded cells or more (0 = none; default 4 Mi) do not join the
+ * solo_cells padded cells or more (0 = none; default 1 Mi) do not join the
  * batch: large grids fill the GPU alone, so they are stepped window by
  * window on their own stream by the single-grid kernels, beside the batch. */
 enum { TLM_SERVE_ARRIVAL = 0, TLM_SERVE_LEAST_WORK = 1 };
