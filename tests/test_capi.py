@@ -98,3 +98,43 @@ def test_request_footprint_without_device(built):
     assert f32 - bf16 == 2 * 12 * P * 2
     w2 = workloads.dipole(32, 32, 48, 21, slab=(2, 6, 3.0), steps=500)
     assert footprint(w2, storage=0) - f32 == 3 * P * 4
+
+
+# ctypes mirror -> C type of the headers
+STRUCTS = {
+    "Grid": "tlm_grid", "MatPropsC": "tlm_matprops", "ConfigC": "tlm_config",
+    "BatchTuningC": "tlm_batch_tuning", "RequestC": "tlm_request", "ServerStatsC": "tlm_server_stats_t",
+    "EmsimFaceC": "emsim_face", "EmsimToolbarC": "emsim_toolbar", "EmsimObjectC": "emsim_object",
+    "EmsimPatternC": "emsim_pattern", "EmsimResultC": "emsim_result", "EmsimCurveC": "emsim_curve",
+    "EmsimFrameC": "emsim_frame", "EmsimCaptureC": "emsim_capture",
+}
+
+
+def test_ctypes_structs_match_the_headers(tmp_path):
+    """Every structure the Python binding passes across the C ABI has the
+    size and field offsets the headers give it (compiled here with g++)."""
+    import shutil
+    import subprocess
+    if not shutil.which("g++"):
+        pytest.skip("no g++")
+    lines = ["#include <cstddef>", "#include <cstdio>", '#include "tlm_b200.h"', '#include "emsim_b200.h"',
+             "int main() {"]
+    for py, c in STRUCTS.items():
+        lines.append(f'std::printf("{py} size %zu\\n", sizeof({c}));')
+        for name, _ in getattr(_lib, py)._fields_:
+            lines.append(f'std::printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.cpp"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        py, name, value = line.split()
+        got[(py, name)] = int(value)
+    for py in STRUCTS:
+        cls = getattr(_lib, py)
+        assert got[(py, "size")] == C.sizeof(cls), py
+        for name, _ in cls._fields_:
+            assert got[(py, name)] == getattr(cls, name).offset, (py, name)
