@@ -337,10 +337,11 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             const unsigned ep = (eBits >> s) & 1u;
             if (a.epart != nullptr) eBits ^= 1u << s;
             if (tail1.y & kTileStubSparse)
-                stepTileInterior<float, 2, true, true>(a, tile, red[s], true, stage + s * kData, ered0 + 8 * s, ep);
+                stepTileInterior<float, 2, true, true, false>(a, tile, red[s], true, stage + s * kData, ered0 + 8 * s,
+                                                              ep);
             else
-                stepTileInterior<float, 2, true>(a, tile, red[s], (tail1.y & kTileDiel) != 0, stage + s * kData,
-                                                 ered0 + 8 * s, ep);
+                stepTileInterior<float, 2, true, false, false>(a, tile, red[s], (tail1.y & kTileDiel) != 0,
+                                                               stage + s * kData, ered0 + 8 * s, ep);
         }
         __syncwarp();
         if ((threadIdx.x & 31) == 0)

@@ -307,7 +307,7 @@ __device__ __forceinline__ void bulkCopy(unsigned dst, const void *src, unsigned
 // kSparse (kStaged only): a kTileStubSparse tile, whose stage holds no
 // stubs; its stub-loaded nodes load theirs from a.stub first thing (a
 // separate instantiation, so the other tiles keep the code they had).
-template <class S, int V, bool kStaged = false, bool kSparse = false>
+template <class S, int V, bool kStaged = false, bool kSparse = false, bool kZeroSkip = true>
 __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile, double *red, bool diel,
                                                  const unsigned char *sm = nullptr, unsigned eBar = 0,
                                                  unsigned eParity = 0)
@@ -573,8 +573,8 @@ __device__ __forceinline__ void stepTileInterior(const StepArgs<S> &a, int tile,
 #pragma unroll
             for (int jj = 0; jj < 3; ++jj) v2[jj] = make_float2(vs[jj][c0], vs[jj][c1]);
             const int id0 = m[c0] - kDiel0, id1 = m[c1] - kDiel0;
-            scatterStub2(in2, v2, make_float2(a.yhat[id0], a.yhat[id1]), make_float2(a.ghat[id0], a.ghat[id1]),
-                         o2, z);
+            scatterStub2<kZeroSkip>(in2, v2, make_float2(a.yhat[id0], a.yhat[id1]),
+                                    make_float2(a.ghat[id0], a.ghat[id1]), o2, z);
 #pragma unroll
             for (int s = 0; s < 12; ++s)
             {
