@@ -708,7 +708,14 @@ def run_batched(args):
     nodes = sum(w.ncells for w in ws)
     work = sum(w.ncells * w.steps for w in ws)
     sequential_solves(ws[:4])                        # warm-up (context, kernels)
+    # Python's cyclic garbage collector is paused in both timed regions, as
+    # timeit does: a collection pass landing in one of them (over the
+    # thousands of workload objects alive here) measured up to 0.8 s
+    import gc
+    gc.collect()
+    gc.disable()
     seq = sequential_solves(ws)
+    gc.enable()
     # the solves through Batch.solve: set-up of the next instances overlaps
     # the device's windows, finished members leave at once
     tp = time.perf_counter()
@@ -734,6 +741,8 @@ def run_batched(args):
     # device pool), so the host work is spread over --host-threads threads
     from concurrent.futures import ThreadPoolExecutor
     pool = ThreadPoolExecutor(max_workers=max(1, args.host_threads))
+    gc.collect()
+    gc.disable()
     t0 = time.perf_counter()
     solvers = list(pool.map(build_solver, ws))
     tb = time.perf_counter()
@@ -753,10 +762,12 @@ def run_batched(args):
     got = list(pool.map(lambda s: s.portDft(0), solvers))
     t2 = time.perf_counter()
     b.close()
+    tc = time.perf_counter()
     nbox = sum(box_nodes(s) for s in solvers)
     list(pool.map(lambda s: s.close(), solvers))
     t3 = time.perf_counter()
     pool.shutdown()
+    gc.enable()
     batched_s = t3 - t0
     # accuracy: S11 of every instance against the FP64 storage mode
     ref = batch_dfts(ws, 3, 0)
@@ -775,7 +786,7 @@ def run_batched(args):
         "config": {"workload": f"batched: {len(ws)} dipole instances, edges U{{24..96}}, 1000 steps",
                    "nodes": nodes, "storage": args.storage, "near_field": nf,
                    "tuning": tuning.__dict__, "autotuned": not args.no_autotune,
-                   "host_threads": args.host_threads,
+                   "host_threads": args.host_threads, "python_gc": "paused in the timed regions",
                    "includes": "setup of every instance, all steps, port DFT read-back, free"},
         "sequential_plain_gpu": {"value": len(ws) / sum(seq), "unit": "solves/s",
                                  "seconds": sum(seq), "p50_s": float(np.percentile(seq, 50)),
@@ -789,7 +800,8 @@ def run_batched(args):
                       "api": "Batch.solve: host set-up of the next chunk overlaps each window"},
         "batched_gpu": {"node_updates_per_s": work / (gpu_ms / 1e3), "seconds": gpu_ms / 1e3,
                         "setup_s": t1 - t0, "setup_build_s": tb - t0, "setup_attach_s": ta - tb,
-                        "readback_s": t2 - t1 - gpu_ms / 1e3,
+                        "readback_s": t2 - t1 - gpu_ms / 1e3, "batch_close_s": tc - t2,
+                        "free_s": t3 - tc,
                         "hbm_frac": bytes_all / (gpu_ms / 1e3) / 1e9 / peak, "peak_kind": kind},
     }
     print(json.dumps(line), flush=True)
