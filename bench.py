@@ -709,8 +709,8 @@ def run_batched(args):
     work = sum(w.ncells * w.steps for w in ws)
     sequential_solves(ws[:4])                        # warm-up (context, kernels)
     # Python's cyclic garbage collector is paused in both timed regions, as
-    # timeit does: a collection pass landing in one of them (over the
-    # thousands of workload objects alive here) measured up to 0.8 s
+    # timeit does, so that a collection pass over the thousands of workload
+    # objects alive here lands in neither
     import gc
     gc.collect()
     gc.disable()
