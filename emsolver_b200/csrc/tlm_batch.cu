@@ -190,13 +190,27 @@ template <class S> MemberDesc<S> makeDesc(tlm_solver *h)
     return d;
 }
 
+// The batch's tables come from the library's stream-ordered pool: allocated
+// and released in order on the batch stream, without the device-wide
+// synchronisation of cudaMalloc/cudaFree (a batch grows its tables between
+// windows while a server's solo requests step on other streams).
+cudaError_t batchAlloc(tlm_batch_s *b, void **p, size_t bytes)
+{
+    cudaMemPool_t pool = devicePool(b->device);
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, b->stream) : cudaMallocAsync(p, bytes, b->stream);
+}
+void batchFree(tlm_batch_s *b, void *p)
+{
+    if (p) cudaFreeAsync(p, b->stream);
+}
+
 tlm_status growBuffer(tlm_batch_s *b, void **p, int *cap, int need, size_t elem)
 {
     if (need <= *cap && *p) return TLM_OK;
     int c = std::max(need, std::max(16, *cap * 2));
     void *q = nullptr;
-    TLM_BCU(b, cudaMalloc(&q, (size_t)c * elem));
-    if (*p) cudaFree(*p);
+    TLM_BCU(b, batchAlloc(b, &q, (size_t)c * elem));
+    batchFree(b, *p);
     *p = q;
     *cap = c;
     b->graphDirty = true;  // kernels captured with the old address
@@ -218,12 +232,12 @@ tlm_status syncGroupTables(tlm_batch_s *b, Group &g)
     TLM_TRY(growBuffer(b, &g.dMembers, &g.capMembers, std::max(nm, 1), g.descBytes));
     if (!g.dNMembers)
     {
-        TLM_BCU(b, cudaMalloc(&g.dNMembers, sizeof(int)));
+        TLM_BCU(b, batchAlloc(b, (void **)&g.dNMembers, sizeof(int)));
         b->graphDirty = true;
     }
     if (!g.dNTiles)
     {
-        TLM_BCU(b, cudaMalloc(&g.dNTiles, sizeof(int)));
+        TLM_BCU(b, batchAlloc(b, (void **)&g.dNTiles, sizeof(int)));
         b->graphDirty = true;
     }
     std::vector<char> descs((size_t)std::max(nm, 1) * g.descBytes, 0);
@@ -265,7 +279,7 @@ tlm_status syncGroupTables(tlm_batch_s *b, Group &g)
     {
         if (!g.dNStaged)
         {
-            TLM_BCU(b, cudaMalloc(&g.dNStaged, sizeof(int)));
+            TLM_BCU(b, batchAlloc(b, (void **)&g.dNStaged, sizeof(int)));
             b->graphDirty = true;
         }
         int scap = g.capStaged;
@@ -618,12 +632,12 @@ tlm_status applyTuning(tlm_batch_s *b, const tlm_batch_tuning &t)
     for (auto &kv : b->groups)
     {
         Group &g = kv.second;
-        if (g.dMembers) cudaFree(g.dMembers);
-        if (g.dTiles) cudaFree(g.dTiles);
-        if (g.dNTiles) cudaFree(g.dNTiles);
-        if (g.dNMembers) cudaFree(g.dNMembers);
-        if (g.dStaged) cudaFree(g.dStaged);
-        if (g.dNStaged) cudaFree(g.dNStaged);
+        batchFree(b, g.dMembers);
+        batchFree(b, g.dTiles);
+        batchFree(b, g.dNTiles);
+        batchFree(b, g.dNMembers);
+        batchFree(b, g.dStaged);
+        batchFree(b, g.dNStaged);
     }
     b->groups = std::move(regrouped);
     b->graphDirty = true;
@@ -660,8 +674,9 @@ tlm_status tlm_batch_create(tlm_batch *out, int device)
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evFork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evJoin, cudaEventDisableTiming);
     // error flags: bounds checks (checked build), staged-tile waits (every build)
-    if (e == cudaSuccess) e = cudaMalloc(&b->dFault, sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMemset(b->dFault, 0, sizeof(unsigned));
+    if (e == cudaSuccess) e = batchAlloc(b, (void **)&b->dFault, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->dFault, 0, sizeof(unsigned), b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess)
     {
         setThreadError(std::string("batch creation: ") + cudaGetErrorString(e));
@@ -685,15 +700,15 @@ tlm_status tlm_batch_destroy(tlm_batch b)
     {
         for (tlm_solver *h : kv.second.members) h->batch = nullptr;
         Group &g = kv.second;
-        if (g.dMembers) cudaFree(g.dMembers);
-        if (g.dTiles) cudaFree(g.dTiles);
-        if (g.dNTiles) cudaFree(g.dNTiles);
-        if (g.dNMembers) cudaFree(g.dNMembers);
-        if (g.dStaged) cudaFree(g.dStaged);
-        if (g.dNStaged) cudaFree(g.dNStaged);
+        batchFree(b, g.dMembers);
+        batchFree(b, g.dTiles);
+        batchFree(b, g.dNTiles);
+        batchFree(b, g.dNMembers);
+        batchFree(b, g.dStaged);
+        batchFree(b, g.dNStaged);
     }
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    if (b->dFault) cudaFree(b->dFault);
+    batchFree(b, b->dFault);
     cudaStreamSynchronize(b->side);
     cudaEventDestroy(b->evJoin);
     cudaEventDestroy(b->evFork);
