@@ -271,14 +271,19 @@ template <unsigned PAUSE_NS>
 __device__ __forceinline__ bool mbarWaitPaused(unsigned bar, unsigned parity,
                                                unsigned long long limitNs = kStageWaitNs)
 {
-    if (mbarTestWait(bar, parity)) return true;
-    if (limitNs == 0) return false;
-    const unsigned long long t0 = globalTimerNs();
-    for (unsigned it = 1;; ++it)
+    if constexpr (PAUSE_NS == 0)
+        return mbarWaitBounded(bar, parity, limitNs);
+    else
     {
-        if (PAUSE_NS > 0) __nanosleep(PAUSE_NS);
         if (mbarTestWait(bar, parity)) return true;
-        if ((it & 15u) == 0 && globalTimerNs() - t0 > limitNs) return false;
+        if (limitNs == 0) return false;
+        const unsigned long long t0 = globalTimerNs();
+        for (unsigned it = 1;; ++it)
+        {
+            __nanosleep(PAUSE_NS);
+            if (mbarTestWait(bar, parity)) return true;
+            if ((it & 15u) == 0 && globalTimerNs() - t0 > limitNs) return false;
+        }
     }
 }
 // FP32 single grid: 512 ns (192^3 heterogeneous 127.9 -> 126.7 us per step;
